@@ -1,0 +1,75 @@
+"""ctypes binding of libcdops.so, the C ABI declared in include/cd_ops.h.
+
+The library is built in-tree (``__graft_entry__.build()`` or ``make -C
+cross-denoiser_b200/csrc``).  There is no fallback: if the shared object is
+missing, :func:`lib` raises, so no op can silently run anywhere but on the
+sm_100a kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcdops.so")
+
+CD_OK, CD_EINVAL, CD_ECUDA, CD_ENOMEM = 0, 1, 2, 3
+REPROJECT_MAX_LIST = 8
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_S = ctypes.c_size_t
+
+# name -> (restype, argtypes); mirrors include/cd_ops.h
+SIGNATURES = {
+    "cd_abi_version": (_I, []),
+    "cd_get_last_error": (ctypes.c_char_p, []),
+    "cd_cross_regression_workspace_size": (_S, [_I, _I, _I, _I]),
+    "cd_cross_regression": (_I, [_P] * 8 + [_I] * 6 + [_P, _S, _P]),
+    "cd_spatial_filter": (_I, [_P] * 9 + [_I] * 4 + [_P]),
+    "cd_spatial_filter_grad": (_I, [_P] * 10 + [_I] * 4 + [_P]),
+    "cd_reproject": (_I, [_P, _I, _P, _P, _P] + [_P] * 8 + [_I] * 3 + [_P]),
+    "cd_erode3x3": (_I, [_P, _P, _I, _I, _I, _P]),
+    "cd_temporal_screening": (_I, [_P] * 10 + [_I] * 5 + [_P]),
+    "cd_erode_temporal_screening": (_I, [_P] * 11 + [_I] * 5 + [_P]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class CudaOpError(RuntimeError):
+    """A CUDA launch or runtime call inside the library failed (CD_ECUDA)."""
+
+
+def lib() -> ctypes.CDLL:
+    """Load libcdops.so once and attach the C signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(
+                    f"{LIB_PATH} is not built; run `python -c 'import __graft_entry__ as g; g.build()'` "
+                    "or `make -C cross-denoiser_b200/csrc` first")
+            handle = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(handle, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = handle
+    return _lib
+
+
+def check(status: int, op: str) -> None:
+    """Raise the Python analogue of a non-zero cd_status."""
+    if status == CD_OK:
+        return
+    msg = lib().cd_get_last_error().decode(errors="replace")
+    if status == CD_EINVAL:
+        raise ValueError(f"{op}: {msg}")
+    if status == CD_ENOMEM:
+        raise MemoryError(f"{op}: {msg}")
+    raise CudaOpError(f"{op}: {msg}")

@@ -1,0 +1,226 @@
+// C ABI of the per-frame hot path (declared in include/cd_ops.h).
+//
+// Every entry point validates its arguments on the host, enqueues its
+// kernels on the caller's stream and reports failures as cd_status codes
+// with a thread-local message; nothing here exits, allocates device memory or
+// synchronises.  The argument checks mirror the reference op wrappers'
+// OP_REQUIRES checks (ops/regression.cc:134-135, 159-160) and reject the
+// shapes on which the reference kernels would index out of bounds.
+#include <cstdarg>
+#include <cstdio>
+#include <cuda_runtime.h>
+#include "cd_common.cuh"
+#include "../../include/cd_ops.h"
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+cd_status fail(cd_status s, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return s;
+}
+
+cd_status cuda_status(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return CD_OK;
+    return fail(CD_ECUDA, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+}
+
+bool dims_ok(int B, int H, int W) { return B >= 1 && B <= 32767 && H >= 1 && W >= 1 && H <= 65535 * 8 && W <= (1 << 24); }
+
+// Shared-memory footprints of the tiled kernels (must agree with the kernel
+// translation units; checked here so that an oversized window is an argument
+// error rather than a launch failure).
+size_t regression_tile_bytes(int hw, int sp)
+{
+    const int pw = 7 * sp + 2 * hw + 1, ph = 2 * hw + 1;
+    return (size_t)16 * ph * (pw | 1) * sizeof(float);
+}
+size_t filter_tile_bytes(int hw) { return (size_t)12 * (32 + 2 * hw) * (8 + 2 * hw) * 4 + 1024; }
+size_t temporal_tile_bytes(int hc)
+{
+    return ((size_t)6 * (32 + 2 * hc) * (8 + 2 * hc) + (size_t)18 * (8 + 2 * hc) * 32) * 4;
+}
+constexpr size_t kSmemLimit = 220 * 1024;
+
+}  // namespace
+
+extern "C" {
+
+int cd_abi_version(void) { return 1; }
+
+const char *cd_get_last_error(void) { return g_err; }
+
+size_t cd_cross_regression_workspace_size(int B, int H, int W, int sparsity)
+{
+    if (!dims_ok(B, H, W) || sparsity < 1) return 0;
+    return (size_t)2 * B * (H / sparsity) * (W / sparsity) * 18 * sizeof(float);
+}
+
+cd_status cd_cross_regression(const float *imga, const float *imgb, const float *albedo,
+                              const float *normal, float *outa, float *outb, float *vara,
+                              float *varb, int B, int H, int W, int win_size, int sparsity,
+                              int recon_scale, void *workspace, size_t workspace_bytes,
+                              cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!imga || !imgb || !albedo || !normal || !outa || !outb || !vara || !varb)
+        return fail(CD_EINVAL, "cross_regression: null tensor pointer");
+    if (!dims_ok(B, H, W)) return fail(CD_EINVAL, "cross_regression: bad shape B=%d H=%d W=%d", B, H, W);
+    if (win_size < 1 || sparsity < 1 || recon_scale < 1)
+        return fail(CD_EINVAL, "cross_regression: win_size, sparsity and recon_scale must be >= 1");
+    if (recon_scale > sparsity)
+        return fail(CD_EINVAL, "recon_scale must be less than or equal to sparsity");
+    if (H % recon_scale != 0 || W % recon_scale != 0)
+        return fail(CD_EINVAL, "Image height and width must be divisible by recon_scale");
+    if (H % sparsity != 0 || W % sparsity != 0)
+        return fail(CD_EINVAL, "cross_regression: image height and width must be divisible by sparsity "
+                               "(got %dx%d, sparsity %d)", H, W, sparsity);
+    const int hw = win_size / 2;
+    if (hw >= H || hw >= W)
+        return fail(CD_EINVAL, "cross_regression: window radius %d must be smaller than the image (%dx%d)", hw, H, W);
+    if (regression_tile_bytes(hw, sparsity) > kSmemLimit)
+        return fail(CD_EINVAL, "cross_regression: win_size %d with sparsity %d exceeds the shared-memory tile", win_size, sparsity);
+    const size_t need = cd_cross_regression_workspace_size(B, H, W, sparsity);
+    if (workspace_bytes < need || (need > 0 && !workspace))
+        return fail(CD_ENOMEM, "cross_regression: workspace of %zu bytes needed, %zu given", need, workspace_bytes);
+
+    float *beta = static_cast<float *>(workspace);
+    cd_status s;
+    if ((s = cuda_status(cd::launch_variance(imga, imgb, vara, varb, B, H, W, stream), "variance")) != CD_OK) return s;
+    if ((s = cuda_status(cd::launch_regression(imga, imgb, albedo, normal, vara, varb, beta, B, H, W,
+                                               win_size, sparsity, stream), "regression")) != CD_OK) return s;
+    return cuda_status(cd::launch_recon(imga, imgb, albedo, normal, vara, varb, beta, outa, outb, B, H,
+                                        W, win_size, sparsity, recon_scale, stream), "recon");
+}
+
+cd_status cd_spatial_filter(const float *imga, const float *imgb, const float *albedo,
+                            const float *normal, const float *band, float *out_acca,
+                            float *out_accb, float *out_wgtsuma, float *out_wgtsumb, int B, int H,
+                            int W, int win_size, cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!imga || !imgb || !albedo || !normal || !band || !out_acca || !out_accb || !out_wgtsuma || !out_wgtsumb)
+        return fail(CD_EINVAL, "spatial_filter: null tensor pointer");
+    if (!dims_ok(B, H, W)) return fail(CD_EINVAL, "spatial_filter: bad shape B=%d H=%d W=%d", B, H, W);
+    if (win_size < 1) return fail(CD_EINVAL, "spatial_filter: win_size must be >= 1");
+    const int hw = win_size / 2;
+    if (hw >= H || hw >= W)
+        return fail(CD_EINVAL, "spatial_filter: window radius %d must be smaller than the image (%dx%d)", hw, H, W);
+    if (filter_tile_bytes(hw) > kSmemLimit)
+        return fail(CD_EINVAL, "spatial_filter: win_size %d exceeds the shared-memory tile", win_size);
+    return cuda_status(cd::launch_spatial_filter(imga, imgb, albedo, normal, band, out_acca, out_accb,
+                                                 out_wgtsuma, out_wgtsumb, B, H, W, win_size, stream),
+                       "spatial_filter");
+}
+
+cd_status cd_spatial_filter_grad(const float *grad_acca, const float *grad_accb,
+                                 const float *grad_wgtsuma, const float *grad_wgtsumb,
+                                 const float *imga, const float *imgb, const float *albedo,
+                                 const float *normal, const float *band, float *out_grad_band,
+                                 int B, int H, int W, int win_size, cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!grad_acca || !grad_accb || !grad_wgtsuma || !grad_wgtsumb || !imga || !imgb || !albedo ||
+        !normal || !band || !out_grad_band)
+        return fail(CD_EINVAL, "spatial_filter_grad: null tensor pointer");
+    if (!dims_ok(B, H, W)) return fail(CD_EINVAL, "spatial_filter_grad: bad shape B=%d H=%d W=%d", B, H, W);
+    if (win_size < 1) return fail(CD_EINVAL, "spatial_filter_grad: win_size must be >= 1");
+    const int hw = win_size / 2;
+    if (hw >= H || hw >= W)
+        return fail(CD_EINVAL, "spatial_filter_grad: window radius %d must be smaller than the image (%dx%d)", hw, H, W);
+    if (filter_tile_bytes(hw) > kSmemLimit)
+        return fail(CD_EINVAL, "spatial_filter_grad: win_size %d exceeds the shared-memory tile", win_size);
+    return cuda_status(cd::launch_spatial_filter_grad(grad_acca, grad_accb, grad_wgtsuma, grad_wgtsumb,
+                                                      imga, imgb, albedo, normal, band, out_grad_band,
+                                                      B, H, W, win_size, stream),
+                       "spatial_filter_grad");
+}
+
+cd_status cd_reproject(const float *mvec, int n_list, const float *const *input_list,
+                       const int *channels, float *const *output_list, const float *linear_z,
+                       const float *prev_linear_z, const float *normal, const float *prev_normal,
+                       const float *pn_fwidth, const float *opacity, const float *prev_opacity,
+                       uint8_t *success, int B, int H, int W, cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!mvec || !linear_z || !prev_linear_z || !normal || !prev_normal || !pn_fwidth || !opacity ||
+        !prev_opacity || !success)
+        return fail(CD_EINVAL, "reproject: null tensor pointer");
+    if (!dims_ok(B, H, W)) return fail(CD_EINVAL, "reproject: bad shape B=%d H=%d W=%d", B, H, W);
+    if (n_list < 1 || n_list > CD_REPROJECT_MAX_LIST || !input_list || !output_list || !channels)
+        return fail(CD_EINVAL, "reproject: input_list must hold 1..%d tensors", CD_REPROJECT_MAX_LIST);
+    cd::ReprojectList list{};
+    list.n = n_list;
+    for (int d = 0; d < n_list; ++d) {
+        if (!input_list[d] || !output_list[d])
+            return fail(CD_EINVAL, "reproject: null pointer in input_list/output_list[%d]", d);
+        if (channels[d] < 1 || channels[d] > 4096)
+            return fail(CD_EINVAL, "reproject: input_list[%d] has %d channels", d, channels[d]);
+        list.in[d] = input_list[d];
+        list.out[d] = output_list[d];
+        list.ch[d] = channels[d];
+    }
+    return cuda_status(cd::launch_reproject(mvec, list, linear_z, prev_linear_z, normal, prev_normal,
+                                            pn_fwidth, opacity, prev_opacity, success, B, H, W, stream),
+                       "reproject");
+}
+
+cd_status cd_erode3x3(const uint8_t *success, float *out, int B, int H, int W, cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!success || !out) return fail(CD_EINVAL, "erode3x3: null tensor pointer");
+    if (!dims_ok(B, H, W)) return fail(CD_EINVAL, "erode3x3: bad shape B=%d H=%d W=%d", B, H, W);
+    return cuda_status(cd::launch_erode3x3(success, out, B, H, W, stream), "erode3x3");
+}
+
+static cd_status temporal_checks(const char *name, int B, int H, int W, int win_curr, int win_prev)
+{
+    if (!dims_ok(B, H, W)) return fail(CD_EINVAL, "%s: bad shape B=%d H=%d W=%d", name, B, H, W);
+    if (win_curr < 1 || win_prev < 1) return fail(CD_EINVAL, "%s: win_curr and win_prev must be >= 1", name);
+    if (temporal_tile_bytes(win_curr / 2) > kSmemLimit)
+        return fail(CD_EINVAL, "%s: win_curr %d exceeds the shared-memory tile", name, win_curr);
+    return CD_OK;
+}
+
+cd_status cd_temporal_screening(const float *current1, const float *current2, const float *prev,
+                                const float *prev1, const float *prev2, const float *reproj_success,
+                                float *output, float *output1, float *output2, float *success,
+                                int B, int H, int W, int win_curr, int win_prev, cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!current1 || !current2 || !prev || !prev1 || !prev2 || !reproj_success || !output || !output1 ||
+        !output2 || !success)
+        return fail(CD_EINVAL, "temporal_screening: null tensor pointer");
+    cd_status s = temporal_checks("temporal_screening", B, H, W, win_curr, win_prev);
+    if (s != CD_OK) return s;
+    return cuda_status(cd::launch_temporal(current1, current2, prev, prev1, prev2, reproj_success, nullptr,
+                                           nullptr, output, output1, output2, success, B, H, W, win_curr,
+                                           win_prev, stream),
+                       "temporal_screening");
+}
+
+cd_status cd_erode_temporal_screening(const float *current1, const float *current2, const float *prev,
+                                      const float *prev1, const float *prev2, const uint8_t *reproj_mask,
+                                      float *eroded, float *output, float *output1, float *output2,
+                                      float *success, int B, int H, int W, int win_curr, int win_prev,
+                                      cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!current1 || !current2 || !prev || !prev1 || !prev2 || !reproj_mask || !eroded || !output ||
+        !output1 || !output2 || !success)
+        return fail(CD_EINVAL, "erode_temporal_screening: null tensor pointer");
+    cd_status s = temporal_checks("erode_temporal_screening", B, H, W, win_curr, win_prev);
+    if (s != CD_OK) return s;
+    return cuda_status(cd::launch_temporal(current1, current2, prev, prev1, prev2, nullptr, reproj_mask,
+                                           eroded, output, output1, output2, success, B, H, W, win_curr,
+                                           win_prev, stream),
+                       "erode_temporal_screening");
+}
+
+}  // extern "C"

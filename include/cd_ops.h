@@ -1,0 +1,193 @@
+/*
+ * cd_ops.h -- C ABI of the B200 (sm_100a) per-frame hot path of the online
+ * cross-regression denoiser.
+ *
+ * Every entry point is stateless and stream ordered: it validates its
+ * arguments on the host, enqueues kernels on `stream` and returns.  Nothing is
+ * allocated behind the caller's back; ops that need scratch memory take a
+ * caller-owned workspace whose size the matching *_workspace_size() call
+ * reports.  Errors are returned as cd_status codes (never exit(), never
+ * abort()); cd_get_last_error() returns a human-readable message for the most
+ * recent failure on the calling host thread.
+ *
+ * Layout: every image is NHWC float32, contiguous, in device memory.  C = 3 for
+ * colour, albedo, normal, motion vectors, linear depth and pn_fwidth; C = 5 for
+ * band; C = 1 for opacity, variances, weight sums and success masks.  Boolean
+ * masks are one byte per pixel (0 or 1), like TensorFlow's DT_BOOL.
+ *
+ * Each declaration cites the reference interface it replaces
+ * (file:line inside the CGLab-GIST/cross-denoiser source tree).
+ */
+#ifndef CD_OPS_H
+#define CD_OPS_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#if defined(__GNUC__)
+#define CD_API __attribute__((visibility("default")))
+#else
+#define CD_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum cd_status {
+    CD_OK = 0,
+    /* An argument is out of range.  Covers the reference's OP_REQUIRES
+       InvalidArgument checks (ops/regression.cc:134-135, 159-160) and the
+       shapes on which the reference kernels would read or write out of bounds. */
+    CD_EINVAL = 1,
+    /* A CUDA runtime call or kernel launch failed (the reference calls exit(1)
+       through CUDA_CHECK, ops/reproject.cc:23-30). */
+    CD_ECUDA = 2,
+    /* The caller's workspace is smaller than the *_workspace_size() figure. */
+    CD_ENOMEM = 3
+} cd_status;
+
+/* Version of this ABI; bumped on any signature change. */
+CD_API int cd_abi_version(void);
+
+/* Message of the last failing call on this host thread ("" if none). */
+CD_API const char *cd_get_last_error(void);
+
+/* ------------------------------------------------------------------------ */
+/* CrossRegression                                                           */
+/* Replaces REGISTER_OP("CrossRegression") + CrossRegressionOp::Compute       */
+/* (ops/regression.cc:25-57, 147-191) and CrossRegressionFunc                 */
+/* (ops/regression.cu.cc:477-500).                                            */
+/*                                                                            */
+/*  imga, imgb, albedo, normal : [B,H,W,3]                                    */
+/*  outa, outb                 : [B,H/recon_scale,W/recon_scale,3]            */
+/*  vara, varb                 : [B,H,W,1]                                    */
+/* outa is imgb regressed on imga's features, outb the converse; vara/varb    */
+/* are the 3x3 leave-centre-out variance estimates of imga/imgb.              */
+/* Requirements (CD_EINVAL otherwise): win_size >= 1, sparsity >= 1,          */
+/* 1 <= recon_scale <= sparsity, H and W divisible by sparsity and by         */
+/* recon_scale, win_size/2 < min(H, W).                                       */
+/* The workspace holds the per-centre regression coefficients (the           */
+/* reference's process-static betaA/betaB, ops/regression.cc:174-180).        */
+/* ------------------------------------------------------------------------ */
+CD_API size_t cd_cross_regression_workspace_size(int B, int H, int W, int sparsity);
+
+CD_API cd_status cd_cross_regression(const float *imga, const float *imgb,
+                              const float *albedo, const float *normal,
+                              float *outa, float *outb, float *vara, float *varb,
+                              int B, int H, int W,
+                              int win_size, int sparsity, int recon_scale,
+                              void *workspace, size_t workspace_bytes,
+                              cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* SpatialFilter (forward)                                                    */
+/* Replaces REGISTER_OP("SpatialFilter") + SpatialFilterOp::Compute           */
+/* (ops/regression.cc:59-86, 242-281) and SpatialFilterFunc                   */
+/* (ops/regression.cu.cc:502-517).                                            */
+/*  imga, imgb, albedo, normal : [B,H,W,3];  band : [B,H,W,5]                 */
+/*  out_acca, out_accb : [B,H,W,3];  out_wgtsuma, out_wgtsumb : [B,H,W,1]     */
+/* Unlike the reference it stores no per-pixel band partials: the backward   */
+/* below recomputes them.  Requirement: win_size/2 < min(H, W).              */
+/* ------------------------------------------------------------------------ */
+CD_API cd_status cd_spatial_filter(const float *imga, const float *imgb,
+                            const float *albedo, const float *normal,
+                            const float *band,
+                            float *out_acca, float *out_accb,
+                            float *out_wgtsuma, float *out_wgtsumb,
+                            int B, int H, int W, int win_size,
+                            cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* SpatialFilterGrad                                                          */
+/* Replaces REGISTER_OP("SpatialFilterGrad") + SpatialFilterGradOp::Compute   */
+/* (ops/regression.cc:88-103, 290-322), SpatialFilterGradFunc                 */
+/* (ops/regression.cu.cc:519-534) and the Python gradient registration        */
+/* (scripts/ops.py:23-32).  Same argument list as the reference op; the      */
+/* images and band, which the reference passes but does not read, are used  */
+/* here to recompute the filter weights.                                      */
+/*  grad_acca, grad_accb : [B,H,W,3];  grad_wgtsuma, grad_wgtsumb : [B,H,W,1] */
+/*  out_grad_band : [B,H,W,5]                                                 */
+/* ------------------------------------------------------------------------ */
+CD_API cd_status cd_spatial_filter_grad(const float *grad_acca, const float *grad_accb,
+                                 const float *grad_wgtsuma, const float *grad_wgtsumb,
+                                 const float *imga, const float *imgb,
+                                 const float *albedo, const float *normal,
+                                 const float *band, float *out_grad_band,
+                                 int B, int H, int W, int win_size,
+                                 cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Reproject                                                                  */
+/* Replaces REGISTER_OP("Reproject") + ReprojectOp::Compute                   */
+/* (ops/reproject.cc:34-69, 93-171) and ReprojectFunc                         */
+/* (ops/reproject.cu.cc:240-273).                                             */
+/*  mvec, linear_z, prev_linear_z, normal, prev_normal, pn_fwidth : [B,H,W,3] */
+/*  opacity, prev_opacity : [B,H,W,1];  success : [B,H,W,1] bytes (0/1)       */
+/*  input_list[i], output_list[i] : [B,H,W,channels[i]]                        */
+/* input_list, output_list and channels are HOST arrays of n_list entries    */
+/* (device pointers / channel counts); they travel in the kernel parameter   */
+/* block, so no pointer table is copied to the device.                       */
+/* Requirements: 1 <= n_list <= CD_REPROJECT_MAX_LIST, channels[i] >= 1.     */
+/* ------------------------------------------------------------------------ */
+#define CD_REPROJECT_MAX_LIST 8
+
+CD_API cd_status cd_reproject(const float *mvec,
+                       int n_list, const float *const *input_list,
+                       const int *channels, float *const *output_list,
+                       const float *linear_z, const float *prev_linear_z,
+                       const float *normal, const float *prev_normal,
+                       const float *pn_fwidth,
+                       const float *opacity, const float *prev_opacity,
+                       uint8_t *success,
+                       int B, int H, int W, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* 3x3 erosion of the reprojection mask                                       */
+/* Replaces tf.cast + tf.nn.erosion2d(SAME, all-ones 3x3) + 1 in             */
+/* scripts/main.py:270-276: out = min over the in-bounds 3x3 window of        */
+/* float(success).                                                            */
+/*  success : [B,H,W,1] bytes;  out : [B,H,W,1] float                         */
+/* ------------------------------------------------------------------------ */
+CD_API cd_status cd_erode3x3(const uint8_t *success, float *out,
+                      int B, int H, int W, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* TemporalScreening                                                          */
+/* Replaces REGISTER_OP("TemporalScreening") + TemporalScreeningOp::Compute   */
+/* (ops/temporal.cu.cc:204-287) and the TemporalScreening kernel (:57-198).  */
+/*  current1, current2, prev, prev1, prev2 : [B,H,W,3]                        */
+/*  reproj_success : [B,H,W,1] float                                          */
+/*  output, output1, output2 : [B,H,W,3];  success : [B,H,W,1] float          */
+/* Requirements: win_curr >= 1, win_prev >= 1.                                */
+/* ------------------------------------------------------------------------ */
+CD_API cd_status cd_temporal_screening(const float *current1, const float *current2,
+                                const float *prev, const float *prev1,
+                                const float *prev2, const float *reproj_success,
+                                float *output, float *output1, float *output2,
+                                float *success,
+                                int B, int H, int W, int win_curr, int win_prev,
+                                cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Erosion fused with temporal screening (one pass instead of           */
+/* scripts/main.py:270-280's erosion2d followed by temporal_screening).       */
+/* Results are identical to cd_erode3x3 followed by cd_temporal_screening;    */
+/* the eroded mask is also written (eroded : [B,H,W,1] float) because the     */
+/* aggregation step reads it (scripts/main.py:223).                           */
+/* ------------------------------------------------------------------------ */
+CD_API cd_status cd_erode_temporal_screening(const float *current1, const float *current2,
+                                      const float *prev, const float *prev1,
+                                      const float *prev2, const uint8_t *reproj_mask,
+                                      float *eroded,
+                                      float *output, float *output1, float *output2,
+                                      float *success,
+                                      int B, int H, int W, int win_curr, int win_prev,
+                                      cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CD_OPS_H */

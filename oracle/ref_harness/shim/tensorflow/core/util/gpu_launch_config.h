@@ -1,0 +1,2 @@
+// Empty stand-in for a TensorFlow header (test infrastructure).
+#pragma once
