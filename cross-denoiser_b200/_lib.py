@@ -33,7 +33,15 @@ SIGNATURES = {
     "cd_erode3x3": (_I, [_P, _P, _I, _I, _I, _P]),
     "cd_temporal_screening": (_I, [_P] * 10 + [_I] * 5 + [_P]),
     "cd_erode_temporal_screening": (_I, [_P] * 11 + [_I] * 5 + [_P]),
+    "cd_fp32_fma_probe": (_I, [_P, _I, _I, _P]),
 }
+
+# kernels each entry point launches (for the launch count of bench.py)
+KERNELS_PER_CALL = {
+    "cd_cross_regression": 3, "cd_spatial_filter": 1, "cd_spatial_filter_grad": 1, "cd_reproject": 1,
+    "cd_erode3x3": 1, "cd_temporal_screening": 1, "cd_erode_temporal_screening": 1,
+}
+LAUNCHES = {"count": 0}
 
 _lib = None
 _lock = threading.Lock()
@@ -64,8 +72,9 @@ def lib() -> ctypes.CDLL:
 
 
 def check(status: int, op: str) -> None:
-    """Raise the Python analogue of a non-zero cd_status."""
+    """Raise the Python analogue of a non-zero cd_status; count launches."""
     if status == CD_OK:
+        LAUNCHES["count"] += KERNELS_PER_CALL.get("cd_" + op, 0)
         return
     msg = lib().cd_get_last_error().decode(errors="replace")
     if status == CD_EINVAL:

@@ -1,0 +1,161 @@
+"""Per-frame step of the online denoiser on the sm_100a ops.
+
+Mirrors the op order of the reference's train_step (scripts/main.py:250-313):
+
+  1. y1, y2 = log1p(color), log1p(color2)                        (:207-212)
+  2. ols1, ols2, var1, var2 = cross_regression(y1, y2, albedo, normal)  (:261)
+  3. success, [prev out_log, ols1, ols2] = Reproject(...)         (:266)
+     with opacity and previous opacity both all-ones, as the reference passes
+  4. 3x3 erosion of float(success)                                (:270-276)
+  5. prev_out, prev_ols1, prev_ols2, success_prev = temporal_screening(...,
+     win_curr=7, win_prev=1)                                      (:280)
+  6. band, alpha = predictor(ols1, ols2, prev_out, albedo, normal) (:291)
+  7. sum1, sum2, sumw1, sumw2 = spatial_filter(ols1, ols2, albedo, normal,
+     band, win_size=11)                                           (:295)
+  8. aggregation loss with labels crossed (label1 = ols2, ...)    (:214-248, 283-286)
+  9. dL/dband through spatial_filter_grad; dL/dalpha              (:302)
+ 10. history hand-off: out_log, ols1, ols2, linearZ, normal       (:338-341)
+
+The predictor (the reference's kernel-predicting U-Net and its Adam update)
+is pluggable: ``FrameStep(predictor=...)`` takes any callable returning
+(band [B,H,W,5], alpha [B,H,W,1]) and receives the gradients through
+``on_gradients``; by default a fixed band/alpha is used.
+
+``plain`` runs the drop-in op sequence (separate erosion and screening
+kernels); ``fused`` runs erosion and screening as one kernel.  Both give
+bit-identical results.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Callable, Dict, Optional
+
+import torch
+
+from . import ops
+
+REGRESSION_WIDTH = 17      # scripts/main.py:71
+FILTER_WIDTH = 11          # scripts/main.py:72
+SPARSITY = 4               # scripts/main.py:73
+WIN_CURR, WIN_PREV = 7, 1  # scripts/main.py:280
+
+
+@dataclass
+class StepConfig:
+    regression_width: int = REGRESSION_WIDTH
+    filter_width: int = FILTER_WIDTH
+    sparsity: int = SPARSITY
+    win_curr: int = WIN_CURR
+    win_prev: int = WIN_PREV
+    fused: bool = False
+
+
+@dataclass
+class History:
+    """Per-stream state carried from one frame to the next
+    (scripts/main.py:323-341); zeros before the first frame."""
+    out_log: torch.Tensor
+    ols1: torch.Tensor
+    ols2: torch.Tensor
+    linearZ: torch.Tensor
+    normal: torch.Tensor
+
+    @staticmethod
+    def zeros(B, H, W, device) -> "History":
+        z = lambda: torch.zeros((B, H, W, 3), dtype=torch.float32, device=device)
+        return History(z(), z(), z(), z(), z())
+
+
+def aggregation_forward_backward(sum1, sumw1, sum2, sumw2, alpha, success, success_prev, prev_out,
+                                 opacity, label1, label2, prev_label1, prev_label2):
+    """aggregation_loss (scripts/main.py:214-248) and its gradient with
+    respect to (sum1, sumw1, sum2, sumw2, alpha), in closed form.
+
+    Returns (out, out_linear, loss, avg_loss, g_sum1, g_sumw1, g_sum2, g_sumw2, g_alpha).
+    """
+    e = 1e-4
+    d1 = sumw1 + e
+    d2 = sumw2 + e
+    o1s = sum1 / d1
+    o2s = sum2 / d2
+    out = (sum1 + sum2) / (sumw1 + sumw2 + e)
+    op = torch.where(opacity > 0, 1.0, 0.0)
+    s = success * success_prev
+    a = s * alpha + (1 - s)
+    out = (a * out + (1 - a) * prev_out) * op
+    o1 = a * o1s + (1 - a) * prev_out
+    o2 = a * o2s + (1 - a) * prev_out
+    n1, n2 = label1 * label1 + 1e-2, label2 * label2 + 1e-2
+    p1, p2 = prev_label1 * prev_label1 + 1e-2, prev_label2 * prev_label2 + 1e-2
+    spatial = ((o1 - label1) ** 2 / n1 + (o2 - label2) ** 2 / n2) * 0.5
+    temporal = ((o1 - prev_label1) ** 2 / p1 + (o2 - prev_label2) ** 2 / p2) * 0.5
+    loss = (spatial + temporal) * 0.5 * op
+    avg = loss.mean()
+    c = 0.5 * 0.5 * op / loss.numel()
+    g_o1 = c * (2 * (o1 - label1) / n1 + 2 * (o1 - prev_label1) / p1)
+    g_o2 = c * (2 * (o2 - label2) / n2 + 2 * (o2 - prev_label2) / p2)
+    g_sum1 = g_o1 * a / d1
+    g_sum2 = g_o2 * a / d2
+    g_sumw1 = -(g_o1 * a * sum1).sum(-1, keepdim=True) / (d1 * d1)
+    g_sumw2 = -(g_o2 * a * sum2).sum(-1, keepdim=True) / (d2 * d2)
+    g_alpha = (s * (g_o1 * (o1s - prev_out) + g_o2 * (o2s - prev_out))).sum(-1, keepdim=True)
+    return (out, torch.clamp(torch.expm1(out), min=0.0), loss, avg,
+            g_sum1, g_sumw1, g_sum2, g_sumw2, g_alpha)
+
+
+class FrameStep:
+    """One stream's per-frame denoise + loss + gradient step."""
+
+    def __init__(self, cfg: StepConfig = StepConfig(), predictor: Optional[Callable] = None,
+                 on_gradients: Optional[Callable] = None):
+        self.cfg = cfg
+        self.predictor = predictor
+        self.on_gradients = on_gradients
+        self.history: Optional[History] = None
+        self.fixed_band: Optional[torch.Tensor] = None
+        self.fixed_alpha: Optional[torch.Tensor] = None
+
+    def reset(self):
+        self.history = None
+
+    def set_fixed_prediction(self, band: torch.Tensor, alpha: torch.Tensor):
+        self.fixed_band, self.fixed_alpha = band, alpha
+
+    def __call__(self, f: Dict[str, torch.Tensor]) -> Dict[str, torch.Tensor]:
+        cfg = self.cfg
+        color = f["color"]
+        B, H, W, _ = color.shape
+        if self.history is None:
+            self.history = History.zeros(B, H, W, color.device)
+        h = self.history
+        y1 = torch.log1p(color)
+        y2 = torch.log1p(f["color2"])
+        albedo, normal = f["albedo"], f["normal"]
+        ols1, ols2, _, _ = ops.cross_regression(y1, y2, albedo, normal, win_size=cfg.regression_width,
+                                                sparsity=cfg.sparsity)
+        ones1 = torch.ones((B, H, W, 1), dtype=torch.float32, device=color.device)
+        success, rep = ops.Reproject(f["mvec"], [h.out_log, h.ols1, h.ols2], f["linearZ"], h.linearZ, normal,
+                                     h.normal, f["pnFwidth"], ones1, ones1)
+        if cfg.fused:
+            prev_out, prev_ols1, prev_ols2, success_prev, success_f = ops.erode_temporal_screening(
+                ols1, ols2, rep[0], rep[1], rep[2], success, cfg.win_curr, cfg.win_prev)
+        else:
+            success_f = ops.erode3x3(success)
+            prev_out, prev_ols1, prev_ols2, success_prev = ops.temporal_screening(
+                ols1, ols2, rep[0], rep[1], rep[2], success_f, win_curr=cfg.win_curr, win_prev=cfg.win_prev)
+        if self.predictor is not None:
+            band, alpha = self.predictor(ols1, ols2, prev_out, albedo, normal)
+        else:
+            band, alpha = self.fixed_band, self.fixed_alpha
+        sum1, sum2, sumw1, sumw2 = ops.spatial_filter(ols1, ols2, albedo, normal, band.detach(),
+                                                      win_size=cfg.filter_width)
+        (out_log, out, loss, avg, g1, gw1, g2, gw2, g_alpha) = aggregation_forward_backward(
+            sum1, sumw1, sum2, sumw2, alpha.detach(), success_f, success_prev, prev_out, f["opacity"],
+            ols2, ols1, prev_ols2, prev_ols1)
+        g_band = ops.spatial_filter_grad(g1, g2, gw1, gw2, ols1, ols2, albedo, normal, band.detach(),
+                                         win_size=cfg.filter_width)
+        if self.on_gradients is not None:
+            self.on_gradients(g_band, g_alpha)
+        self.history = History(out_log, ols1, ols2, f["linearZ"], normal)
+        return {"out": out, "out_log": out_log, "loss": loss, "avg_loss": avg, "ols1": ols1, "ols2": ols2,
+                "g_band": g_band, "g_alpha": g_alpha, "success": success}

@@ -186,6 +186,14 @@ CD_API cd_status cd_erode_temporal_screening(const float *current1, const float 
                                       int B, int H, int W, int win_curr, int win_prev,
                                       cudaStream_t stream);
 
+/* ------------------------------------------------------------------------ */
+/* FP32 FMA throughput probe (no counterpart in the reference): `blocks`     */
+/* CTAs of 256 threads each issue iters x 128 fused multiply-adds and store  */
+/* one float per thread to out[blocks * 256].  Timed by the caller; gives    */
+/* the measured FP32 peak that bounds the filter and regression kernels.     */
+/* ------------------------------------------------------------------------ */
+CD_API cd_status cd_fp32_fma_probe(float *out, int blocks, int iters, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

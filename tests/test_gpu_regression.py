@@ -1,0 +1,95 @@
+"""CrossRegression on the GPU against the oracle, the golden reference
+outputs and the live reference kernel, within rtol 1e-4 (absolute floor 1e-5
+for outputs that the reference clamps at zero); variance outputs; batches;
+known answers and argument errors."""
+import numpy as np
+import pytest
+import torch
+
+from gpu_util import N, T, frames, needs_reference
+from helpers import assert_close, golden, golden_names
+from oracle import oracle as orc
+from oracle import reference as ref
+
+pytestmark = pytest.mark.gpu
+ATOL = 1e-5
+
+
+def run(cd, y1, y2, alb, nrm, win, sp, rs=1):
+    o = cd.ops.cross_regression(T(y1), T(y2), T(alb), T(nrm), win_size=win, sparsity=sp, recon_scale=rs)
+    torch.cuda.synchronize()
+    return [N(x) for x in o]
+
+
+def inputs(cd, H, W, seed):
+    _, f = frames(cd, H, W, seed=seed)
+    return np.log1p(f["color"]), np.log1p(f["color2"]), f["albedo"], f["normal"]
+
+
+@pytest.mark.parametrize("name", golden_names("regression_"))
+def test_golden(cd, cuda, name):
+    g = golden(name)
+    o = run(cd, g["in_imga"], g["in_imgb"], g["in_albedo"], g["in_normal"], int(g["attr_win_size"]),
+            int(g["attr_sparsity"]), int(g["attr_recon_scale"]))
+    for x, key in zip(o, ("ref_outa", "ref_outb", "ref_vara", "ref_varb")):
+        assert_close(x, g[key], f"{name} {key}", atol=ATOL)
+
+
+@pytest.mark.parametrize("win,sp,rs", [(11, 4, 1), (15, 4, 1), (17, 4, 1), (19, 4, 1), (15, 4, 2), (17, 4, 4),
+                                       (9, 2, 1), (7, 1, 1), (5, 8, 8)])
+def test_vs_oracle(cd, cuda, win, sp, rs):
+    y1, y2, alb, nrm = inputs(cd, 128, 160, seed=win * 10 + sp)
+    o = run(cd, y1, y2, alb, nrm, win, sp, rs)
+    r = orc.cross_regression(y1, y2, alb, nrm, win, sp, rs)
+    for i, nm in enumerate(("outa", "outb", "vara", "varb")):
+        assert_close(o[i], r[i], nm, atol=ATOL)
+
+
+def test_batches_are_independent(cd, cuda):
+    a = inputs(cd, 64, 96, seed=1)
+    b = inputs(cd, 64, 96, seed=2)
+    both = [np.concatenate([x, y]) for x, y in zip(a, b)]
+    o = run(cd, *both, 15, 4)
+    oa = run(cd, *a, 15, 4)
+    ob = run(cd, *b, 15, 4)
+    for i in range(4):
+        np.testing.assert_array_equal(o[i][0:1], oa[i])
+        np.testing.assert_array_equal(o[i][1:2], ob[i])
+
+
+def test_production_size(cd, cuda):
+    y1, y2, alb, nrm = inputs(cd, 1080, 1920, seed=9)
+    o = run(cd, y1, y2, alb, nrm, 15, 4)
+    r = orc.cross_regression(y1, y2, alb, nrm, 15, 4, 1)
+    for i, nm in enumerate(("outa", "outb", "vara", "varb")):
+        assert_close(o[i], r[i], nm + " 1080p", atol=ATOL)
+
+
+@needs_reference
+@pytest.mark.parametrize("win", [11, 15, 17, 19])
+def test_vs_reference_kernel(cd, cuda, win):
+    y1, y2, alb, nrm = inputs(cd, 256, 320, seed=win)
+    o = run(cd, y1, y2, alb, nrm, win, 4)
+    r = ref.cross_regression(T(y1), T(y2), T(alb), T(nrm), win, 4, 1)
+    torch.cuda.synchronize()
+    for i, nm in enumerate(("outa", "outb", "vara", "varb")):
+        assert_close(o[i], N(r[i]), nm + " vs reference", atol=ATOL)
+
+
+def test_constant_target(cd, cuda):
+    H, W = 64, 64
+    c = np.full((1, H, W, 3), 0.7, np.float32)
+    rng = np.random.default_rng(0)
+    alb = rng.uniform(0.1, 0.9, (1, H, W, 3)).astype(np.float32)
+    o = run(cd, c, c, alb, alb, 15, 4)
+    assert_close(o[0], np.full_like(o[0], 0.7), "constant", rtol=1e-4)
+
+
+def test_argument_errors(cd, cuda):
+    x = torch.zeros((1, 64, 64, 3), device=cuda)
+    with pytest.raises(ValueError, match="recon_scale"):
+        cd.ops.cross_regression(x, x, x, x, win_size=15, sparsity=2, recon_scale=4)
+    with pytest.raises(ValueError, match="divisible"):
+        cd.ops.cross_regression(x[:, :62], x[:, :62], x[:, :62], x[:, :62], win_size=15, sparsity=4)
+    with pytest.raises(ValueError):
+        cd.ops.cross_regression(x[:, :8, :8], x[:, :8, :8], x[:, :8, :8], x[:, :8, :8], win_size=17, sparsity=4)
