@@ -212,8 +212,9 @@ def max_over_ranks(x, world):
 # ---------------------------------------------------------------------------
 def op_timer(stepper, stream):
     """Wrap the ops the step calls so every call is bracketed by CUDA events."""
-    names = ("cross_regression", "Reproject", "erode3x3", "temporal_screening", "erode_temporal_screening",
-             "spatial_filter", "spatial_filter_grad")
+    names = ("prepare_input", "cross_regression", "Reproject", "erode3x3", "temporal_screening",
+             "erode_temporal_screening", "spatial_filter", "aggregation_loss", "spatial_filter_grad",
+             "filter_aggregate")
     store = {n: [] for n in names}
     orig = {n: getattr(ops, n) for n in names}
 
@@ -401,7 +402,8 @@ def run_mine(a, rank, world, device):
     px = H * W
     flop = {"cross_regression": regression_flop(H, W, a.win, 4),
             "spatial_filter": px * a.filter_win ** 2 * FLOP["filter_tap"],
-            "spatial_filter_grad": px * a.filter_win ** 2 * FLOP["grad_tap"]}
+            "spatial_filter_grad": px * a.filter_win ** 2 * FLOP["grad_tap"],
+            "filter_aggregate": px * a.filter_win ** 2 * FLOP["grad_tap"]}
     if dom in flop:
         ach = flop[dom] / (per_op[dom] * 1e-3) / 1e12
         res["roofline"] = {"kernel": dom, "bound": "fp32", "achieved": round(ach, 2), "peak": round(peak, 2),

@@ -33,6 +33,11 @@ SIGNATURES = {
     "cd_erode3x3": (_I, [_P, _P, _I, _I, _I, _P]),
     "cd_temporal_screening": (_I, [_P] * 10 + [_I] * 5 + [_P]),
     "cd_erode_temporal_screening": (_I, [_P] * 11 + [_I] * 5 + [_P]),
+    "cd_prepare_input": (_I, [_P, _P, _P, _P, _S, _P]),
+    "cd_aggregation_workspace_size": (_S, [_I, _I, _I]),
+    "cd_aggregation_loss": (_I, [_P] * 22 + [_I] * 3 + [_P, _S, _P]),
+    "cd_filter_aggregate_workspace_size": (_S, [_I, _I, _I]),
+    "cd_filter_aggregate": (_I, [_P] * 17 + [_I] * 4 + [_P, _S, _P]),
     "cd_fp32_fma_probe": (_I, [_P, _I, _I, _P]),
 }
 
@@ -40,6 +45,7 @@ SIGNATURES = {
 KERNELS_PER_CALL = {
     "cd_cross_regression": 3, "cd_spatial_filter": 1, "cd_spatial_filter_grad": 1, "cd_reproject": 1,
     "cd_erode3x3": 1, "cd_temporal_screening": 1, "cd_erode_temporal_screening": 1,
+    "cd_prepare_input": 1, "cd_aggregation_loss": 2, "cd_filter_aggregate": 2,
 }
 LAUNCHES = {"count": 0}
 

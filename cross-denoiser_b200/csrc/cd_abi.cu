@@ -36,11 +36,6 @@ bool dims_ok(int B, int H, int W) { return B >= 1 && B <= 32767 && H >= 1 && W >
 // Shared-memory footprints of the tiled kernels (must agree with the kernel
 // translation units; checked here so that an oversized window is an argument
 // error rather than a launch failure).
-size_t regression_tile_bytes(int hw, int sp)
-{
-    const int pw = 7 * sp + 2 * hw + 1, ph = 2 * hw + 1;
-    return (size_t)16 * ph * (pw | 1) * sizeof(float);
-}
 size_t filter_tile_bytes(int hw) { return (size_t)12 * (32 + 2 * hw) * (8 + 2 * hw) * 4 + 1024; }
 size_t temporal_tile_bytes(int hc)
 {
@@ -59,7 +54,8 @@ const char *cd_get_last_error(void) { return g_err; }
 size_t cd_cross_regression_workspace_size(int B, int H, int W, int sparsity)
 {
     if (!dims_ok(B, H, W) || sparsity < 1) return 0;
-    return (size_t)2 * B * (H / sparsity) * (W / sparsity) * 18 * sizeof(float);
+    // coefficients of both buffers, then sqrt(var) of both images
+    return ((size_t)2 * B * (H / sparsity) * (W / sparsity) * 18 + (size_t)2 * B * H * W) * sizeof(float);
 }
 
 cd_status cd_cross_regression(const float *imga, const float *imgb, const float *albedo,
@@ -84,19 +80,25 @@ cd_status cd_cross_regression(const float *imga, const float *imgb, const float 
     const int hw = win_size / 2;
     if (hw >= H || hw >= W)
         return fail(CD_EINVAL, "cross_regression: window radius %d must be smaller than the image (%dx%d)", hw, H, W);
-    if (regression_tile_bytes(hw, sparsity) > kSmemLimit)
-        return fail(CD_EINVAL, "cross_regression: win_size %d with sparsity %d exceeds the shared-memory tile", win_size, sparsity);
+    if (cd::regression_smem_bytes(win_size, sparsity) > kSmemLimit ||
+        cd::recon_smem_bytes(win_size, sparsity, recon_scale) > kSmemLimit)
+        return fail(CD_EINVAL, "cross_regression: win_size %d with sparsity %d / recon_scale %d exceeds the "
+                               "shared-memory tiles", win_size, sparsity, recon_scale);
     const size_t need = cd_cross_regression_workspace_size(B, H, W, sparsity);
     if (workspace_bytes < need || (need > 0 && !workspace))
         return fail(CD_ENOMEM, "cross_regression: workspace of %zu bytes needed, %zu given", need, workspace_bytes);
 
     float *beta = static_cast<float *>(workspace);
+    float *sda = beta + (size_t)2 * B * (H / sparsity) * (W / sparsity) * 18;
+    float *sdb = sda + (size_t)B * H * W;
     cd_status s;
-    if ((s = cuda_status(cd::launch_variance(imga, imgb, vara, varb, B, H, W, stream), "variance")) != CD_OK) return s;
-    if ((s = cuda_status(cd::launch_regression(imga, imgb, albedo, normal, vara, varb, beta, B, H, W,
-                                               win_size, sparsity, stream), "regression")) != CD_OK) return s;
-    return cuda_status(cd::launch_recon(imga, imgb, albedo, normal, vara, varb, beta, outa, outb, B, H,
-                                        W, win_size, sparsity, recon_scale, stream), "recon");
+    if ((s = cuda_status(cd::launch_variance(imga, imgb, vara, varb, sda, sdb, B, H, W, stream), "variance")) != CD_OK)
+        return s;
+    if ((s = cuda_status(cd::launch_regression(imga, imgb, albedo, normal, vara, varb, sda, sdb, beta, B, H, W,
+                                               win_size, sparsity, stream), "regression")) != CD_OK)
+        return s;
+    return cuda_status(cd::launch_recon(imga, imgb, albedo, normal, vara, varb, sda, sdb, beta, outa, outb, B,
+                                        H, W, win_size, sparsity, recon_scale, stream), "recon");
 }
 
 cd_status cd_spatial_filter(const float *imga, const float *imgb, const float *albedo,
@@ -221,6 +223,78 @@ cd_status cd_erode_temporal_screening(const float *current1, const float *curren
                                            eroded, output, output1, output2, success, B, H, W, win_curr,
                                            win_prev, stream),
                        "erode_temporal_screening");
+}
+
+cd_status cd_prepare_input(const float *color, const float *color2, float *y1, float *y2, size_t n,
+                           cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!color || !color2 || !y1 || !y2) return fail(CD_EINVAL, "prepare_input: null tensor pointer");
+    if (n == 0) return CD_OK;
+    return cuda_status(cd::launch_log1p(color, color2, y1, y2, n, stream), "prepare_input");
+}
+
+size_t cd_aggregation_workspace_size(int B, int H, int W)
+{
+    if (!dims_ok(B, H, W)) return 0;
+    return cd::aggregation_partials(B, H, W) * sizeof(float);
+}
+
+cd_status cd_aggregation_loss(const float *sum1, const float *sumw1, const float *sum2, const float *sumw2,
+                              const float *alpha, const float *success, const float *success_prev,
+                              const float *prev_out, const float *opacity, const float *label1,
+                              const float *label2, const float *prev_label1, const float *prev_label2,
+                              float *out_log, float *out, float *loss, float *avg_loss, float *grad_sum1,
+                              float *grad_sumw1, float *grad_sum2, float *grad_sumw2, float *grad_alpha,
+                              int B, int H, int W, void *workspace, size_t workspace_bytes,
+                              cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!sum1 || !sumw1 || !sum2 || !sumw2 || !alpha || !success || !success_prev || !prev_out || !opacity ||
+        !label1 || !label2 || !prev_label1 || !prev_label2 || !out_log || !out || !avg_loss || !grad_sum1 ||
+        !grad_sumw1 || !grad_sum2 || !grad_sumw2 || !grad_alpha)
+        return fail(CD_EINVAL, "aggregation_loss: null tensor pointer");
+    if (!dims_ok(B, H, W)) return fail(CD_EINVAL, "aggregation_loss: bad shape B=%d H=%d W=%d", B, H, W);
+    const size_t need = cd_aggregation_workspace_size(B, H, W);
+    if (workspace_bytes < need || !workspace)
+        return fail(CD_ENOMEM, "aggregation_loss: workspace of %zu bytes needed, %zu given", need, workspace_bytes);
+    cd::AggArgs A{sum1, sumw1, sum2, sumw2, alpha, success, success_prev, prev_out, opacity, label1, label2,
+                  prev_label1, prev_label2, out_log, out, loss, grad_sum1, grad_sumw1, grad_sum2, grad_sumw2,
+                  grad_alpha};
+    return cuda_status(cd::launch_aggregation(A, static_cast<float *>(workspace), avg_loss, B, H, W, stream),
+                       "aggregation_loss");
+}
+
+size_t cd_filter_aggregate_workspace_size(int B, int H, int W) { return cd_aggregation_workspace_size(B, H, W); }
+
+cd_status cd_filter_aggregate(const float *ols1, const float *ols2, const float *albedo, const float *normal,
+                              const float *band, const float *alpha, const float *success,
+                              const float *success_prev, const float *prev_out, const float *opacity,
+                              const float *prev_ols1, const float *prev_ols2, float *out_log, float *out,
+                              float *avg_loss, float *grad_band, float *grad_alpha, int B, int H, int W,
+                              int win_size, void *workspace, size_t workspace_bytes, cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!ols1 || !ols2 || !albedo || !normal || !band || !alpha || !success || !success_prev || !prev_out ||
+        !opacity || !prev_ols1 || !prev_ols2 || !out_log || !out || !avg_loss || !grad_band || !grad_alpha)
+        return fail(CD_EINVAL, "filter_aggregate: null tensor pointer");
+    if (!dims_ok(B, H, W)) return fail(CD_EINVAL, "filter_aggregate: bad shape B=%d H=%d W=%d", B, H, W);
+    if (win_size < 1) return fail(CD_EINVAL, "filter_aggregate: win_size must be >= 1");
+    const int hw = win_size / 2;
+    if (hw >= H || hw >= W)
+        return fail(CD_EINVAL, "filter_aggregate: window radius %d must be smaller than the image (%dx%d)", hw, H, W);
+    if (cd::filter_aggregate_smem(win_size) > kSmemLimit)
+        return fail(CD_EINVAL, "filter_aggregate: win_size %d exceeds the shared-memory tile", win_size);
+    const size_t need = cd_filter_aggregate_workspace_size(B, H, W);
+    if (workspace_bytes < need || !workspace)
+        return fail(CD_ENOMEM, "filter_aggregate: workspace of %zu bytes needed, %zu given", need, workspace_bytes);
+    cd::AggArgs A{nullptr, nullptr, nullptr, nullptr, alpha, success, success_prev, prev_out, opacity, nullptr,
+                  nullptr, prev_ols2, prev_ols1, out_log, out, nullptr, nullptr, nullptr, nullptr, nullptr,
+                  grad_alpha};
+    return cuda_status(cd::launch_filter_aggregate(ols1, ols2, albedo, normal, band, A, grad_band,
+                                                   static_cast<float *>(workspace), avg_loss, B, H, W, win_size,
+                                                   stream),
+                       "filter_aggregate");
 }
 
 }  // extern "C"

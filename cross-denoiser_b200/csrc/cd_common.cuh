@@ -39,15 +39,18 @@ CD_DEV float norm2(float x, float y, float z) { return x * x + y * y + z * z; }
 namespace cd {
 
 cudaError_t launch_variance(const float *imga, const float *imgb, float *vara, float *varb,
-                            int B, int H, int W, cudaStream_t st);
+                            float *sda, float *sdb, int B, int H, int W, cudaStream_t st);
 cudaError_t launch_regression(const float *imga, const float *imgb, const float *albedo,
                               const float *normal, const float *vara, const float *varb,
-                              float *beta, int B, int H, int W, int win, int sparsity,
-                              cudaStream_t st);
+                              const float *sda, const float *sdb, float *beta, int B, int H, int W,
+                              int win, int sparsity, cudaStream_t st);
 cudaError_t launch_recon(const float *imga, const float *imgb, const float *albedo,
                          const float *normal, const float *vara, const float *varb,
-                         const float *beta, float *outa, float *outb, int B, int H, int W,
-                         int win, int sparsity, int recon_scale, cudaStream_t st);
+                         const float *sda, const float *sdb, const float *beta, float *outa,
+                         float *outb, int B, int H, int W, int win, int sparsity, int recon_scale,
+                         cudaStream_t st);
+size_t regression_smem_bytes(int win, int sparsity);
+size_t recon_smem_bytes(int win, int sparsity, int recon_scale);
 
 cudaError_t launch_spatial_filter(const float *imga, const float *imgb, const float *albedo,
                                   const float *normal, const float *band, float *acca,
@@ -76,5 +79,19 @@ cudaError_t launch_temporal(const float *c1, const float *c2, const float *prev,
                             const uint8_t *raw_mask, float *eroded, float *out, float *out1,
                             float *out2, float *succ, int B, int H, int W, int win_curr,
                             int win_prev, cudaStream_t st);
+
+struct AggArgs {
+    const float *s1, *w1, *s2, *w2, *alpha, *succ, *succ_prev, *prev, *opac, *l1, *l2, *pl1, *pl2;
+    float *out_log, *out, *loss, *g_s1, *g_w1, *g_s2, *g_w2, *g_alpha;
+};
+size_t aggregation_partials(int B, int H, int W);
+cudaError_t launch_log1p(const float *a, const float *b, float *ya, float *yb, size_t n, cudaStream_t st);
+cudaError_t launch_aggregation(const AggArgs &A, float *partial, float *avg, int B, int H, int W,
+                               cudaStream_t st);
+size_t filter_aggregate_smem(int win);
+cudaError_t launch_filter_aggregate(const float *imga, const float *imgb, const float *albedo,
+                                    const float *normal, const float *band, const AggArgs &A,
+                                    float *gband, float *partial, float *avg, int B, int H, int W,
+                                    int win, cudaStream_t st);
 
 }  // namespace cd

@@ -21,13 +21,16 @@ constexpr int kBeta = kP * 3;    // floats per centre and buffer
 
 // ---------------------------------------------------------------------------
 // Variance: var = |mean of the in-bounds 3x3 neighbours minus the centre -
-// centre|^2 summed over channels (ops/regression.cu.cc:244-276).
-// blockIdx.z = 2 * batch + buffer.
+// centre|^2 summed over channels (ops/regression.cu.cc:244-276).  Also
+// writes sqrt(var) to a workspace plane: the regression and reconstruction
+// read the standard deviation of every tap.  blockIdx.z = 2 * batch + buffer.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) variance_kernel(const float *__restrict__ imga,
                                                        const float *__restrict__ imgb,
                                                        float *__restrict__ vara,
-                                                       float *__restrict__ varb, int H, int W)
+                                                       float *__restrict__ varb,
+                                                       float *__restrict__ sda,
+                                                       float *__restrict__ sdb, int H, int W)
 {
     const int cx = blockIdx.x * blockDim.x + threadIdx.x;
     const int cy = blockIdx.y * blockDim.y + threadIdx.y;
@@ -36,6 +39,7 @@ __global__ void __launch_bounds__(256) variance_kernel(const float *__restrict__
     const size_t base = (size_t)(blockIdx.z >> 1) * H * W;
     const float *img = (buf ? imgb : imga) + 3 * base;
     float *var = (buf ? varb : vara) + base;
+    float *sd = (buf ? sdb : sda) + base;
     const int sx = max(0, cx - 1), ex = min(W - 1, cx + 1);
     const int sy = max(0, cy - 1), ey = min(H - 1, cy + 1);
     float ax = 0.f, ay = 0.f, az = 0.f;
@@ -51,7 +55,9 @@ __global__ void __launch_bounds__(256) variance_kernel(const float *__restrict__
         }
     const float fn = (float)n;
     const float3 c = ld3(img, (size_t)cy * W + cx);
-    var[(size_t)cy * W + cx] = norm2(ax / fn - c.x, ay / fn - c.y, az / fn - c.z);
+    const float v = norm2(ax / fn - c.x, ay / fn - c.y, az / fn - c.z);
+    var[(size_t)cy * W + cx] = v;
+    sd[(size_t)cy * W + cx] = sqrtf(v);
 }
 
 // ---------------------------------------------------------------------------
@@ -79,6 +85,11 @@ CD_DEV void normal_zero(Normal &n)
     }
 }
 
+// |v|^2 as the reference's compiled norm2 rounds it: fma(z, z, fma(x, x, y*y))
+// (the contraction the reference kernels were observed to use for
+// x*x + y*y + z*z, see reproject.cu).
+CD_DEV float sqnorm(float x, float y, float z) { return fmaf(z, z, fmaf(x, x, y * y)); }
+
 // One window tap of one buffer: features f (centre fc), target y, variance
 // and standard deviation (v, sd), shared albedo / normal differences.
 // Follows ops/regression.cu.cc:418-445: delta = [1, (f_t-f_c)/(sd_c+sd_t+1e-2),
@@ -88,7 +99,7 @@ CD_DEV void normal_tap(Normal &n, float3 ft, float3 fc, float3 y, float vt, floa
 {
     const float df[3] = {ft.x - fc.x, ft.y - fc.y, ft.z - fc.z};
     const float den = (sdc + sdt) + 1e-2f;
-    const float dist = norm2(df[0], df[1], df[2]) / ((vc + vt) + 1e-4f);
+    const float dist = sqnorm(df[0], df[1], df[2]) / ((vc + vt) + 1e-4f);
     const float w = __expf(-dist) + 1e-7f;
     const float wn0 = w * dn[0], wn1 = w * dn[1], wn2 = w * dn[2];
     n.a00 += w;
@@ -123,49 +134,6 @@ CD_DEV void normal_tap(Normal &n, float3 ft, float3 fc, float3 y, float vt, floa
         n.x3[k] = fmaf(wn0, yv[k], n.x3[k]);
         n.x4[k] = fmaf(wn1, yv[k], n.x4[k]);
         n.x5[k] = fmaf(wn2, yv[k], n.x5[k]);
-    }
-}
-
-// Sum the accumulators over the `width` lanes of a group (xor butterfly, so
-// every lane of the group ends with the same total).
-CD_DEV float group_sum(float v, int width)
-{
-    for (int m = 1; m < width; m <<= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
-    return v;
-}
-
-CD_DEV void normal_reduce(Normal &n, int width)
-{
-    if (width == 1) return;
-    n.a00 = group_sum(n.a00, width);
-    n.a03 = group_sum(n.a03, width);
-    n.a04 = group_sum(n.a04, width);
-    n.a05 = group_sum(n.a05, width);
-    n.a33 = group_sum(n.a33, width);
-    n.a34 = group_sum(n.a34, width);
-    n.a35 = group_sum(n.a35, width);
-    n.a44 = group_sum(n.a44, width);
-    n.a45 = group_sum(n.a45, width);
-    n.a55 = group_sum(n.a55, width);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        n.a01[k] = group_sum(n.a01[k], width);
-        n.a02[k] = group_sum(n.a02[k], width);
-        n.a11[k] = group_sum(n.a11[k], width);
-        n.a12[k] = group_sum(n.a12[k], width);
-        n.a13[k] = group_sum(n.a13[k], width);
-        n.a14[k] = group_sum(n.a14[k], width);
-        n.a15[k] = group_sum(n.a15[k], width);
-        n.a22[k] = group_sum(n.a22[k], width);
-        n.a23[k] = group_sum(n.a23[k], width);
-        n.a24[k] = group_sum(n.a24[k], width);
-        n.a25[k] = group_sum(n.a25[k], width);
-        n.x0[k] = group_sum(n.x0[k], width);
-        n.x1[k] = group_sum(n.x1[k], width);
-        n.x2[k] = group_sum(n.x2[k], width);
-        n.x3[k] = group_sum(n.x3[k], width);
-        n.x4[k] = group_sum(n.x4[k], width);
-        n.x5[k] = group_sum(n.x5[k], width);
     }
 }
 
@@ -223,163 +191,67 @@ CD_DEV void solve_channel(const Normal &n, int k, float *beta)
 
 // ---------------------------------------------------------------------------
 // Regression kernel.
-// A CTA owns a tile of kTCX x kTCY centres.  Its window footprint (centres
-// plus the window radius on every side, reflect-101 at the image border) is
-// staged once in shared memory as 16 SoA planes: imga.xyz, imgb.xyz,
-// albedo.xyz, normal.xyz, varA, varB, sdA, sdB.  Four lanes work on one
-// centre and split the window rows (lane j takes rows j, j+4, ...); each lane
-// accumulates both buffers' normal equations in registers, the four partial
-// sums are combined with warp shuffles, and the six channel systems
-// (3 channels x 2 buffers) are solved by the four lanes in registers.
-// With centres 4 px apart and an odd plane pitch the 32 lanes of a warp read
-// 32 distinct banks.
+// A CTA owns 32 consecutive centres of one centre row; warp 0 solves buffer A
+// and warp 1 buffer B, one thread per (centre, buffer), so every centre sums
+// its window taps in the reference's order (rows, then columns) with the
+// reference's per-tap arithmetic.  The window rows stream through two
+// shared-memory row slots (cp.async, double buffered): row r + 1 is copied
+// while row r is consumed.  A row slot stores, per pixel of the row segment
+// the 32 windows cover, four float4 groups
+//   g0 = (imga.xyz, varA)  g1 = (imgb.xyz, varB)
+//   g2 = (albedo.xyz, sdA) g3 = (normal.xyz, sdB)
+// and positions are de-interleaved by the sparsity (position p at
+// (p % s) * q + p / s), so the 32 lanes, whose centres are s pixels apart,
+// read 32 consecutive float4s: four conflict-free LDS.128 per tap.
 // ---------------------------------------------------------------------------
-constexpr int kTCX = 8;       // centres per CTA along x (one warp row)
-constexpr int kLanes = 4;     // lanes per centre
-constexpr int kPlanes = 16;
+constexpr int kCX = 32;       // centres per CTA
+constexpr int kThreads = 64;
 
-struct TileGeom {
-    int tcy;        // centres per CTA along y (= warps per CTA)
-    int pw, ph;     // footprint in pixels
-    int pitch;      // plane row pitch (odd)
-    size_t smem;    // bytes
+struct RowGeom {
+    int rw;      // row segment width in pixels
+    int q;       // de-interleave stride
+    int npos;    // positions per group (q * sparsity)
 };
 
-__host__ __device__ inline TileGeom tile_geom(int hw, int sp, int tcy)
+__host__ __device__ inline RowGeom row_geom(int hw, int sp)
 {
-    TileGeom g;
-    g.tcy = tcy;
-    g.pw = (kTCX - 1) * sp + 2 * hw + 1;
-    g.ph = (tcy - 1) * sp + 2 * hw + 1;
-    g.pitch = g.pw | 1;
-    g.smem = (size_t)kPlanes * g.ph * g.pitch * sizeof(float);
+    RowGeom g;
+    g.rw = (kCX - 1) * sp + 2 * hw + 1;
+    g.q = (g.rw + sp - 1) / sp;
+    g.npos = g.q * sp;
     return g;
 }
 
-__global__ void __launch_bounds__(256) regression_kernel(
-    const float *__restrict__ imga, const float *__restrict__ imgb,
-    const float *__restrict__ albedo, const float *__restrict__ normal,
-    const float *__restrict__ vara, const float *__restrict__ varb, float *__restrict__ beta,
-    int H, int W, int hw, int sp, int tcy)
+// two row slots of 4 float4 groups, then the per-position tables
+__host__ __device__ inline size_t regression_smem(int hw, int sp)
 {
-    extern __shared__ float smem[];
-    const TileGeom g = tile_geom(hw, sp, tcy);
-    const int plane = g.ph * g.pitch;
-    const int Ws = W / sp, Hs = H / sp;
-    const int b = blockIdx.z;
-    const size_t px = (size_t)H * W;
-    imga += 3 * px * b;
-    imgb += 3 * px * b;
-    albedo += 3 * px * b;
-    normal += 3 * px * b;
-    vara += px * b;
-    varb += px * b;
-
-    const int i0 = blockIdx.x * kTCX, j0 = blockIdx.y * tcy;
-    const int x0 = i0 * sp - hw, y0 = j0 * sp - hw;
-
-    // Stage the footprint.  Pixels past the reflect range belong to no valid
-    // centre's window; they are clamped only to keep the loads in bounds.
-    for (int t = threadIdx.x; t < g.pw * g.ph; t += blockDim.x) {
-        const int ty = t / g.pw, tx = t - ty * g.pw;
-        const int gx = min(max(mirror(x0 + tx, W), 0), W - 1);
-        const int gy = min(max(mirror(y0 + ty, H), 0), H - 1);
-        const size_t q = (size_t)gy * W + gx;
-        const int o = ty * g.pitch + tx;
-        const float3 a = ld3(imga, q), bb = ld3(imgb, q), al = ld3(albedo, q), nr = ld3(normal, q);
-        const float va = __ldg(vara + q), vb = __ldg(varb + q);
-        smem[0 * plane + o] = a.x;
-        smem[1 * plane + o] = a.y;
-        smem[2 * plane + o] = a.z;
-        smem[3 * plane + o] = bb.x;
-        smem[4 * plane + o] = bb.y;
-        smem[5 * plane + o] = bb.z;
-        smem[6 * plane + o] = al.x;
-        smem[7 * plane + o] = al.y;
-        smem[8 * plane + o] = al.z;
-        smem[9 * plane + o] = nr.x;
-        smem[10 * plane + o] = nr.y;
-        smem[11 * plane + o] = nr.z;
-        smem[12 * plane + o] = va;
-        smem[13 * plane + o] = vb;
-        smem[14 * plane + o] = sqrtf(va);
-        smem[15 * plane + o] = sqrtf(vb);
-    }
-    __syncthreads();
-
-    const int lane = threadIdx.x & 31;
-    const int ci = lane / kLanes;          // centre column inside the tile
-    const int sub = lane % kLanes;         // row slice of the window
-    const int cj = threadIdx.x >> 5;       // centre row inside the tile (warp)
-    const int ctx = ci * sp + hw, cty = cj * sp + hw;   // centre in tile coordinates
-    const int co = cty * g.pitch + ctx;
-
-    const float3 fa_c = make_float3(smem[co], smem[plane + co], smem[2 * plane + co]);
-    const float3 fb_c = make_float3(smem[3 * plane + co], smem[4 * plane + co], smem[5 * plane + co]);
-    const float al_c[3] = {smem[6 * plane + co], smem[7 * plane + co], smem[8 * plane + co]};
-    const float nr_c[3] = {smem[9 * plane + co], smem[10 * plane + co], smem[11 * plane + co]};
-    const float va_c = smem[12 * plane + co], vb_c = smem[13 * plane + co];
-    const float sa_c = smem[14 * plane + co], sb_c = smem[15 * plane + co];
-
-    Normal na, nb;
-    normal_zero(na);
-    normal_zero(nb);
-
-    for (int dy = -hw + sub; dy <= hw; dy += kLanes) {
-        const int rowo = (cty + dy) * g.pitch + ctx;
-        for (int dx = -hw; dx <= hw; ++dx) {
-            const int o = rowo + dx;
-            const float3 ta = make_float3(smem[o], smem[plane + o], smem[2 * plane + o]);
-            const float3 tb = make_float3(smem[3 * plane + o], smem[4 * plane + o], smem[5 * plane + o]);
-            const float da[3] = {smem[6 * plane + o] - al_c[0], smem[7 * plane + o] - al_c[1],
-                                 smem[8 * plane + o] - al_c[2]};
-            const float dn[3] = {smem[9 * plane + o] - nr_c[0], smem[10 * plane + o] - nr_c[1],
-                                 smem[11 * plane + o] - nr_c[2]};
-            const float va_t = smem[12 * plane + o], vb_t = smem[13 * plane + o];
-            const float sa_t = smem[14 * plane + o], sb_t = smem[15 * plane + o];
-            normal_tap(na, ta, fa_c, tb, va_t, va_c, sa_t, sa_c, da, dn);
-            normal_tap(nb, tb, fb_c, ta, vb_t, vb_c, sb_t, sb_c, da, dn);
-        }
-    }
-
-    normal_reduce(na, kLanes);
-    normal_reduce(nb, kLanes);
-
-    const int ci_g = i0 + ci, cj_g = j0 + cj;
-    if (ci_g >= Ws || cj_g >= Hs) return;
-    const size_t nb_img = (size_t)Hs * Ws;
-    const size_t cidx = (size_t)b * nb_img + (size_t)cj_g * Ws + ci_g;
-    const size_t buf_stride = (size_t)gridDim.z * nb_img * kBeta;
-    float *ba = beta + cidx * kBeta;
-    float *bbp = beta + buf_stride + cidx * kBeta;
-    // six (buffer, channel) systems over four lanes: lane s takes s and s+4
-#pragma unroll
-    for (int p = 0; p < 6; ++p) {
-        if (p % kLanes != sub) continue;
-        if (p < 3)
-            solve_channel(na, p, ba);
-        else
-            solve_channel(nb, p - 3, bbp);
-    }
+    const RowGeom g = row_geom(hw, sp);
+    return (size_t)2 * 4 * g.npos * sizeof(float4) + (size_t)2 * g.rw * sizeof(int);
 }
 
-// ---------------------------------------------------------------------------
-// Block reconstruction (ops/regression.cu.cc:289-365).  Each thread owns one
-// output pixel of both buffers and sums, over the centres inside its window
-// (centre range clamped to the image with the reference's iDivUp), the
-// weighted predictions beta_c . delta(p, c) with delta taken as (p - c).
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) recon_kernel(
+CD_DEV void cp_async4(float *dst, const float *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+CD_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> CD_DEV void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+CD_DEV int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
+
+__global__ void __launch_bounds__(kThreads) regression_kernel(
     const float *__restrict__ imga, const float *__restrict__ imgb,
     const float *__restrict__ albedo, const float *__restrict__ normal,
     const float *__restrict__ vara, const float *__restrict__ varb,
-    const float *__restrict__ beta, float *__restrict__ outa, float *__restrict__ outb,
-    int H, int W, int hw, int sp, int rs)
+    const float *__restrict__ sda, const float *__restrict__ sdb, float *__restrict__ beta,
+    int H, int W, int hw, int sp)
 {
-    const int Wr = W / rs, Hr = H / rs;
-    const int cx = blockIdx.x * blockDim.x + threadIdx.x;
-    const int cy = blockIdx.y * blockDim.y + threadIdx.y;
-    if (cx >= Wr || cy >= Hr) return;
+    extern __shared__ float4 sm4[];
+    const RowGeom g = row_geom(hw, sp);
+    const int slot = 4 * g.npos;                                   // float4s per slot
+    int *pos_gx = reinterpret_cast<int *>(sm4 + 2 * slot);
+    int *pos_dst = pos_gx + g.rw;
+    const int Ws = W / sp, Hs = H / sp;
     const int b = blockIdx.z;
     const size_t px = (size_t)H * W;
     imga += 3 * px * b;
@@ -388,11 +260,185 @@ __global__ void __launch_bounds__(256) recon_kernel(
     normal += 3 * px * b;
     vara += px * b;
     varb += px * b;
+    sda += px * b;
+    sdb += px * b;
+
+    const int i0 = blockIdx.x * kCX;
+    const int cy = blockIdx.y * sp;
+    const int x0 = i0 * sp - hw;
+    const int buf = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int R = 2 * hw + 1;
+
+    // Column of every row position (reflect-101; positions past the reflect
+    // range feed no valid centre and are clamped only to stay in bounds) and
+    // its de-interleaved slot index.
+    for (int p = threadIdx.x; p < g.rw; p += kThreads) {
+        pos_gx[p] = clampi(mirror(x0 + p, W), 0, W - 1);
+        pos_dst[p] = (p % sp) * g.q + p / sp;
+    }
+    __syncthreads();
+
+    auto stage = [&](int r, int s) {
+        float *base = reinterpret_cast<float *>(sm4 + s * slot);
+        const int gy = clampi(mirror(cy - hw + r, H), 0, H - 1);
+        const size_t row = (size_t)gy * W;
+        for (int p = threadIdx.x; p < g.rw; p += kThreads) {
+            const size_t q = row + pos_gx[p];
+            float *d = base + 4 * pos_dst[p];
+            const float *a = imga + 3 * q, *c = imgb + 3 * q, *l = albedo + 3 * q, *n = normal + 3 * q;
+            float *d0 = d, *d1 = d + 4 * g.npos, *d2 = d + 8 * g.npos, *d3 = d + 12 * g.npos;
+            cp_async4(d0, a); cp_async4(d0 + 1, a + 1); cp_async4(d0 + 2, a + 2); cp_async4(d0 + 3, vara + q);
+            cp_async4(d1, c); cp_async4(d1 + 1, c + 1); cp_async4(d1 + 2, c + 2); cp_async4(d1 + 3, varb + q);
+            cp_async4(d2, l); cp_async4(d2 + 1, l + 1); cp_async4(d2 + 2, l + 2); cp_async4(d2 + 3, sda + q);
+            cp_async4(d3, n); cp_async4(d3 + 1, n + 1); cp_async4(d3 + 2, n + 2); cp_async4(d3 + 3, sdb + q);
+        }
+    };
+
+    stage(0, 0);
+    cp_async_commit();
+
+    // centre values, read directly (clamped for lanes past the last centre)
+    const int ci = min(i0 + lane, Ws - 1);
+    const size_t c = (size_t)cy * W + (size_t)ci * sp;
+    const float3 fc = ld3(buf ? imgb : imga, c);
+    const float3 alc = ld3(albedo, c), nrc = ld3(normal, c);
+    const float vc = __ldg((buf ? varb : vara) + c), sdc = __ldg((buf ? sdb : sda) + c);
+    const float al_c[3] = {alc.x, alc.y, alc.z}, nr_c[3] = {nrc.x, nrc.y, nrc.z};
+    // groups read by this buffer: own features + variance, target, albedo, normal
+    const int gf = buf ? 1 : 0, gy_ = buf ? 0 : 1;
+
+    Normal nm;
+    normal_zero(nm);
+    for (int r = 0; r < R; ++r) {
+        if (r + 1 < R) {
+            stage(r + 1, (r + 1) & 1);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const float4 *P = sm4 + (r & 1) * slot;
+        const float4 *Gf = P + gf * g.npos, *Gy = P + gy_ * g.npos;
+        const float4 *Ga = P + 2 * g.npos, *Gn = P + 3 * g.npos;
+        int tm = 0, td = 0;
+        for (int t = 0; t < R; ++t) {
+            const int o = tm * g.q + td + lane;
+            const float4 f4 = Gf[o], y4 = Gy[o], a4 = Ga[o], n4 = Gn[o];
+            // own standard deviation: sdA rides in g2.w, sdB in g3.w
+            const float sdt = buf ? n4.w : a4.w;
+            const float da[3] = {a4.x - al_c[0], a4.y - al_c[1], a4.z - al_c[2]};
+            const float dn[3] = {n4.x - nr_c[0], n4.y - nr_c[1], n4.z - nr_c[2]};
+            normal_tap(nm, make_float3(f4.x, f4.y, f4.z), fc, make_float3(y4.x, y4.y, y4.z), f4.w, vc, sdt,
+                       sdc, da, dn);
+            if (++tm == sp) {
+                tm = 0;
+                ++td;
+            }
+        }
+        __syncthreads();
+    }
+
+    if (i0 + lane >= Ws) return;
+    const size_t nb_img = (size_t)Hs * Ws;
+    const size_t cidx = (size_t)b * nb_img + (size_t)blockIdx.y * Ws + (i0 + lane);
+    float *bo = beta + (size_t)buf * gridDim.z * nb_img * kBeta + cidx * kBeta;
+    solve_channel(nm, 0, bo);
+    solve_channel(nm, 1, bo);
+    solve_channel(nm, 2, bo);
+}
+
+// ---------------------------------------------------------------------------
+// Block reconstruction (ops/regression.cu.cc:289-365).  A CTA owns 32x4
+// output pixels.  The centres their windows reach are staged in shared
+// memory as 13 float4 records each:
+//   [0..8]  beta of buffers A and B (18 + 18 floats: coefficient-major)
+//   [9]  (imga.xyz, varA)  [10] (imgb.xyz, varB)
+//   [11] (albedo.xyz, sdA) [12] (normal.xyz, sdB)
+// Each thread sums, over the centres of its own window (the reference's
+// clamped iDivUp range, in its order), w * (beta_c . delta(p, c)) with delta
+// taken as (p - c).  The quotients use a reciprocal and a multiply: unlike
+// the regression's normal equations, nothing downstream amplifies their
+// last-bit differences.
+// ---------------------------------------------------------------------------
+constexpr int kRX = 32, kRY = 4;
+constexpr int kRec = 13;   // float4 per staged centre
+
+__host__ __device__ inline int floordiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+__host__ __device__ inline size_t recon_smem(int hw, int sp, int rs)
+{
+    const int cxmax = ((kRX - 1) * rs + 2 * hw) / sp + 2;
+    const int cymax = ((kRY - 1) * rs + 2 * hw) / sp + 2;
+    return (size_t)kRec * cxmax * cymax * sizeof(float4);
+}
+
+CD_DEV float4 ld4f(const float *p) { return make_float4(__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3)); }
+
+__global__ void __launch_bounds__(kRX * kRY) recon_kernel(
+    const float *__restrict__ imga, const float *__restrict__ imgb,
+    const float *__restrict__ albedo, const float *__restrict__ normal,
+    const float *__restrict__ vara, const float *__restrict__ varb,
+    const float *__restrict__ sda, const float *__restrict__ sdb,
+    const float *__restrict__ beta, float *__restrict__ outa, float *__restrict__ outb,
+    int H, int W, int hw, int sp, int rs)
+{
+    extern __shared__ float4 rec[];
+    const int Wr = W / rs, Hr = H / rs;
     const int Ws = W / sp, Hs = H / sp;
+    const int b = blockIdx.z;
+    const size_t px = (size_t)H * W;
+    imga += 3 * px * b;
+    imgb += 3 * px * b;
+    albedo += 3 * px * b;
+    normal += 3 * px * b;
+    vara += px * b;
+    varb += px * b;
+    sda += px * b;
+    sdb += px * b;
     const size_t nb_img = (size_t)Hs * Ws;
     const float *betaA = beta + (size_t)b * nb_img * kBeta;
     const float *betaB = beta + (size_t)gridDim.z * nb_img * kBeta + (size_t)b * nb_img * kBeta;
 
+    // centres any pixel of this tile can reach (a superset of every
+    // per-pixel range below)
+    const int ox0 = blockIdx.x * kRX, oy0 = blockIdx.y * kRY;
+    const int ox1 = min(ox0 + kRX - 1, Wr - 1), oy1 = min(oy0 + kRY - 1, Hr - 1);
+    const int cx_lo = max(0, floordiv(ox0 * rs - hw, sp));
+    const int cx_hi = min(Ws - 1, (ox1 * rs + hw) / sp);
+    const int cy_lo = max(0, floordiv(oy0 * rs - hw, sp));
+    const int cy_hi = min(Hs - 1, (oy1 * rs + hw) / sp);
+    const int ncx = cx_hi - cx_lo + 1, ncy = cy_hi - cy_lo + 1;
+    const int nc = ncx * ncy;
+
+    const int tid = threadIdx.y * kRX + threadIdx.x;
+    for (int e = tid; e < nc * 9; e += kRX * kRY) {
+        const int n = e / 9, f = e - 9 * n;
+        const int iy = cy_lo + n / ncx, ix = cx_lo + n % ncx;
+        const size_t cb = ((size_t)iy * Ws + ix) * kBeta;
+        float4 v;
+        if (f < 4)
+            v = ld4f(betaA + cb + 4 * f);
+        else if (f == 4)
+            v = make_float4(__ldg(betaA + cb + 16), __ldg(betaA + cb + 17), __ldg(betaB + cb), __ldg(betaB + cb + 1));
+        else
+            v = ld4f(betaB + cb + 2 + 4 * (f - 5));
+        rec[n * kRec + f] = v;
+    }
+    for (int n = tid; n < nc; n += kRX * kRY) {
+        const int iy = cy_lo + n / ncx, ix = cx_lo + n % ncx;
+        const size_t t = (size_t)(iy * sp) * W + ix * sp;
+        const float3 fa = ld3(imga, t), fb = ld3(imgb, t), al = ld3(albedo, t), nr = ld3(normal, t);
+        rec[n * kRec + 9] = make_float4(fa.x, fa.y, fa.z, __ldg(vara + t));
+        rec[n * kRec + 10] = make_float4(fb.x, fb.y, fb.z, __ldg(varb + t));
+        rec[n * kRec + 11] = make_float4(al.x, al.y, al.z, __ldg(sda + t));
+        rec[n * kRec + 12] = make_float4(nr.x, nr.y, nr.z, __ldg(sdb + t));
+    }
+    __syncthreads();
+
+    const int cx = ox0 + threadIdx.x, cy = oy0 + threadIdx.y;
+    if (cx >= Wr || cy >= Hr) return;
     const int pxo = cx * rs, pyo = cy * rs;
     const size_t p = (size_t)pyo * W + pxo;
     const int sx = max(0, idivup(pxo - hw, sp));
@@ -402,101 +448,128 @@ __global__ void __launch_bounds__(256) recon_kernel(
 
     const float3 fa = ld3(imga, p), fb = ld3(imgb, p), al = ld3(albedo, p), nr = ld3(normal, p);
     const float va = __ldg(vara + p), vb = __ldg(varb + p);
-    const float sa = sqrtf(va), sb = sqrtf(vb);
-    float oa[3] = {0.f, 0.f, 0.f}, ob[3] = {0.f, 0.f, 0.f};
+    const float sa = __ldg(sda + p), sb = __ldg(sdb + p);
+    float oa0 = 0.f, oa1 = 0.f, oa2 = 0.f, ob0 = 0.f, ob1 = 0.f, ob2 = 0.f;
     float swa = 0.f, swb = 0.f;
     for (int iy = sy; iy <= ey; ++iy) {
+        const int nrow = (iy - cy_lo) * ncx - cx_lo;
         for (int ix = sx; ix <= ex; ++ix) {
-            const size_t t = (size_t)(iy * sp) * W + ix * sp;
-            const size_t cb = ((size_t)iy * Ws + ix) * kBeta;
-            const float3 ta = ld3(imga, t), tb = ld3(imgb, t), tal = ld3(albedo, t), tnr = ld3(normal, t);
-            const float vta = __ldg(vara + t), vtb = __ldg(varb + t);
-            const float da[3] = {al.x - tal.x, al.y - tal.y, al.z - tal.z};
-            const float dn[3] = {nr.x - tnr.x, nr.y - tnr.y, nr.z - tnr.z};
+            const float4 *R = rec + (nrow + ix) * kRec;
+            const float4 A9 = R[9], B10 = R[10], L11 = R[11], N12 = R[12];
+            const float da0 = al.x - L11.x, da1 = al.y - L11.y, da2 = al.z - L11.z;
+            const float dn0 = nr.x - N12.x, dn1 = nr.y - N12.y, dn2 = nr.z - N12.z;
+            // buffer A: features imga, coefficients records 0..4.x
             {
-                const float df[3] = {fa.x - ta.x, fa.y - ta.y, fa.z - ta.z};
-                const float den = (sa + sqrtf(vta)) + 1e-2f;
-                const float dist = norm2(-df[0], -df[1], -df[2]) / ((va + vta) + 1e-4f);
-                const float w = __expf(-dist) + 1e-7f;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    const float *bc = betaA + cb + k;
-                    float pr = __ldg(bc);
-                    pr = fmaf(__ldg(bc + 3), df[k] / den, pr);
-                    pr = fmaf(__ldg(bc + 6), da[k], pr);
-                    pr = fmaf(__ldg(bc + 9), dn[0], pr);
-                    pr = fmaf(__ldg(bc + 12), dn[1], pr);
-                    pr = fmaf(__ldg(bc + 15), dn[2], pr);
-                    oa[k] = fmaf(w, pr, oa[k]);
-                }
+                const float d0 = fa.x - A9.x, d1 = fa.y - A9.y, d2 = fa.z - A9.z;
+                const float rden = __fdividef(1.f, (sa + L11.w) + 1e-2f);
+                const float w = __expf(-(sqnorm(d0, d1, d2) * __fdividef(1.f, (va + A9.w) + 1e-4f))) + 1e-7f;
+                const float4 c0 = R[0], c1 = R[1], c2 = R[2], c3 = R[3], c4 = R[4];
+                // beta layout r * 3 + k: c0 = (b0x b0y b0z b1x) c1 = (b1y b1z b2x b2y)
+                // c2 = (b2z b3x b3y b3z) c3 = (b4x b4y b4z b5x) c4 = (b5y b5z | B b0x b0y)
+                float p0 = c0.x, p1 = c0.y, p2 = c0.z;
+                p0 = fmaf(c0.w, d0 * rden, p0);
+                p1 = fmaf(c1.x, d1 * rden, p1);
+                p2 = fmaf(c1.y, d2 * rden, p2);
+                p0 = fmaf(c1.z, da0, p0);
+                p1 = fmaf(c1.w, da1, p1);
+                p2 = fmaf(c2.x, da2, p2);
+                p0 = fmaf(c2.y, dn0, p0);
+                p1 = fmaf(c2.z, dn0, p1);
+                p2 = fmaf(c2.w, dn0, p2);
+                p0 = fmaf(c3.x, dn1, p0);
+                p1 = fmaf(c3.y, dn1, p1);
+                p2 = fmaf(c3.z, dn1, p2);
+                p0 = fmaf(c3.w, dn2, p0);
+                p1 = fmaf(c4.x, dn2, p1);
+                p2 = fmaf(c4.y, dn2, p2);
+                oa0 = fmaf(w, p0, oa0);
+                oa1 = fmaf(w, p1, oa1);
+                oa2 = fmaf(w, p2, oa2);
                 swa += w;
             }
+            // buffer B: features imgb, coefficients records 4.zw..8
             {
-                const float df[3] = {fb.x - tb.x, fb.y - tb.y, fb.z - tb.z};
-                const float den = (sb + sqrtf(vtb)) + 1e-2f;
-                const float dist = norm2(-df[0], -df[1], -df[2]) / ((vb + vtb) + 1e-4f);
-                const float w = __expf(-dist) + 1e-7f;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    const float *bc = betaB + cb + k;
-                    float pr = __ldg(bc);
-                    pr = fmaf(__ldg(bc + 3), df[k] / den, pr);
-                    pr = fmaf(__ldg(bc + 6), da[k], pr);
-                    pr = fmaf(__ldg(bc + 9), dn[0], pr);
-                    pr = fmaf(__ldg(bc + 12), dn[1], pr);
-                    pr = fmaf(__ldg(bc + 15), dn[2], pr);
-                    ob[k] = fmaf(w, pr, ob[k]);
-                }
+                const float d0 = fb.x - B10.x, d1 = fb.y - B10.y, d2 = fb.z - B10.z;
+                const float rden = __fdividef(1.f, (sb + N12.w) + 1e-2f);
+                const float w = __expf(-(sqnorm(d0, d1, d2) * __fdividef(1.f, (vb + B10.w) + 1e-4f))) + 1e-7f;
+                const float4 c4 = R[4], c5 = R[5], c6 = R[6], c7 = R[7], c8 = R[8];
+                // c4.zw = (b0x b0y) c5 = (b0z b1x b1y b1z) c6 = (b2x b2y b2z b3x)
+                // c7 = (b3y b3z b4x b4y) c8 = (b4z b5x b5y b5z)
+                float p0 = c4.z, p1 = c4.w, p2 = c5.x;
+                p0 = fmaf(c5.y, d0 * rden, p0);
+                p1 = fmaf(c5.z, d1 * rden, p1);
+                p2 = fmaf(c5.w, d2 * rden, p2);
+                p0 = fmaf(c6.x, da0, p0);
+                p1 = fmaf(c6.y, da1, p1);
+                p2 = fmaf(c6.z, da2, p2);
+                p0 = fmaf(c6.w, dn0, p0);
+                p1 = fmaf(c7.x, dn0, p1);
+                p2 = fmaf(c7.y, dn0, p2);
+                p0 = fmaf(c7.z, dn1, p0);
+                p1 = fmaf(c7.w, dn1, p1);
+                p2 = fmaf(c8.x, dn1, p2);
+                p0 = fmaf(c8.y, dn2, p0);
+                p1 = fmaf(c8.z, dn2, p1);
+                p2 = fmaf(c8.w, dn2, p2);
+                ob0 = fmaf(w, p0, ob0);
+                ob1 = fmaf(w, p1, ob1);
+                ob2 = fmaf(w, p2, ob2);
                 swb += w;
             }
         }
     }
     const float dA = fmaxf(swa, 1e-7f), dB = fmaxf(swb, 1e-7f);
     const size_t o = (size_t)b * Hr * Wr + (size_t)cy * Wr + cx;
-    st3(outa, o, make_float3(fmaxf(0.f, oa[0] / dA), fmaxf(0.f, oa[1] / dA), fmaxf(0.f, oa[2] / dA)));
-    st3(outb, o, make_float3(fmaxf(0.f, ob[0] / dB), fmaxf(0.f, ob[1] / dB), fmaxf(0.f, ob[2] / dB)));
+    st3(outa, o, make_float3(fmaxf(0.f, oa0 / dA), fmaxf(0.f, oa1 / dA), fmaxf(0.f, oa2 / dA)));
+    st3(outb, o, make_float3(fmaxf(0.f, ob0 / dB), fmaxf(0.f, ob1 / dB), fmaxf(0.f, ob2 / dB)));
 }
 
 }  // namespace
 
-cudaError_t launch_variance(const float *imga, const float *imgb, float *vara, float *varb,
-                            int B, int H, int W, cudaStream_t st)
+cudaError_t launch_variance(const float *imga, const float *imgb, float *vara, float *varb, float *sda,
+                            float *sdb, int B, int H, int W, cudaStream_t st)
 {
     dim3 block(32, 8);
     dim3 grid((W + 31) / 32, (H + 7) / 8, 2 * B);
-    variance_kernel<<<grid, block, 0, st>>>(imga, imgb, vara, varb, H, W);
+    variance_kernel<<<grid, block, 0, st>>>(imga, imgb, vara, varb, sda, sdb, H, W);
     return cudaGetLastError();
 }
 
+size_t regression_smem_bytes(int win, int sp) { return regression_smem(win / 2, sp); }
+size_t recon_smem_bytes(int win, int sp, int rs) { return recon_smem(win / 2, sp, rs); }
+
 cudaError_t launch_regression(const float *imga, const float *imgb, const float *albedo,
                               const float *normal, const float *vara, const float *varb,
-                              float *beta, int B, int H, int W, int win, int sp, cudaStream_t st)
+                              const float *sda, const float *sdb, float *beta, int B, int H, int W,
+                              int win, int sp, cudaStream_t st)
 {
     const int hw = win / 2;
-    int tcy = 4;
-    while (tcy > 1 && tile_geom(hw, sp, tcy).smem > 200 * 1024) tcy >>= 1;
-    const TileGeom g = tile_geom(hw, sp, tcy);
-    if (g.smem > 220 * 1024) return cudaErrorInvalidConfiguration;
-    cudaError_t e = cudaFuncSetAttribute(regression_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem);
+    const size_t smem = regression_smem(hw, sp);
+    cudaError_t e = cudaFuncSetAttribute(regression_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
     if (e != cudaSuccess) return e;
     const int Ws = W / sp, Hs = H / sp;
-    dim3 grid((Ws + kTCX - 1) / kTCX, (Hs + tcy - 1) / tcy, B);
-    regression_kernel<<<grid, 32 * tcy, g.smem, st>>>(imga, imgb, albedo, normal, vara, varb,
-                                                      beta, H, W, hw, sp, tcy);
+    dim3 grid((Ws + kCX - 1) / kCX, Hs, B);
+    regression_kernel<<<grid, kThreads, smem, st>>>(imga, imgb, albedo, normal, vara, varb, sda, sdb, beta,
+                                                    H, W, hw, sp);
     return cudaGetLastError();
 }
 
 cudaError_t launch_recon(const float *imga, const float *imgb, const float *albedo,
-                         const float *normal, const float *vara, const float *varb,
-                         const float *beta, float *outa, float *outb, int B, int H, int W,
-                         int win, int sp, int rs, cudaStream_t st)
+                         const float *normal, const float *vara, const float *varb, const float *sda,
+                         const float *sdb, const float *beta, float *outa, float *outb, int B, int H,
+                         int W, int win, int sp, int rs, cudaStream_t st)
 {
+    const int hw = win / 2;
+    const size_t smem = recon_smem(hw, sp, rs);
+    cudaError_t e = cudaFuncSetAttribute(recon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
     const int Wr = W / rs, Hr = H / rs;
-    dim3 block(32, 8);
-    dim3 grid((Wr + 31) / 32, (Hr + 7) / 8, B);
-    recon_kernel<<<grid, block, 0, st>>>(imga, imgb, albedo, normal, vara, varb, beta, outa, outb,
-                                         H, W, win / 2, sp, rs);
+    dim3 block(kRX, kRY);
+    dim3 grid((Wr + kRX - 1) / kRX, (Hr + kRY - 1) / kRY, B);
+    recon_kernel<<<grid, block, smem, st>>>(imga, imgb, albedo, normal, vara, varb, sda, sdb, beta, outa,
+                                            outb, H, W, hw, sp, rs);
     return cudaGetLastError();
 }
 

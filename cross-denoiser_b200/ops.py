@@ -28,7 +28,8 @@ from . import _lib
 
 __all__ = [
     "cross_regression", "spatial_filter", "spatial_filter_grad", "temporal_screening",
-    "Reproject", "reproject", "erode3x3", "erode_temporal_screening",
+    "Reproject", "reproject", "erode3x3", "erode_temporal_screening", "prepare_input",
+    "aggregation_loss", "filter_aggregate",
 ]
 
 
@@ -280,3 +281,84 @@ def erode_temporal_screening(current1, current2, prev, prev1, prev2, reproj_mask
         _ptr(eroded), _ptr(out), _ptr(out1), _ptr(out2), _ptr(succ), B, H, W, int(win_curr),
         int(win_prev), _stream()), "erode_temporal_screening")
     return out, out1, out2, succ, eroded
+
+
+# ---------------------------------------------------------------------------
+# The rest of the per-frame step: input preparation and the aggregation loss
+# ---------------------------------------------------------------------------
+def prepare_input(color, color2):
+    """(y1, y2) = (log1p(color), log1p(color2)): prepare_input of
+    scripts/main.py:207-212."""
+    color = _img(color, "color", 3)
+    color2 = _img(color2, "color2", 3, color)
+    y1, y2 = torch.empty_like(color), torch.empty_like(color2)
+    _lib.check(_lib.lib().cd_prepare_input(_ptr(color), _ptr(color2), _ptr(y1), _ptr(y2), color.numel(),
+                                           _stream()), "prepare_input")
+    return y1, y2
+
+
+def _ws(nbytes, device):
+    return torch.empty((max(int(nbytes), 4),), dtype=torch.uint8, device=device)
+
+
+def aggregation_loss(sum1, sumw1, sum2, sumw2, alpha, success, success_prev, prev_out, opacity, label1,
+                     label2, prev_label1, prev_label2, with_loss: bool = True):
+    """aggregation_loss of scripts/main.py:214-248 with its gradient.
+
+    Returns (out_log, out, loss, avg_loss, grad_sum1, grad_sumw1, grad_sum2,
+    grad_sumw2, grad_alpha); ``out_log`` is the reference's ``out`` (log
+    domain), ``out`` its max(0, expm1(.)), the gradients are dL/d(input) of
+    L = avg_loss.  ``loss`` is None when ``with_loss`` is False.
+    """
+    sum1 = _img(sum1, "sum1", 3)
+    ref = sum1
+    sumw1, sum2, sumw2 = _img(sumw1, "sumw1", 1, ref), _img(sum2, "sum2", 3, ref), _img(sumw2, "sumw2", 1, ref)
+    alpha, success = _img(alpha, "alpha", 1, ref), _img(success, "success", 1, ref)
+    success_prev, prev_out = _img(success_prev, "success_prev", 1, ref), _img(prev_out, "prev_out", 3, ref)
+    opacity = _img(opacity, "opacity", 1, ref)
+    labels = [_img(t, n, 3, ref) for t, n in ((label1, "label1"), (label2, "label2"),
+                                                (prev_label1, "prev_label1"), (prev_label2, "prev_label2"))]
+    B, H, W, _ = sum1.shape
+    out_log, out = torch.empty_like(sum1), torch.empty_like(sum1)
+    loss = torch.empty_like(sum1) if with_loss else None
+    avg = sum1.new_empty(())
+    g1, g2 = torch.empty_like(sum1), torch.empty_like(sum1)
+    gw1, gw2, ga = torch.empty_like(sumw1), torch.empty_like(sumw1), torch.empty_like(sumw1)
+    L = _lib.lib()
+    nbytes = L.cd_aggregation_workspace_size(B, H, W)
+    ws = _ws(nbytes, sum1.device)
+    _lib.check(L.cd_aggregation_loss(_ptr(sum1), _ptr(sumw1), _ptr(sum2), _ptr(sumw2), _ptr(alpha), _ptr(success),
+                                     _ptr(success_prev), _ptr(prev_out), _ptr(opacity), *[_ptr(t) for t in labels],
+                                     _ptr(out_log), _ptr(out), _ptr(loss) if with_loss else None, _ptr(avg),
+                                     _ptr(g1), _ptr(gw1), _ptr(g2), _ptr(gw2), _ptr(ga), B, H, W, _ptr(ws),
+                                     nbytes, _stream()), "aggregation_loss")
+    return out_log, out, loss, avg, g1, gw1, g2, gw2, ga
+
+
+def filter_aggregate(ols1, ols2, albedo, normal, band, alpha, success, success_prev, prev_out, opacity,
+                     prev_ols1, prev_ols2, win_size: int):
+    """spatial_filter -> aggregation_loss -> spatial_filter_grad
+    (scripts/main.py:295-302) in one kernel pass.
+
+    Returns (out_log, out, avg_loss, grad_band, grad_alpha).
+    """
+    ols1 = _img(ols1, "ols1", 3)
+    ref = ols1
+    ols2, albedo, normal = _img(ols2, "ols2", 3, ref), _img(albedo, "albedo", 3, ref), _img(normal, "normal", 3, ref)
+    band, alpha = _img(band, "band", 5, ref), _img(alpha, "alpha", 1, ref)
+    success, success_prev = _img(success, "success", 1, ref), _img(success_prev, "success_prev", 1, ref)
+    prev_out, opacity = _img(prev_out, "prev_out", 3, ref), _img(opacity, "opacity", 1, ref)
+    prev_ols1, prev_ols2 = _img(prev_ols1, "prev_ols1", 3, ref), _img(prev_ols2, "prev_ols2", 3, ref)
+    B, H, W, _ = ols1.shape
+    out_log, out = torch.empty_like(ols1), torch.empty_like(ols1)
+    avg = ols1.new_empty(())
+    gband, galpha = torch.empty_like(band), torch.empty_like(alpha)
+    L = _lib.lib()
+    nbytes = L.cd_filter_aggregate_workspace_size(B, H, W)
+    ws = _ws(nbytes, ols1.device)
+    _lib.check(L.cd_filter_aggregate(_ptr(ols1), _ptr(ols2), _ptr(albedo), _ptr(normal), _ptr(band), _ptr(alpha),
+                                     _ptr(success), _ptr(success_prev), _ptr(prev_out), _ptr(opacity),
+                                     _ptr(prev_ols1), _ptr(prev_ols2), _ptr(out_log), _ptr(out), _ptr(avg),
+                                     _ptr(gband), _ptr(galpha), B, H, W, int(win_size), _ptr(ws), nbytes,
+                                     _stream()), "filter_aggregate")
+    return out_log, out, avg, gband, galpha

@@ -21,9 +21,11 @@ is pluggable: ``FrameStep(predictor=...)`` takes any callable returning
 (band [B,H,W,5], alpha [B,H,W,1]) and receives the gradients through
 ``on_gradients``; by default a fixed band/alpha is used.
 
-``plain`` runs the drop-in op sequence (separate erosion and screening
-kernels); ``fused`` runs erosion and screening as one kernel.  Both give
-bit-identical results.
+``plain`` runs the drop-in op sequence (separate erosion, screening,
+filter, aggregation and gradient kernels); ``fused`` runs erosion with
+screening as one kernel and the filter, aggregation loss and band gradient
+as one kernel.  The two agree within rounding of the loss terms; the masks,
+the filtered frame and the history are identical.
 """
 from __future__ import annotations
 
@@ -68,8 +70,11 @@ class History:
 
 def aggregation_forward_backward(sum1, sumw1, sum2, sumw2, alpha, success, success_prev, prev_out,
                                  opacity, label1, label2, prev_label1, prev_label2):
-    """aggregation_loss (scripts/main.py:214-248) and its gradient with
-    respect to (sum1, sumw1, sum2, sumw2, alpha), in closed form.
+    """Eager PyTorch restatement of aggregation_loss (scripts/main.py:214-248)
+    and its gradient with respect to (sum1, sumw1, sum2, sumw2, alpha), in
+    closed form: the FP32 reference the fused CUDA kernels are tested
+    against, and the glue of the baseline arm that drives the reference's
+    kernels.
 
     Returns (out, out_linear, loss, avg_loss, g_sum1, g_sumw1, g_sum2, g_sumw2, g_alpha).
     """
@@ -128,8 +133,7 @@ class FrameStep:
         if self.history is None:
             self.history = History.zeros(B, H, W, color.device)
         h = self.history
-        y1 = torch.log1p(color)
-        y2 = torch.log1p(f["color2"])
+        y1, y2 = ops.prepare_input(color, f["color2"])
         albedo, normal = f["albedo"], f["normal"]
         ols1, ols2, _, _ = ops.cross_regression(y1, y2, albedo, normal, win_size=cfg.regression_width,
                                                 sparsity=cfg.sparsity)
@@ -147,13 +151,20 @@ class FrameStep:
             band, alpha = self.predictor(ols1, ols2, prev_out, albedo, normal)
         else:
             band, alpha = self.fixed_band, self.fixed_alpha
-        sum1, sum2, sumw1, sumw2 = ops.spatial_filter(ols1, ols2, albedo, normal, band.detach(),
-                                                      win_size=cfg.filter_width)
-        (out_log, out, loss, avg, g1, gw1, g2, gw2, g_alpha) = aggregation_forward_backward(
-            sum1, sumw1, sum2, sumw2, alpha.detach(), success_f, success_prev, prev_out, f["opacity"],
-            ols2, ols1, prev_ols2, prev_ols1)
-        g_band = ops.spatial_filter_grad(g1, g2, gw1, gw2, ols1, ols2, albedo, normal, band.detach(),
-                                         win_size=cfg.filter_width)
+        band, alpha = band.detach(), alpha.detach()
+        loss = None
+        if cfg.fused:
+            out_log, out, avg, g_band, g_alpha = ops.filter_aggregate(
+                ols1, ols2, albedo, normal, band, alpha, success_f, success_prev, prev_out, f["opacity"],
+                prev_ols1, prev_ols2, win_size=cfg.filter_width)
+        else:
+            sum1, sum2, sumw1, sumw2 = ops.spatial_filter(ols1, ols2, albedo, normal, band,
+                                                          win_size=cfg.filter_width)
+            (out_log, out, loss, avg, g1, gw1, g2, gw2, g_alpha) = ops.aggregation_loss(
+                sum1, sumw1, sum2, sumw2, alpha, success_f, success_prev, prev_out, f["opacity"],
+                ols2, ols1, prev_ols2, prev_ols1)
+            g_band = ops.spatial_filter_grad(g1, g2, gw1, gw2, ols1, ols2, albedo, normal, band,
+                                             win_size=cfg.filter_width)
         if self.on_gradients is not None:
             self.on_gradients(g_band, g_alpha)
         self.history = History(out_log, ols1, ols2, f["linearZ"], normal)

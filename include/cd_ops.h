@@ -69,7 +69,8 @@ CD_API const char *cd_get_last_error(void);
 /* 1 <= recon_scale <= sparsity, H and W divisible by sparsity and by         */
 /* recon_scale, win_size/2 < min(H, W).                                       */
 /* The workspace holds the per-centre regression coefficients (the           */
-/* reference's process-static betaA/betaB, ops/regression.cc:174-180).        */
+/* reference's process-static betaA/betaB, ops/regression.cc:174-180) and    */
+/* the per-pixel standard deviations of both images.                          */
 /* ------------------------------------------------------------------------ */
 CD_API size_t cd_cross_regression_workspace_size(int B, int H, int W, int sparsity);
 
@@ -185,6 +186,57 @@ CD_API cd_status cd_erode_temporal_screening(const float *current1, const float 
                                       float *success,
                                       int B, int H, int W, int win_curr, int win_prev,
                                       cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Input preparation: y1 = log1p(color), y2 = log1p(color2), the            */
+/* prepare_input of scripts/main.py:207-212.  n = number of floats in each.  */
+/* ------------------------------------------------------------------------ */
+CD_API cd_status cd_prepare_input(const float *color, const float *color2, float *y1, float *y2,
+                                  size_t n, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Aggregation loss, forward and backward                                     */
+/* Replaces aggregation_loss (scripts/main.py:214-248) and the part of the    */
+/* TensorFlow gradient (scripts/main.py:302) that flows into the spatial      */
+/* filter's outputs and alpha.                                                */
+/*  sum1, sum2, prev_out, label1, label2, prev_label1, prev_label2 : [B,H,W,3] */
+/*  sumw1, sumw2, alpha, success, success_prev, opacity : [B,H,W,1]           */
+/*  out_log (before expm1), out (max(0, expm1(out_log))), loss : [B,H,W,3]    */
+/*  avg_loss : one float, mean of loss over B*H*W*3 elements                  */
+/*  grad_sum1, grad_sum2 : [B,H,W,3]; grad_sumw1, grad_sumw2, grad_alpha      */
+/*  : [B,H,W,1] -- dL/d(input) of L = avg_loss.  loss may be NULL.            */
+/* The workspace holds per-CTA partial sums of the loss (the mean is reduced */
+/* in a fixed order, so it is deterministic).                                 */
+/* ------------------------------------------------------------------------ */
+CD_API size_t cd_aggregation_workspace_size(int B, int H, int W);
+CD_API cd_status cd_aggregation_loss(const float *sum1, const float *sumw1, const float *sum2,
+                                     const float *sumw2, const float *alpha, const float *success,
+                                     const float *success_prev, const float *prev_out,
+                                     const float *opacity, const float *label1, const float *label2,
+                                     const float *prev_label1, const float *prev_label2,
+                                     float *out_log, float *out, float *loss, float *avg_loss,
+                                     float *grad_sum1, float *grad_sumw1, float *grad_sum2,
+                                     float *grad_sumw2, float *grad_alpha, int B, int H, int W,
+                                     void *workspace, size_t workspace_bytes, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Spatial filter + aggregation loss + band gradient in one pass             */
+/* The spatial_filter -> aggregation_loss -> SpatialFilterGrad sequence of    */
+/* scripts/main.py:295-302 with the labels crossed as :283-286 sets them      */
+/* (label1 = ols2, label2 = ols1, prev_label1 = prev_ols2, prev_label2 =      */
+/* prev_ols1).  Same results as cd_spatial_filter, cd_aggregation_loss and    */
+/* cd_spatial_filter_grad in sequence, without the filter sums leaving the   */
+/* chip.  grad_band : [B,H,W,5] = dL/dband, grad_alpha : [B,H,W,1].          */
+/* ------------------------------------------------------------------------ */
+CD_API size_t cd_filter_aggregate_workspace_size(int B, int H, int W);
+CD_API cd_status cd_filter_aggregate(const float *ols1, const float *ols2, const float *albedo,
+                                     const float *normal, const float *band, const float *alpha,
+                                     const float *success, const float *success_prev,
+                                     const float *prev_out, const float *opacity,
+                                     const float *prev_ols1, const float *prev_ols2,
+                                     float *out_log, float *out, float *avg_loss, float *grad_band,
+                                     float *grad_alpha, int B, int H, int W, int win_size,
+                                     void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
 /* FP32 FMA throughput probe (no counterpart in the reference): `blocks`     */

@@ -55,7 +55,7 @@ def test_invalid_arguments_are_rejected_without_a_device(cd):
     assert rc == cd._lib.CD_EINVAL
     rc = lib.cd_erode3x3(None, p, 1, 8, 8, st)
     assert rc == cd._lib.CD_EINVAL
-    assert lib.cd_cross_regression_workspace_size(2, 64, 32, 4) == 2 * 2 * 16 * 8 * 18 * 4
+    assert lib.cd_cross_regression_workspace_size(2, 64, 32, 4) == (2 * 2 * 16 * 8 * 18 + 2 * 2 * 64 * 32) * 4
 
 
 def test_ops_refuse_cpu_tensors(cd):

@@ -1,0 +1,124 @@
+"""The rest of the frame step on the GPU: input preparation, the aggregation
+loss forward/backward against its eager PyTorch FP32 restatement and FP64,
+the fused filter + loss + gradient kernel against the plain op sequence,
+and whole frames of FrameStep against the CPU oracle."""
+import numpy as np
+import pytest
+import torch
+
+from gpu_util import N, T, frames
+from helpers import assert_close, assert_equal
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def test_prepare_input(cd, cuda):
+    _, f = frames(cd, 64, 96, seed=1)
+    y1, y2 = cd.ops.prepare_input(T(f["color"]), T(f["color2"]))
+    assert_close(N(y1), np.log1p(f["color"]), "y1", rtol=4e-7, atol=0)   # 2 ulp
+    assert_close(N(y2), np.log1p(f["color2"]), "y2", rtol=4e-7, atol=0)
+
+
+def agg_inputs(H, W, B, seed, device):
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    r = lambda c, lo=0.0, hi=1.0: (lo + (hi - lo) * torch.rand((B, H, W, c), generator=g)).to(device)
+    w1, w2 = r(1, 0.5, 30.0), r(1, 0.5, 30.0)
+    s1, s2 = r(3, 0, 3) * w1, r(3, 0, 3) * w2
+    succ = (r(1) > 0.2).float()
+    sp = (r(1) > 0.3).float()
+    opac = (r(1) > 0.05).float()
+    return [s1, w1, s2, w2, r(1), succ, sp, r(3, 0, 3), opac, r(3, 0, 3), r(3, 0, 3), r(3, 0, 3), r(3, 0, 3)]
+
+
+@pytest.mark.parametrize("H,W,B", [(64, 96, 1), (37, 53, 2), (270, 480, 1)])
+def test_aggregation_vs_torch_and_fp64(cd, cuda, H, W, B):
+    x = agg_inputs(H, W, B, seed=H, device=cuda)
+    mine = cd.ops.aggregation_loss(*x)
+    ref32 = cd.step.aggregation_forward_backward(*x)
+    ref64 = cd.step.aggregation_forward_backward(*[t.double() for t in x])
+    names = ("out_log", "out", "loss", "avg_loss", "g_sum1", "g_sumw1", "g_sum2", "g_sumw2", "g_alpha")
+    for m, r32, r64, nm in zip(mine, ref32, ref64, names):
+        scale = float(r64.abs().max())
+        assert_close(N(m), N(r32), nm + " vs torch fp32", atol=1e-6 * scale)
+        assert_close(N(m), N(r64), nm + " vs fp64", atol=1e-6 * scale)
+    again = cd.ops.aggregation_loss(*x)
+    assert float(again[3]) == float(mine[3]), "the mean is reduced in a fixed order"
+
+
+def filter_inputs(cd, H, W, seed, device):
+    _, f = frames(cd, H, W, seed=seed)
+    y1, y2 = np.log1p(f["color"]), np.log1p(f["color2"])
+    g = torch.Generator().manual_seed(seed)
+    band = cd.synth.random_band((1, H, W), g)
+    x = agg_inputs(H, W, 1, seed, device)
+    alpha, succ, sp, prev, opac, pl1, pl2 = x[4], x[5], x[6], x[7], x[8], x[11], x[12]
+    return (T(y1), T(y2), T(f["albedo"]), T(f["normal"]), band.to(device), alpha, succ, sp, prev, opac, pl2, pl1)
+
+
+@pytest.mark.parametrize("win", [11, 7])
+def test_filter_aggregate_equals_plain_sequence(cd, cuda, win):
+    ols1, ols2, alb, nrm, band, alpha, succ, sp, prev, opac, prev_ols1, prev_ols2 = filter_inputs(cd, 96, 128, win, cuda)
+    fused = cd.ops.filter_aggregate(ols1, ols2, alb, nrm, band, alpha, succ, sp, prev, opac, prev_ols1, prev_ols2, win)
+    s1, s2, w1, w2 = cd.ops.spatial_filter(ols1, ols2, alb, nrm, band, win_size=win)
+    agg = cd.ops.aggregation_loss(s1, w1, s2, w2, alpha, succ, sp, prev, opac, ols2, ols1, prev_ols2, prev_ols1)
+    gb = cd.ops.spatial_filter_grad(agg[4], agg[6], agg[5], agg[7], ols1, ols2, alb, nrm, band, win_size=win)
+    torch.cuda.synchronize()
+    assert_equal(N(fused[0]), N(agg[0]), "out_log")
+    assert_equal(N(fused[1]), N(agg[1]), "out")
+    assert float(fused[2]) == float(agg[3]), "avg_loss"
+    assert_equal(N(fused[3]), N(gb), "grad_band")
+    assert_equal(N(fused[4]), N(agg[8]), "grad_alpha")
+
+
+def test_plain_and_fused_steps_agree(cd, cuda):
+    H, W = 128, 192
+    seq = cd.synth.make_sequence(H, W, seed=4, object_motion=2.0)
+    band = cd.synth.random_band((1, H, W), torch.Generator().manual_seed(1)).to(cuda)
+    alpha = torch.full((1, H, W, 1), 0.7, device=cuda)
+    steps = []
+    for fused in (False, True):
+        st = cd.step.FrameStep(cd.step.StepConfig(regression_width=15, fused=fused))
+        st.set_fixed_prediction(band, alpha)
+        outs = [st({k: v.to(cuda) for k, v in seq.frame(t).items()}) for t in range(4)]
+        steps.append(outs)
+    torch.cuda.synchronize()
+    for a, b in zip(*steps):
+        for k in ("out_log", "out", "g_band", "g_alpha", "success"):
+            assert_equal(N(a[k]), N(b[k]), k)
+        assert float(a["avg_loss"]) == float(b["avg_loss"])
+
+
+def test_frames_vs_cpu_oracle(cd, cuda):
+    """Four consecutive frames of the plain step against the same sequence of
+    oracle ops on the CPU.  The reprojection masks match exactly; a value may
+    differ where a near-tie in temporal screening resolves differently after
+    the regression's last-bit differences, so the test bounds that share."""
+    H, W = 96, 128
+    seq = cd.synth.make_sequence(H, W, seed=8, object_motion=2.0)
+    band = cd.synth.random_band((1, H, W), torch.Generator().manual_seed(2))
+    alpha = torch.full((1, H, W, 1), 0.6)
+    st = cd.step.FrameStep(cd.step.StepConfig(regression_width=15))
+    st.set_fixed_prediction(band.to(cuda), alpha.to(cuda))
+    z3 = np.zeros((1, H, W, 3), np.float32)
+    hist = dict(out_log=z3, ols1=z3, ols2=z3, linz=z3, nrm=z3)
+    one = np.ones((1, H, W, 1), np.float32)
+    for t in range(4):
+        fr = {k: v.numpy() for k, v in seq.frame(t).items()}
+        o = st({k: T(v) for k, v in fr.items()})
+        torch.cuda.synchronize()
+        y1, y2 = np.log1p(fr["color"]), np.log1p(fr["color2"])
+        o1, o2, _, _ = orc.cross_regression(y1, y2, fr["albedo"], fr["normal"], 15, 4, 1)
+        s, rep = orc.reproject(fr["mvec"], [hist["out_log"], hist["ols1"], hist["ols2"]], fr["linearZ"],
+                               hist["linz"], fr["normal"], hist["nrm"], fr["pnFwidth"], one, one)
+        assert_equal(N(o["success"]), s, f"frame {t} reprojection mask")
+        ero = orc.erode3x3(s)
+        po, p1, p2, sp = orc.temporal_screening(o1, o2, rep[0], rep[1], rep[2], ero, 7, 1)
+        s1, s2, w1, w2 = orc.spatial_filter(o1, o2, fr["albedo"], fr["normal"], band.numpy(), 11)
+        tt = torch.from_numpy
+        agg = cd.step.aggregation_forward_backward(tt(s1), tt(w1), tt(s2), tt(w2), alpha, tt(ero), tt(sp), tt(po),
+                                                   tt(fr["opacity"]), tt(o2), tt(o1), tt(p2), tt(p1))
+        ol = agg[0].numpy()
+        bad = ~np.isclose(N(o["out_log"]), ol, rtol=1e-4, atol=1e-5)
+        assert bad.mean() < 2e-3, f"frame {t}: {bad.mean():.2e} of values differ"
+        hist = dict(out_log=ol, ols1=o1, ols2=o2, linz=fr["linearZ"], nrm=fr["normal"])

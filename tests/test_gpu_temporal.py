@@ -54,7 +54,8 @@ def test_vs_oracle(cd, cuda, H, W, B, wc, wp):
     f = cd.ops.erode_temporal_screening(*ins, T(mask), wc, wp)
     torch.cuda.synchronize()
     assert_equal(N(me), ero, "erosion")
-    assert 0.3 < ro[3].mean() < 1.0
+    if wc > 1:
+        assert 0.3 < ro[3].mean() < 1.0     # a 1x1 window can never pass the strict overlap test
     for i in range(4):
         assert_equal(N(o[i]), ro[i], f"out{i}")
         assert_equal(N(f[i]), ro[i], f"fused out{i}")
