@@ -27,6 +27,8 @@ SIGNATURES = {
     "cd_get_last_error": (ctypes.c_char_p, []),
     "cd_cross_regression_workspace_size": (_S, [_I, _I, _I, _I]),
     "cd_cross_regression": (_I, [_P] * 8 + [_I] * 6 + [_P, _S, _P]),
+    "cd_cross_regression_noalloc_capacity": (_S, []),
+    "cd_cross_regression_noalloc": (_I, [_P] * 8 + [_I] * 6 + [_P]),
     "cd_spatial_filter": (_I, [_P] * 9 + [_I] * 4 + [_P]),
     "cd_spatial_filter_grad": (_I, [_P] * 10 + [_I] * 4 + [_P]),
     "cd_reproject": (_I, [_P, _I, _P, _P, _P] + [_P] * 8 + [_I] * 3 + [_P]),

@@ -45,6 +45,10 @@ constexpr size_t kSmemLimit = 220 * 1024;
 
 }  // namespace
 
+namespace cd {
+void set_last_error(const char *msg) { snprintf(g_err, sizeof(g_err), "%s", msg); }
+}  // namespace cd
+
 extern "C" {
 
 int cd_abi_version(void) { return 1; }

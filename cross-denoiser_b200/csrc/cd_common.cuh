@@ -80,6 +80,9 @@ cudaError_t launch_temporal(const float *c1, const float *c2, const float *prev,
                             float *out2, float *succ, int B, int H, int W, int win_curr,
                             int win_prev, cudaStream_t st);
 
+// Records msg as the calling thread's cd_get_last_error() message.
+void set_last_error(const char *msg);
+
 struct AggArgs {
     const float *s1, *w1, *s2, *w2, *alpha, *succ, *succ_prev, *prev, *opac, *l1, *l2, *pl1, *pl2;
     float *out_log, *out, *loss, *g_s1, *g_w1, *g_s2, *g_w2, *g_alpha;

@@ -83,6 +83,34 @@ CD_API cd_status cd_cross_regression(const float *imga, const float *imgb,
                               cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* CrossRegression without a workspace (no counterpart in the reference).    */
+/* For callers that cannot allocate device memory when the op runs: a       */
+/* renderer's or engine's frame loop that owns all device memory through its */
+/* own pool and forbids mid-frame allocations (cudaMalloc may synchronise the */
+/* device or fail under memory pressure), or a plugin host that passes       */
+/* tensors in but gives plugins no allocator.  Same arguments and results as */
+/* cd_cross_regression, minus the workspace: the scratch lives in one        */
+/* file-scope device array of CD_NOALLOC_SCRATCH_MIB MiB that the driver     */
+/* allocates when the library is loaded on a device and keeps until the      */
+/* process exits (enough for one 1920x1080 frame at sparsity 4).  Problems   */
+/* needing more scratch than that (cd_cross_regression_workspace_size) fail  */
+/* with CD_ENOMEM.  All calls share the array: calls whose kernels overlap   */
+/* on the GPU race and must be serialised by the caller.  The first call on  */
+/* a device looks up the array's device address; make it before any stream  */
+/* capture.  Nothing in the array needs to start at zero.                    */
+/* ------------------------------------------------------------------------ */
+#define CD_NOALLOC_SCRATCH_MIB 40
+
+CD_API size_t cd_cross_regression_noalloc_capacity(void);
+
+CD_API cd_status cd_cross_regression_noalloc(const float *imga, const float *imgb,
+                                              const float *albedo, const float *normal,
+                                              float *outa, float *outb, float *vara, float *varb,
+                                              int B, int H, int W,
+                                              int win_size, int sparsity, int recon_scale,
+                                              cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
 /* SpatialFilter (forward)                                                    */
 /* Replaces REGISTER_OP("SpatialFilter") + SpatialFilterOp::Compute           */
 /* (ops/regression.cc:59-86, 242-281) and SpatialFilterFunc                   */
