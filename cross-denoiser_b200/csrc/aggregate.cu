@@ -16,6 +16,7 @@
 // pass gives the filtered frame, the loss and dL/dband.
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
+#include "filter_sweep.cuh"
 
 namespace cd {
 namespace {
@@ -166,107 +167,51 @@ __global__ void __launch_bounds__(256) aggregation_kernel(AggPtrs P, int H, int 
 // band partials of the gradient kernel; the epilogue evaluates the loss and
 // its gradient at the pixel and dots it with the partials.
 // ---------------------------------------------------------------------------
-constexpr int kBX = 32, kBY = 8, kPlanes = 12;
-
+template <int HW>
 __global__ void __launch_bounds__(256) filter_aggregate_kernel(
     const float *__restrict__ imga, const float *__restrict__ imgb, const float *__restrict__ albedo,
     const float *__restrict__ normal, const float *__restrict__ band, AggPtrs P,
-    float *__restrict__ gband, int H, int W, int hw, float inv_n)
+    float *__restrict__ gband, int H, int W, int hw_rt, float inv_n)
 {
-    extern __shared__ float sm[];
-    const int tw = kBX + 2 * hw, th = kBY + 2 * hw, plane = tw * th;
-    float *tab = sm + kPlanes * plane;
+    extern __shared__ ulonglong2 tile[];
+    const int hw = HW > 0 ? HW : hw_rt;
+    const int tw = fsw::kBX + 2 * hw, th = fsw::kBY + 2 * hw;
+    fsw::f2 *pdtab = reinterpret_cast<fsw::f2 *>(tile + 3 * tw * th);
     const size_t px = (size_t)H * W, b = blockIdx.z;
-    const float *ia = imga + 3 * px * b, *ib = imgb + 3 * px * b;
-    const float *al = albedo + 3 * px * b, *nr = normal + 3 * px * b;
-    {
-        const int x0 = blockIdx.x * kBX - hw, y0 = blockIdx.y * kBY - hw;
-        const int tid = threadIdx.y * kBX + threadIdx.x;
-        for (int t = tid; t < plane; t += kBX * kBY) {
-            const int ty = t / tw, tx = t - ty * tw;
-            const int gx = min(max(mirror(x0 + tx, W), 0), W - 1);
-            const int gy = min(max(mirror(y0 + ty, H), 0), H - 1);
-            const size_t q = (size_t)gy * W + gx;
-            const float3 a = ld3(ia, q), c = ld3(ib, q), l = ld3(al, q), n = ld3(nr, q);
-            const float v[12] = {a.x, a.y, a.z, c.x, c.y, c.z, l.x, l.y, l.z, n.x, n.y, n.z};
-#pragma unroll
-            for (int k = 0; k < 12; ++k) sm[k * plane + t] = v[k];
-        }
-        for (int k = tid; k <= 2 * hw; k += kBX * kBY) tab[k] = (float)(hw - k) / (float)hw;
-    }
+    fsw::stage(tile, pdtab, imga + 3 * px * b, imgb + 3 * px * b, albedo + 3 * px * b, normal + 3 * px * b,
+               H, W, hw);
     __syncthreads();
 
-    const int cx = blockIdx.x * kBX + threadIdx.x, cy = blockIdx.y * kBY + threadIdx.y;
-    const bool ok = cx < W && cy < H;
+    const int cx = blockIdx.x * fsw::kBX + threadIdx.x, cy = blockIdx.y * fsw::kBY + threadIdx.y;
     float loss = 0.f;
-    if (ok) {
+    if (cx < W && cy < H) {
         const size_t p = b * px + (size_t)cy * W + cx;
-        const float b0 = __ldg(band + 5 * p), b1 = __ldg(band + 5 * p + 1), b2 = __ldg(band + 5 * p + 2);
-        const float b3 = __ldg(band + 5 * p + 3), b4 = __ldg(band + 5 * p + 4);
-        const int co = (threadIdx.y + hw) * tw + threadIdx.x + hw;
-        float c[12];
-#pragma unroll
-        for (int k = 0; k < 12; ++k) c[k] = sm[k * plane + co];
-
-        float aA[3] = {0.f, 0.f, 0.f}, aB[3] = {0.f, 0.f, 0.f}, sA = 0.f, sB = 0.f;
-        float4 pA[4], pB[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            pA[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-            pB[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        for (int ky = 0; ky <= 2 * hw; ++ky) {
-            const float dyf = tab[ky];
-            const int rowo = (threadIdx.y + ky) * tw + threadIdx.x;
-            for (int kx = 0; kx <= 2 * hw; ++kx) {
-                const float dxf = tab[kx];
-                const float pd = dxf * dxf + dyf * dyf;
-                const int o = rowo + kx;
-                float t[12];
-#pragma unroll
-                for (int k = 0; k < 12; ++k) t[k] = sm[k * plane + o];
-                const float dA = norm2(c[0] - t[0], c[1] - t[1], c[2] - t[2]);
-                const float dB = norm2(c[3] - t[3], c[4] - t[4], c[5] - t[5]);
-                const float dAl = norm2(c[6] - t[6], c[7] - t[7], c[8] - t[8]);
-                const float dN = norm2(c[9] - t[9], c[10] - t[10], c[11] - t[11]);
-                const float eA = -b0 * dA - b2 * dAl - b3 * dN - b4 * pd;
-                const float eB = -b1 * dB - b2 * dAl - b3 * dN - b4 * pd;
-                const float wA = __expf(eA), wB = __expf(eB);
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    aA[k] = fmaf(wA, t[k], aA[k]);
-                    aB[k] = fmaf(wB, t[3 + k], aB[k]);
-                }
-                sA += wA;
-                sB += wB;
-                const float kA[4] = {dA, dAl, dN, pd}, kB[4] = {dB, dAl, dN, pd};
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const float da = wA * (-kA[k]), db = wB * (-kB[k]);
-                    pA[k].x = fmaf(da, t[0], pA[k].x);
-                    pA[k].y = fmaf(da, t[1], pA[k].y);
-                    pA[k].z = fmaf(da, t[2], pA[k].z);
-                    pA[k].w += da;
-                    pB[k].x = fmaf(db, t[3], pB[k].x);
-                    pB[k].y = fmaf(db, t[4], pB[k].y);
-                    pB[k].z = fmaf(db, t[5], pB[k].z);
-                    pB[k].w += db;
-                }
-            }
-        }
+        const fsw::Centre c = fsw::centre(tile, hw, band + 5 * p);
+        fsw::Sums s;
+        fsw::zero(s);
+        fsw::sweep<HW, true, true>(tile, pdtab, hw, c, s);
         AggIn in;
+        in.s1[0] = fsw::lo(s.acc_x);
+        in.s1[1] = fsw::lo(s.acc_y);
+        in.s1[2] = fsw::lo(s.acc_z);
+        in.s2[0] = fsw::hi(s.acc_x);
+        in.s2[1] = fsw::hi(s.acc_y);
+        in.s2[2] = fsw::hi(s.acc_z);
+        in.w1 = fsw::lo(s.acc_w);
+        in.w2 = fsw::hi(s.acc_w);
+        // labels crossed as train_step sets them: label1 = ols2, label2 = ols1
+        in.l1[0] = fsw::hi(c.ab_x);
+        in.l1[1] = fsw::hi(c.ab_y);
+        in.l1[2] = fsw::hi(c.ab_z);
+        in.l2[0] = fsw::lo(c.ab_x);
+        in.l2[1] = fsw::lo(c.ab_y);
+        in.l2[2] = fsw::lo(c.ab_z);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            in.s1[k] = aA[k];
-            in.s2[k] = aB[k];
             in.prev[k] = __ldg(P.prev + 3 * p + k);
-            in.l1[k] = c[3 + k];                       // label1 = ols2
-            in.l2[k] = c[k];                           // label2 = ols1
             in.pl1[k] = __ldg(P.pl1 + 3 * p + k);      // prev_label1 = prev_ols2
             in.pl2[k] = __ldg(P.pl2 + 3 * p + k);      // prev_label2 = prev_ols1
         }
-        in.w1 = sA;
-        in.w2 = sB;
         in.alpha = __ldg(P.alpha + p);
         in.succ = __ldg(P.succ + p);
         in.succ_prev = __ldg(P.succ_prev + p);
@@ -276,20 +221,10 @@ __global__ void __launch_bounds__(256) filter_aggregate_kernel(
         st3(P.out, p, make_float3(r.out[0], r.out[1], r.out[2]));
         P.g_alpha[p] = r.g_alpha;
         loss = r.loss;
-        float oA[4], oB[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            oA[k] = fmaf(r.g_w1, pA[k].w, fmaf(r.g_s1[2], pA[k].z, fmaf(r.g_s1[0], pA[k].x, r.g_s1[1] * pA[k].y)));
-            oB[k] = fmaf(r.g_w2, pB[k].w, fmaf(r.g_s2[2], pB[k].z, fmaf(r.g_s2[0], pB[k].x, r.g_s2[1] * pB[k].y)));
-        }
-        float *o = gband + 5 * p;
-        o[0] = oA[0];
-        o[1] = oB[0];
-        o[2] = oA[1] + oB[1];
-        o[3] = oA[2] + oB[2];
-        o[4] = oA[3] + oB[3];
+        fsw::band_grad(s, make_float3(r.g_s1[0], r.g_s1[1], r.g_s1[2]), make_float3(r.g_s2[0], r.g_s2[1], r.g_s2[2]),
+                       r.g_w1, r.g_w2, gband + 5 * p);
     }
-    block_partial(loss, P.partial, kBX * kBY);
+    block_partial(loss, P.partial, fsw::kBX * fsw::kBY);
 }
 
 }  // namespace
@@ -316,11 +251,7 @@ cudaError_t launch_aggregation(const AggArgs &A, float *partial, float *avg, int
     return cudaGetLastError();
 }
 
-size_t filter_aggregate_smem(int win)
-{
-    const int hw = win / 2;
-    return (size_t)kPlanes * (kBX + 2 * hw) * (kBY + 2 * hw) * sizeof(float) + 256 * sizeof(float);
-}
+size_t filter_aggregate_smem(int win) { return fsw::smem_bytes(win / 2); }
 
 cudaError_t launch_filter_aggregate(const float *imga, const float *imgb, const float *albedo,
                                     const float *normal, const float *band, const AggArgs &A, float *gband,
@@ -330,15 +261,22 @@ cudaError_t launch_filter_aggregate(const float *imga, const float *imgb, const 
               nullptr, A.pl1, A.pl2, A.out_log, A.out, nullptr, nullptr, nullptr, nullptr, nullptr,
               A.g_alpha, partial};
     const int hw = win / 2;
-    const size_t smem = filter_aggregate_smem(win);
-    cudaError_t e = cudaFuncSetAttribute(filter_aggregate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
+    const size_t smem = fsw::smem_bytes(hw);
     const float inv_n = 1.f / (3.f * (float)B * (float)H * (float)W);
-    dim3 block(kBX, kBY), grid((W + kBX - 1) / kBX, (H + kBY - 1) / kBY, B);
-    filter_aggregate_kernel<<<grid, block, smem, st>>>(imga, imgb, albedo, normal, band, P, gband, H, W, hw,
-                                                       inv_n);
-    e = cudaGetLastError();
+    dim3 block(fsw::kBX, fsw::kBY), grid((W + fsw::kBX - 1) / fsw::kBX, (H + fsw::kBY - 1) / fsw::kBY, B);
+    auto go = [&](auto kern) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        kern<<<grid, block, smem, st>>>(imga, imgb, albedo, normal, band, P, gband, H, W, hw, inv_n);
+        return cudaGetLastError();
+    };
+    cudaError_t e;
+    switch (hw) {
+    case 3: e = go(filter_aggregate_kernel<3>); break;
+    case 5: e = go(filter_aggregate_kernel<5>); break;
+    case 7: e = go(filter_aggregate_kernel<7>); break;
+    default: e = go(filter_aggregate_kernel<0>); break;
+    }
     if (e != cudaSuccess) return e;
     loss_reduce_kernel<<<1, 1024, 0, st>>>(partial, (int)(grid.x * grid.y * grid.z), inv_n, avg);
     return cudaGetLastError();

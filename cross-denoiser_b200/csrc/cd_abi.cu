@@ -36,7 +36,6 @@ bool dims_ok(int B, int H, int W) { return B >= 1 && B <= 32767 && H >= 1 && W >
 // Shared-memory footprints of the tiled kernels (must agree with the kernel
 // translation units; checked here so that an oversized window is an argument
 // error rather than a launch failure).
-size_t filter_tile_bytes(int hw) { return (size_t)12 * (32 + 2 * hw) * (8 + 2 * hw) * 4 + 1024; }
 size_t temporal_tile_bytes(int hc)
 {
     return ((size_t)6 * (32 + 2 * hc) * (8 + 2 * hc) + (size_t)18 * (8 + 2 * hc) * 32) * 4;
@@ -118,7 +117,7 @@ cd_status cd_spatial_filter(const float *imga, const float *imgb, const float *a
     const int hw = win_size / 2;
     if (hw >= H || hw >= W)
         return fail(CD_EINVAL, "spatial_filter: window radius %d must be smaller than the image (%dx%d)", hw, H, W);
-    if (filter_tile_bytes(hw) > kSmemLimit)
+    if (cd::spatial_filter_smem_bytes(win_size) > kSmemLimit)
         return fail(CD_EINVAL, "spatial_filter: win_size %d exceeds the shared-memory tile", win_size);
     return cuda_status(cd::launch_spatial_filter(imga, imgb, albedo, normal, band, out_acca, out_accb,
                                                  out_wgtsuma, out_wgtsumb, B, H, W, win_size, stream),
@@ -140,7 +139,7 @@ cd_status cd_spatial_filter_grad(const float *grad_acca, const float *grad_accb,
     const int hw = win_size / 2;
     if (hw >= H || hw >= W)
         return fail(CD_EINVAL, "spatial_filter_grad: window radius %d must be smaller than the image (%dx%d)", hw, H, W);
-    if (filter_tile_bytes(hw) > kSmemLimit)
+    if (cd::spatial_filter_smem_bytes(win_size) > kSmemLimit)
         return fail(CD_EINVAL, "spatial_filter_grad: win_size %d exceeds the shared-memory tile", win_size);
     return cuda_status(cd::launch_spatial_filter_grad(grad_acca, grad_accb, grad_wgtsuma, grad_wgtsumb,
                                                       imga, imgb, albedo, normal, band, out_grad_band,

@@ -52,6 +52,7 @@ cudaError_t launch_recon(const float *imga, const float *imgb, const float *albe
 size_t regression_smem_bytes(int win, int sparsity);
 size_t recon_smem_bytes(int win, int sparsity, int recon_scale);
 
+size_t spatial_filter_smem_bytes(int win);
 cudaError_t launch_spatial_filter(const float *imga, const float *imgb, const float *albedo,
                                   const float *normal, const float *band, float *acca,
                                   float *accb, float *wsa, float *wsb, int B, int H, int W,
