@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(256) aggregation_kernel(AggPtrs P, int H, int 
 // its gradient at the pixel and dots it with the partials.
 // ---------------------------------------------------------------------------
 template <int HW>
-__global__ void __launch_bounds__(256) filter_aggregate_kernel(
+__global__ void __launch_bounds__(256, 3) filter_aggregate_kernel(
     const float *__restrict__ imga, const float *__restrict__ imgb, const float *__restrict__ albedo,
     const float *__restrict__ normal, const float *__restrict__ band, AggPtrs P,
     float *__restrict__ gband, int H, int W, int hw_rt, float inv_n)

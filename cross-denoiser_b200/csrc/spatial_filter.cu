@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(256) sf_forward_kernel(
 }
 
 template <int HW>
-__global__ void __launch_bounds__(256) sf_grad_kernel(
+__global__ void __launch_bounds__(256, 3) sf_grad_kernel(
     const float *__restrict__ gacca, const float *__restrict__ gaccb,
     const float *__restrict__ gwsa, const float *__restrict__ gwsb,
     const float *__restrict__ imga, const float *__restrict__ imgb,

@@ -87,6 +87,13 @@ __global__ void __launch_bounds__(256) temporal_kernel(
     const int tid = threadIdx.y * kTX + threadIdx.x;
     const int x0 = blockIdx.x * kTX - hc, y0 = blockIdx.y * kTY - hc;
     const float qnan = __int_as_float(0x7fffffff);
+    // The pixel's history and mask do not depend on the tile: issue their
+    // loads first so their latency overlaps the staging and the row pass.
+    const int cx = blockIdx.x * kTX + threadIdx.x, cy = blockIdx.y * kTY + threadIdx.y;
+    const bool inside = cx < W && cy < H;
+    const size_t p = inside ? (size_t)cy * W + cx : 0;
+    const float3 h0 = ld3(prev, p), h1 = ld3(prev1, p), h2 = ld3(prev2, p);
+    const float m = inside ? (kFused ? eroded_at(raw, cx, cy, H, W) : __ldg(rs + p)) : 0.f;
     for (int t = tid; t < tplane; t += kTX * kTY) {
         const int ty = t / tw, tx = t - ty * tw;
         const int gx = x0 + tx, gy = y0 + ty;
@@ -133,18 +140,12 @@ __global__ void __launch_bounds__(256) temporal_kernel(
     }
     __syncthreads();
 
-    const int cx = blockIdx.x * kTX + threadIdx.x, cy = blockIdx.y * kTY + threadIdx.y;
-    if (cx >= W || cy >= H) return;
-    const size_t p = (size_t)cy * W + cx;
-    const float3 a1 = ld3(cur1, p), a2 = ld3(cur2, p);
+    if (!inside) return;
+    const int co = (threadIdx.y + hc) * tw + threadIdx.x + hc;
+    const float3 a1 = make_float3(tile[co], tile[tplane + co], tile[2 * tplane + co]);
+    const float3 a2 = make_float3(tile[3 * tplane + co], tile[4 * tplane + co], tile[5 * tplane + co]);
     const float3 cu = make_float3((a1.x + a2.x) * 0.5f, (a1.y + a2.y) * 0.5f, (a1.z + a2.z) * 0.5f);
-    float m;
-    if (kFused) {
-        m = eroded_at(raw, cx, cy, H, W);
-        eroded[p] = m;
-    } else {
-        m = __ldg(rs + p);
-    }
+    if (kFused) eroded[p] = m;
     if (m + 1e-4f < 1.f) {
         st3(out, p, cu);
         st3(out1, p, a1);
@@ -178,10 +179,11 @@ __global__ void __launch_bounds__(256) temporal_kernel(
         for (int ix = cx - hp; ix <= cx + hp; ++ix) {
             if (ix < 0 || ix >= W || iy < 0 || iy >= H) continue;
             const size_t q = (size_t)iy * W + ix;
-            const float mq = (kFused ? ((ix == cx && iy == cy) ? m : eroded_at(raw, ix, iy, H, W))
-                                     : __ldg(rs + q));
+            const bool centre = ix == cx && iy == cy;
+            const float mq = centre ? m : (kFused ? eroded_at(raw, ix, iy, H, W) : __ldg(rs + q));
             if (mq < 1.f) continue;
-            const float3 v0 = ld3(prev, q), v1 = ld3(prev1, q), v2 = ld3(prev2, q);
+            const float3 v0 = centre ? h0 : ld3(prev, q), v1 = centre ? h1 : ld3(prev1, q);
+            const float3 v2 = centre ? h2 : ld3(prev2, q);
             const float v[kVals] = {v1.x, v1.y, v1.z, v2.x, v2.y, v2.z, v0.x, v0.y, v0.z};
 #pragma unroll
             for (int k = 0; k < kVals; ++k) {
@@ -199,9 +201,9 @@ __global__ void __launch_bounds__(256) temporal_kernel(
             o = o && (mnP[3 * g + k] < mxC[3 * g + k]) && (mnC[3 * g + k] < mxP[3 * g + k]);
         ok[g] = o;
     }
-    st3(out1, p, ok[0] ? ld3(prev1, p) : a1);
-    st3(out2, p, ok[1] ? ld3(prev2, p) : a2);
-    st3(out, p, ok[2] ? ld3(prev, p) : cu);
+    st3(out1, p, ok[0] ? h1 : a1);
+    st3(out2, p, ok[1] ? h2 : a2);
+    st3(out, p, ok[2] ? h0 : cu);
     succ[p] = ok[2] ? 1.f : 0.f;
 }
 
