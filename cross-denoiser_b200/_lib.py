@@ -27,6 +27,8 @@ SIGNATURES = {
     "cd_get_last_error": (ctypes.c_char_p, []),
     "cd_cross_regression_workspace_size": (_S, [_I, _I, _I, _I]),
     "cd_cross_regression": (_I, [_P] * 8 + [_I] * 6 + [_P, _S, _P]),
+    "cd_cross_regression_grad_workspace_size": (_S, [_I] * 5),
+    "cd_cross_regression_grad": (_I, [_P] * 12 + [_I] * 6 + [_P, _S, _P]),
     "cd_cross_regression_noalloc_capacity": (_S, []),
     "cd_cross_regression_noalloc": (_I, [_P] * 8 + [_I] * 6 + [_P]),
     "cd_spatial_filter": (_I, [_P] * 9 + [_I] * 4 + [_P]),
@@ -45,7 +47,7 @@ SIGNATURES = {
 
 # kernels each entry point launches (for the launch count of bench.py)
 KERNELS_PER_CALL = {
-    "cd_cross_regression": 3, "cd_spatial_filter": 1, "cd_spatial_filter_grad": 1, "cd_reproject": 1,
+    "cd_cross_regression": 3, "cd_cross_regression_grad": 8, "cd_spatial_filter": 1, "cd_spatial_filter_grad": 1, "cd_reproject": 1,
     "cd_erode3x3": 1, "cd_temporal_screening": 1, "cd_erode_temporal_screening": 1,
     "cd_prepare_input": 1, "cd_aggregation_loss": 2, "cd_filter_aggregate": 2,
 }

@@ -61,6 +61,29 @@ size_t cd_cross_regression_workspace_size(int B, int H, int W, int sparsity)
     return ((size_t)2 * B * (H / sparsity) * (W / sparsity) * 18 + (size_t)2 * B * H * W) * sizeof(float);
 }
 
+// Shape and attribute checks shared by CrossRegression's forward and backward.
+static cd_status check_regression(const char *op, int B, int H, int W, int win_size, int sparsity, int recon_scale)
+{
+    if (!dims_ok(B, H, W)) return fail(CD_EINVAL, "%s: bad shape B=%d H=%d W=%d", op, B, H, W);
+    if (win_size < 1 || sparsity < 1 || recon_scale < 1)
+        return fail(CD_EINVAL, "%s: win_size, sparsity and recon_scale must be >= 1", op);
+    if (recon_scale > sparsity)
+        return fail(CD_EINVAL, "recon_scale must be less than or equal to sparsity");
+    if (H % recon_scale != 0 || W % recon_scale != 0)
+        return fail(CD_EINVAL, "Image height and width must be divisible by recon_scale");
+    if (H % sparsity != 0 || W % sparsity != 0)
+        return fail(CD_EINVAL, "%s: image height and width must be divisible by sparsity "
+                               "(got %dx%d, sparsity %d)", op, H, W, sparsity);
+    const int hw = win_size / 2;
+    if (hw >= H || hw >= W)
+        return fail(CD_EINVAL, "%s: window radius %d must be smaller than the image (%dx%d)", op, hw, H, W);
+    if (cd::regression_smem_bytes(win_size, sparsity) > kSmemLimit ||
+        cd::recon_smem_bytes(win_size, sparsity, recon_scale) > kSmemLimit)
+        return fail(CD_EINVAL, "%s: win_size %d with sparsity %d / recon_scale %d exceeds the "
+                               "shared-memory tiles", op, win_size, sparsity, recon_scale);
+    return CD_OK;
+}
+
 cd_status cd_cross_regression(const float *imga, const float *imgb, const float *albedo,
                               const float *normal, float *outa, float *outb, float *vara,
                               float *varb, int B, int H, int W, int win_size, int sparsity,
@@ -70,23 +93,8 @@ cd_status cd_cross_regression(const float *imga, const float *imgb, const float 
     g_err[0] = 0;
     if (!imga || !imgb || !albedo || !normal || !outa || !outb || !vara || !varb)
         return fail(CD_EINVAL, "cross_regression: null tensor pointer");
-    if (!dims_ok(B, H, W)) return fail(CD_EINVAL, "cross_regression: bad shape B=%d H=%d W=%d", B, H, W);
-    if (win_size < 1 || sparsity < 1 || recon_scale < 1)
-        return fail(CD_EINVAL, "cross_regression: win_size, sparsity and recon_scale must be >= 1");
-    if (recon_scale > sparsity)
-        return fail(CD_EINVAL, "recon_scale must be less than or equal to sparsity");
-    if (H % recon_scale != 0 || W % recon_scale != 0)
-        return fail(CD_EINVAL, "Image height and width must be divisible by recon_scale");
-    if (H % sparsity != 0 || W % sparsity != 0)
-        return fail(CD_EINVAL, "cross_regression: image height and width must be divisible by sparsity "
-                               "(got %dx%d, sparsity %d)", H, W, sparsity);
-    const int hw = win_size / 2;
-    if (hw >= H || hw >= W)
-        return fail(CD_EINVAL, "cross_regression: window radius %d must be smaller than the image (%dx%d)", hw, H, W);
-    if (cd::regression_smem_bytes(win_size, sparsity) > kSmemLimit ||
-        cd::recon_smem_bytes(win_size, sparsity, recon_scale) > kSmemLimit)
-        return fail(CD_EINVAL, "cross_regression: win_size %d with sparsity %d / recon_scale %d exceeds the "
-                               "shared-memory tiles", win_size, sparsity, recon_scale);
+    cd_status s = check_regression("cross_regression", B, H, W, win_size, sparsity, recon_scale);
+    if (s != CD_OK) return s;
     const size_t need = cd_cross_regression_workspace_size(B, H, W, sparsity);
     if (workspace_bytes < need || (need > 0 && !workspace))
         return fail(CD_ENOMEM, "cross_regression: workspace of %zu bytes needed, %zu given", need, workspace_bytes);
@@ -94,7 +102,6 @@ cd_status cd_cross_regression(const float *imga, const float *imgb, const float 
     float *beta = static_cast<float *>(workspace);
     float *sda = beta + (size_t)2 * B * (H / sparsity) * (W / sparsity) * 18;
     float *sdb = sda + (size_t)B * H * W;
-    cd_status s;
     if ((s = cuda_status(cd::launch_variance(imga, imgb, vara, varb, sda, sdb, B, H, W, stream), "variance")) != CD_OK)
         return s;
     if ((s = cuda_status(cd::launch_regression(imga, imgb, albedo, normal, vara, varb, sda, sdb, beta, B, H, W,
@@ -102,6 +109,36 @@ cd_status cd_cross_regression(const float *imga, const float *imgb, const float 
         return s;
     return cuda_status(cd::launch_recon(imga, imgb, albedo, normal, vara, varb, sda, sdb, beta, outa, outb, B,
                                         H, W, win_size, sparsity, recon_scale, stream), "recon");
+}
+
+size_t cd_cross_regression_grad_workspace_size(int B, int H, int W, int sparsity, int recon_scale)
+{
+    if (!dims_ok(B, H, W) || sparsity < 1 || recon_scale < 1) return 0;
+    return cd::regression_grad_workspace_floats(B, H, W, sparsity, recon_scale) * sizeof(float);
+}
+
+cd_status cd_cross_regression_grad(const float *imga, const float *imgb, const float *albedo,
+                                   const float *normal, const float *grad_outa, const float *grad_outb,
+                                   const float *grad_vara, const float *grad_varb, float *grad_imga,
+                                   float *grad_imgb, float *grad_albedo, float *grad_normal, int B, int H,
+                                   int W, int win_size, int sparsity, int recon_scale, void *workspace,
+                                   size_t workspace_bytes, cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!imga || !imgb || !albedo || !normal || !grad_outa || !grad_outb || !grad_imga || !grad_imgb ||
+        !grad_albedo || !grad_normal)
+        return fail(CD_EINVAL, "cross_regression_grad: null tensor pointer");
+    cd_status s = check_regression("cross_regression_grad", B, H, W, win_size, sparsity, recon_scale);
+    if (s != CD_OK) return s;
+    const size_t need = cd_cross_regression_grad_workspace_size(B, H, W, sparsity, recon_scale);
+    if (workspace_bytes < need || !workspace)
+        return fail(CD_ENOMEM, "cross_regression_grad: workspace of %zu bytes needed, %zu given", need,
+                    workspace_bytes);
+    return cuda_status(cd::launch_regression_grad(imga, imgb, albedo, normal, grad_outa, grad_outb, grad_vara,
+                                                  grad_varb, grad_imga, grad_imgb, grad_albedo, grad_normal, B, H,
+                                                  W, win_size, sparsity, recon_scale,
+                                                  static_cast<float *>(workspace), stream),
+                       "cross_regression_grad");
 }
 
 cd_status cd_spatial_filter(const float *imga, const float *imgb, const float *albedo,

@@ -43,13 +43,22 @@ cudaError_t launch_variance(const float *imga, const float *imgb, float *vara, f
 cudaError_t launch_regression(const float *imga, const float *imgb, const float *albedo,
                               const float *normal, const float *vara, const float *varb,
                               const float *sda, const float *sdb, float *beta, int B, int H, int W,
-                              int win, int sparsity, cudaStream_t st);
+                              int win, int sparsity, cudaStream_t st, float *chol = nullptr);
 cudaError_t launch_recon(const float *imga, const float *imgb, const float *albedo,
                          const float *normal, const float *vara, const float *varb,
                          const float *sda, const float *sdb, const float *beta, float *outa,
                          float *outb, int B, int H, int W, int win, int sparsity, int recon_scale,
                          cudaStream_t st);
 size_t regression_smem_bytes(int win, int sparsity);
+// CrossRegression backward (regression_grad.cu); ws holds
+// regression_grad_workspace_floats() floats.
+size_t regression_grad_workspace_floats(int B, int H, int W, int sparsity, int recon_scale);
+cudaError_t launch_regression_grad(const float *imga, const float *imgb, const float *albedo,
+                                   const float *normal, const float *g_outa, const float *g_outb,
+                                   const float *g_vara, const float *g_varb, float *g_imga,
+                                   float *g_imgb, float *g_albedo, float *g_normal, int B, int H,
+                                   int W, int win, int sparsity, int recon_scale, float *ws,
+                                   cudaStream_t st);
 size_t recon_smem_bytes(int win, int sparsity, int recon_scale);
 
 size_t spatial_filter_smem_bytes(int win);

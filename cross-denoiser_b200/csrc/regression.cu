@@ -141,7 +141,9 @@ CD_DEV void normal_tap(Normal &n, float3 ft, float3 fc, float3 y, float vt, floa
 // ridge-regularised 6x6 system, in the reference's operation order
 // (ops/regression.cu.cc:206-242, 449-467): diagonal pivots
 // sqrt(max(1e-5, a_ii - s)), off-diagonals (1/L_jj) * (a_ji - s).
-CD_DEV void solve_channel(const Normal &n, int k, float *beta)
+// Lo (nullable) receives the factor, row-major packed lower triangle
+// (21 floats per channel), for the backward pass.
+CD_DEV void solve_channel(const Normal &n, int k, float *beta, float *Lo)
 {
     float A[kP][kP];
     A[0][0] = n.a00; A[0][1] = n.a01[k]; A[0][2] = n.a02[k]; A[0][3] = n.a03; A[0][4] = n.a04; A[0][5] = n.a05;
@@ -166,6 +168,12 @@ CD_DEV void solve_channel(const Normal &n, int k, float *beta)
             else
                 L[i][j] = (1.f / L[j][j]) * (A[j][i] - s);
         }
+    }
+    if (Lo) {
+#pragma unroll
+        for (int i = 0; i < kP; ++i)
+#pragma unroll
+            for (int j = 0; j <= i; ++j) Lo[21 * k + i * (i + 1) / 2 + j] = L[i][j];
     }
     float Y[kP];
     Y[0] = X[0] / L[0][0];
@@ -244,7 +252,7 @@ __global__ void __launch_bounds__(kThreads) regression_kernel(
     const float *__restrict__ albedo, const float *__restrict__ normal,
     const float *__restrict__ vara, const float *__restrict__ varb,
     const float *__restrict__ sda, const float *__restrict__ sdb, float *__restrict__ beta,
-    int H, int W, int hw, int sp)
+    float *__restrict__ chol, int H, int W, int hw, int sp)
 {
     extern __shared__ float4 sm4[];
     const RowGeom g = row_geom(hw, sp);
@@ -344,9 +352,10 @@ __global__ void __launch_bounds__(kThreads) regression_kernel(
     const size_t nb_img = (size_t)Hs * Ws;
     const size_t cidx = (size_t)b * nb_img + (size_t)blockIdx.y * Ws + (i0 + lane);
     float *bo = beta + (size_t)buf * gridDim.z * nb_img * kBeta + cidx * kBeta;
-    solve_channel(nm, 0, bo);
-    solve_channel(nm, 1, bo);
-    solve_channel(nm, 2, bo);
+    float *lo = chol ? chol + ((size_t)buf * gridDim.z * nb_img + cidx) * 63 : nullptr;
+    solve_channel(nm, 0, bo, lo);
+    solve_channel(nm, 1, bo, lo);
+    solve_channel(nm, 2, bo, lo);
 }
 
 // ---------------------------------------------------------------------------
@@ -541,7 +550,7 @@ size_t recon_smem_bytes(int win, int sp, int rs) { return recon_smem(win / 2, sp
 cudaError_t launch_regression(const float *imga, const float *imgb, const float *albedo,
                               const float *normal, const float *vara, const float *varb,
                               const float *sda, const float *sdb, float *beta, int B, int H, int W,
-                              int win, int sp, cudaStream_t st)
+                              int win, int sp, cudaStream_t st, float *chol)
 {
     const int hw = win / 2;
     const size_t smem = regression_smem(hw, sp);
@@ -551,7 +560,7 @@ cudaError_t launch_regression(const float *imga, const float *imgb, const float 
     const int Ws = W / sp, Hs = H / sp;
     dim3 grid((Ws + kCX - 1) / kCX, Hs, B);
     regression_kernel<<<grid, kThreads, smem, st>>>(imga, imgb, albedo, normal, vara, varb, sda, sdb, beta,
-                                                    H, W, hw, sp);
+                                                    chol, H, W, hw, sp);
     return cudaGetLastError();
 }
 

@@ -64,27 +64,26 @@ def _img(t: torch.Tensor, name: str, channels: int | None, ref: torch.Tensor | N
 # ---------------------------------------------------------------------------
 # CrossRegression
 # ---------------------------------------------------------------------------
-def cross_regression(imga, imgb, albedo, normal, win_size: int, sparsity: int,
-                     recon_scale: int = 1, name=None):
-    """(outa, outb, out_vara, out_varb) = cross_regression(imga, imgb, albedo, normal, ...).
-
-    Reference: REGISTER_OP("CrossRegression") ops/regression.cc:25-57 and
-    CrossRegressionFunc ops/regression.cu.cc:477-500.  outa is imgb predicted
-    from imga's features, outb imga from imgb's; out_vara/out_varb are the
-    3x3 variance estimates of imga/imgb.
-    """
+def _regression_args(imga, imgb, albedo, normal, win_size, sparsity, recon_scale):
     imga = _img(imga, "imga", 3)
     imgb = _img(imgb, "imgb", 3, imga)
     albedo = _img(albedo, "albedo", 3, imga)
     normal = _img(normal, "normal", 3, imga)
-    B, H, W, _ = imga.shape
     rs = int(recon_scale)
     if int(win_size) < 1 or int(sparsity) < 1 or rs < 1:
         raise ValueError("win_size, sparsity and recon_scale must be >= 1")
     if rs > int(sparsity):
         raise ValueError("recon_scale must be less than or equal to sparsity")
+    B, H, W, _ = imga.shape
     if H % rs or W % rs:
         raise ValueError("Image height and width must be divisible by recon_scale")
+    return imga, imgb, albedo, normal, rs
+
+
+def _cross_regression_raw(imga, imgb, albedo, normal, win_size, sparsity, recon_scale):
+    imga, imgb, albedo, normal, rs = _regression_args(imga, imgb, albedo, normal, win_size, sparsity,
+                                                      recon_scale)
+    B, H, W, _ = imga.shape
     L = _lib.lib()
     outa = torch.empty((B, H // rs, W // rs, 3), dtype=torch.float32, device=imga.device)
     outb = torch.empty_like(outa)
@@ -97,6 +96,84 @@ def cross_regression(imga, imgb, albedo, normal, win_size: int, sparsity: int,
                                      B, H, W, int(win_size), int(sparsity), rs,
                                      _ptr(ws), nbytes, _stream()), "cross_regression")
     return outa, outb, vara, varb
+
+
+def cross_regression_grad(grad_outa, grad_outb, grad_vara, grad_varb, imga, imgb, albedo, normal,
+                          win_size: int, sparsity: int, recon_scale: int = 1):
+    """(grad_imga, grad_imgb, grad_albedo, grad_normal) of CrossRegression.
+
+    No counterpart in the reference, which registers a gradient only for
+    SpatialFilter (scripts/ops.py:23-32).  The analytic derivative of the
+    forward above; grad_vara / grad_varb may be None.  The forward is
+    recomputed, so only its inputs are needed.
+    """
+    imga, imgb, albedo, normal, rs = _regression_args(imga, imgb, albedo, normal, win_size, sparsity,
+                                                      recon_scale)
+    B, H, W, _ = imga.shape
+    gshape = (B, H // rs, W // rs, 3)
+    grad_outa = _img(grad_outa, "grad_outa", 3)
+    grad_outb = _img(grad_outb, "grad_outb", 3, grad_outa)
+    if tuple(grad_outa.shape) != gshape:
+        raise ValueError(f"grad_outa must have shape {gshape}, got {tuple(grad_outa.shape)}")
+    gv = []
+    for g, nm in ((grad_vara, "grad_vara"), (grad_varb, "grad_varb")):
+        if g is not None:
+            g = _img(g, nm, 1)
+            if tuple(g.shape) != (B, H, W, 1):
+                raise ValueError(f"{nm} must have shape {(B, H, W, 1)}, got {tuple(g.shape)}")
+        gv.append(g)
+    L = _lib.lib()
+    outs = [torch.empty_like(imga) for _ in range(4)]
+    nbytes = L.cd_cross_regression_grad_workspace_size(B, H, W, int(sparsity), rs)
+    ws = torch.empty((max(nbytes, 1),), dtype=torch.uint8, device=imga.device)
+    _lib.check(L.cd_cross_regression_grad(
+        _ptr(imga), _ptr(imgb), _ptr(albedo), _ptr(normal), _ptr(grad_outa), _ptr(grad_outb),
+        None if gv[0] is None else _ptr(gv[0]), None if gv[1] is None else _ptr(gv[1]),
+        *[_ptr(o) for o in outs], B, H, W, int(win_size), int(sparsity), rs, _ptr(ws), nbytes,
+        _stream()), "cross_regression_grad")
+    return tuple(outs)
+
+
+class _CrossRegressionFn(torch.autograd.Function):
+    """Autograd wrapper: forward cd_cross_regression, backward
+    cd_cross_regression_grad."""
+
+    @staticmethod
+    def forward(ctx, imga, imgb, albedo, normal, win_size, sparsity, recon_scale):
+        outs = _cross_regression_raw(imga, imgb, albedo, normal, win_size, sparsity, recon_scale)
+        ctx.save_for_backward(imga, imgb, albedo, normal)
+        ctx.attrs = (int(win_size), int(sparsity), int(recon_scale))
+        return outs
+
+    @staticmethod
+    def backward(ctx, g_outa, g_outb, g_vara, g_varb):
+        imga, imgb, albedo, normal = ctx.saved_tensors
+        B, H, W, _ = imga.shape
+        rs = ctx.attrs[2]
+        if g_outa is None:
+            g_outa = imga.new_zeros((B, H // rs, W // rs, 3))
+        if g_outb is None:
+            g_outb = imga.new_zeros((B, H // rs, W // rs, 3))
+        grads = cross_regression_grad(g_outa, g_outb, g_vara, g_varb, imga, imgb, albedo, normal,
+                                      *ctx.attrs)
+        return (*grads, None, None, None)
+
+
+def cross_regression(imga, imgb, albedo, normal, win_size: int, sparsity: int,
+                     recon_scale: int = 1, name=None):
+    """(outa, outb, out_vara, out_varb) = cross_regression(imga, imgb, albedo, normal, ...).
+
+    Reference: REGISTER_OP("CrossRegression") ops/regression.cc:25-57 and
+    CrossRegressionFunc ops/regression.cu.cc:477-500.  outa is imgb predicted
+    from imga's features, outb imga from imgb's; out_vara/out_varb are the
+    3x3 variance estimates of imga/imgb.  Differentiable with respect to the
+    four images through cross_regression_grad when any of them requires grad.
+    """
+    if torch.is_grad_enabled() and any(isinstance(t, torch.Tensor) and t.requires_grad
+                                       for t in (imga, imgb, albedo, normal)):
+        return _CrossRegressionFn.apply(imga, imgb, albedo, normal, int(win_size), int(sparsity),
+                                        int(recon_scale))
+    return _cross_regression_raw(imga, imgb, albedo, normal, win_size, sparsity, recon_scale)
 
 
 # ---------------------------------------------------------------------------

@@ -83,6 +83,36 @@ CD_API cd_status cd_cross_regression(const float *imga, const float *imgb,
                               cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* CrossRegression backward (no counterpart in the reference, which          */
+/* registers a gradient only for SpatialFilter, scripts/ops.py:23-32; the     */
+/* reference's training step runs the regression outside its GradientTape,  */
+/* scripts/main.py:259-261 vs 289).  The analytic derivative of               */
+/* cd_cross_regression: given dL/d(outa, outb, vara, varb) it returns         */
+/* dL/d(imga, imgb, albedo, normal).  grad_vara / grad_varb may be NULL       */
+/* (no loss on the variances).  It recomputes the forward, so it needs only  */
+/* the forward's inputs.  Same requirements as cd_cross_regression; the      */
+/* workspace holds the recomputed coefficients, their Cholesky factors and   */
+/* the per-pixel partial gradients (with recon_scale 1: 274 floats per      */
+/* pixel at sparsity 1, 55 at sparsity 4).                                    */
+/*  grad_outa, grad_outb : [B,H/recon_scale,W/recon_scale,3]                  */
+/*  grad_vara, grad_varb : [B,H,W,1] or NULL                                  */
+/*  grad_imga, grad_imgb, grad_albedo, grad_normal : [B,H,W,3]                */
+/* ------------------------------------------------------------------------ */
+CD_API size_t cd_cross_regression_grad_workspace_size(int B, int H, int W, int sparsity,
+                                                      int recon_scale);
+
+CD_API cd_status cd_cross_regression_grad(const float *imga, const float *imgb,
+                                          const float *albedo, const float *normal,
+                                          const float *grad_outa, const float *grad_outb,
+                                          const float *grad_vara, const float *grad_varb,
+                                          float *grad_imga, float *grad_imgb,
+                                          float *grad_albedo, float *grad_normal,
+                                          int B, int H, int W,
+                                          int win_size, int sparsity, int recon_scale,
+                                          void *workspace, size_t workspace_bytes,
+                                          cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
 /* CrossRegression without a workspace (no counterpart in the reference).    */
 /* For callers that cannot allocate device memory when the op runs: a       */
 /* renderer's or engine's frame loop that owns all device memory through its */

@@ -1,0 +1,116 @@
+"""CrossRegression backward (cd_cross_regression_grad) against torch.autograd
+through the float64 restatement oracle/regression_fp64.py.
+
+The reference has no gradient for this op, so the FP64 restatement of its
+forward (itself checked against central differences in
+test_oracle_regression_fp64.py) is the oracle.  FP32 gradient vs FP64
+gradient tolerance, per output tensor:
+    |g - g64| <= 5e-4 * max|g64| + 1e-3 * |g64|
+(the forward alone differs from FP64 by up to ~7e-5 relative; the backward
+passes through two 6x6 solves and the reconstruction's quotient; measured
+worst case 7e-5 of max|g64|).
+"""
+import numpy as np
+import pytest
+import torch
+
+from gpu_util import T, N, frames
+from oracle import regression_fp64 as r64
+
+pytestmark = pytest.mark.gpu
+RTOL_MAX, RTOL_EL = 5e-4, 1e-3
+NAMES = ("grad_imga", "grad_imgb", "grad_albedo", "grad_normal")
+
+
+def inputs(cd, H, W, seed, B=1):
+    out = []
+    for b in range(B):
+        _, f = frames(cd, H, W, seed=seed + b)
+        out.append((np.log1p(f["color"]), np.log1p(f["color2"]), f["albedo"], f["normal"]))
+    return [np.concatenate([o[i] for o in out]) for i in range(4)]
+
+
+def upstream(B, H, W, rs, seed, with_var=True):
+    g = np.random.default_rng(seed)
+    go = [g.standard_normal((B, H // rs, W // rs, 3)).astype(np.float32) for _ in range(2)]
+    gv = [g.standard_normal((B, H, W, 1)).astype(np.float32) if with_var else None for _ in range(2)]
+    return go + gv
+
+
+def fp64_grads(ins, ups, win, sp, rs):
+    x = [torch.from_numpy(a).double().requires_grad_(True) for a in ins]
+    outs = r64.cross_regression(*x, win, sp, rs)
+    loss = 0
+    for o, g in zip(outs, ups):
+        if g is not None:
+            loss = loss + (o * torch.from_numpy(g).double()).sum()
+    loss.backward()
+    return [t.grad.numpy() for t in x]
+
+
+def check(got, want, what):
+    for g, w, nm in zip(got, want, NAMES):
+        err = np.abs(g.astype(np.float64) - w)
+        bound = RTOL_MAX * np.abs(w).max() + RTOL_EL * np.abs(w)
+        bad = err > bound
+        assert not bad.any(), (f"{what} {nm}: {bad.sum()} of {bad.size} beyond tolerance, "
+                               f"max err {err.max():.3g}, max|g64| {np.abs(w).max():.3g}")
+
+
+@pytest.mark.parametrize("H,W,win,sp,rs", [(16, 20, 5, 1, 1), (24, 32, 7, 2, 1), (24, 32, 7, 2, 2),
+                                            (32, 40, 9, 4, 1), (32, 40, 11, 4, 2), (24, 32, 5, 4, 4)])
+def test_vs_fp64_autograd(cd, cuda, H, W, win, sp, rs):
+    ins = inputs(cd, H, W, seed=H + win)
+    ups = upstream(1, H, W, rs, seed=win * 7 + sp)
+    got = cd.ops.cross_regression_grad(*[T(u) if u is not None else None for u in ups],
+                                       *[T(a) for a in ins], win, sp, rs)
+    torch.cuda.synchronize()
+    check([N(g) for g in got], fp64_grads(ins, ups, win, sp, rs), f"{H}x{W} win {win} sp {sp} rs {rs}")
+
+
+def test_outputs_only(cd, cuda):
+    """NULL variance gradients: the variances reach the loss only through
+    the regression and the reconstruction."""
+    H, W, win, sp, rs = 24, 32, 7, 2, 1
+    ins = inputs(cd, H, W, seed=3)
+    ups = upstream(1, H, W, rs, seed=4, with_var=False)
+    got = cd.ops.cross_regression_grad(T(ups[0]), T(ups[1]), None, None, *[T(a) for a in ins], win, sp, rs)
+    check([N(g) for g in got], fp64_grads(ins, ups, win, sp, rs), "no variance gradients")
+
+
+def test_batch(cd, cuda):
+    H, W, win, sp, rs = 16, 24, 5, 2, 1
+    ins = inputs(cd, H, W, seed=11, B=2)
+    ups = upstream(2, H, W, rs, seed=12)
+    got = cd.ops.cross_regression_grad(*[T(u) for u in ups], *[T(a) for a in ins], win, sp, rs)
+    check([N(g) for g in got], fp64_grads(ins, ups, win, sp, rs), "batch of 2")
+
+
+def test_autograd_function(cd, cuda):
+    """cross_regression is differentiable through torch.autograd when an
+    input requires grad, and the gradient is cd_cross_regression_grad's."""
+    H, W, win, sp = 16, 20, 5, 2
+    ins = inputs(cd, H, W, seed=21)
+    x = [T(a).requires_grad_(True) for a in ins]
+    outa, outb, va, vb = cd.ops.cross_regression(*x, win_size=win, sparsity=sp)
+    ups = upstream(1, H, W, 1, seed=22)
+    loss = sum((o * T(g)).sum() for o, g in zip((outa, outb, va, vb), ups))
+    loss.backward()
+    direct = cd.ops.cross_regression_grad(*[T(u) for u in ups], *[T(a) for a in ins], win, sp, 1)
+    for t, d in zip(x, direct):
+        np.testing.assert_array_equal(N(t.grad), N(d))
+    # without requires_grad the plain forward runs (no graph)
+    o = cd.ops.cross_regression(*[T(a) for a in ins], win_size=win, sparsity=sp)
+    assert o[0].grad_fn is None
+    np.testing.assert_array_equal(N(o[0]), N(outa.detach()))
+
+
+def test_argument_errors(cd, cuda):
+    ins = [T(a) for a in inputs(cd, 16, 20, seed=1)]
+    g = torch.zeros((1, 16, 20, 3), device="cuda:0")
+    with pytest.raises(ValueError):
+        cd.ops.cross_regression_grad(g[:, :8], g, None, None, *ins, 5, 2, 1)
+    with pytest.raises(ValueError, match="recon_scale"):
+        cd.ops.cross_regression_grad(g, g, None, None, *ins, 5, 2, 4)
+    with pytest.raises(ValueError, match="sparsity"):
+        cd.ops.cross_regression_grad(g, g, None, None, *ins, 5, 3, 1)
