@@ -110,7 +110,9 @@ CD_DEV void stage(ulonglong2 *tile, f2 *pdtab, const float *ia, const float *ib,
     for (int k = tid; k < w * w; k += kBX * kBY) {
         const int ky = k / w, kx = k - ky * w;
         const float dy = (float)(hw - ky) / (float)hw, dx = (float)(hw - kx) / (float)hw;
-        const float pd = dx * dx + dy * dy;   // the reference's expression, contracted alike
+        // dx * dx + dy * dy as the reference's compiled loop rounds it: dy * dy
+        // (outer loop) is hoisted and rounded, dx * dx is fused into the add
+        const float pd = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
         pdtab[k] = pack(pd, pd);
     }
 }
