@@ -276,6 +276,17 @@ def regression_flop(H, W, win, sp):
     return taps * FLOP["regression_tap"] + pairs * FLOP["recon_pair"] + 2 * H * W * FLOP["variance_px"]
 
 
+def unet_flop(H, W):
+    """Tensor-core FLOP of one training step of the U-Net (forward + input and
+    weight gradients of the 3x3 convolutions) at H x W, counting only the
+    real channels (the kernels pad N to 16 and K to 16)."""
+    convs = [(15, 8, 0), (8, 8, 0), (8, 16, 1), (16, 16, 1), (16, 32, 2), (32, 32, 2), (48, 16, 1),
+             (16, 16, 1), (24, 8, 0)]
+    fwd = sum(2 * 9 * ci * co * (H >> l) * (W >> l) for ci, co, l in convs)
+    dgrad = fwd - 2 * 9 * 15 * 8 * H * W
+    return {"forward": fwd, "backward": dgrad + fwd}
+
+
 def cpu_baseline(H, W, win, fwin, seed):
     """The oracle (C, OpenMP over all host threads) on a bounded sample: whole
     1080p frames through the same op sequence, until ~10 s have elapsed."""
@@ -382,6 +393,39 @@ def run_mine(a, rank, world, device):
         e2e_steps = max(1, min(a.steps, 40))
         total, ms = timed_steps(e2e_step, frames, min(a.warmup, 4), e2e_steps, stream)
         total = max_over_ranks(total, world)
+        # full step: the fused ops plus the online-trained U-Net (forward,
+        # backward through band/alpha, Adam), as the reference's train_step
+        net = cd.unet.UNet(device, seed=a.seed)
+        full = stepmod.FrameStep(stepmod.StepConfig(regression_width=a.win, filter_width=a.filter_win, fused=True),
+                                 predictor=net, on_gradients=net.on_gradients)
+        net_ev = {"unet_forward": [], "unet_backward": [], "adam_update": []}
+        orig_m = {"unet_forward": net.forward, "unet_backward": net.backward, "adam_update": net.apply_gradients}
+
+        def timed(name):
+            def f(*args):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                r = orig_m[name](*args)
+                e1.record(stream)
+                net_ev[name].append((e0, e1))
+                return r
+            return f
+        net.forward, net.backward, net.apply_gradients = (timed("unet_forward"), timed("unet_backward"),
+                                                          timed("adam_update"))
+        full.predictor = net.forward
+        if world > 1:
+            torch.distributed.barrier()
+        total, ms = timed_steps(lambda f, t: full(f), frames, a.warmup, a.steps, stream)
+        total = max_over_ranks(total, world)
+        fo = {}
+        for k, evs in net_ev.items():
+            evs = evs[a.warmup:]
+            if evs:
+                fo[k] = round(statistics.mean(e0.elapsed_time(e1) for e0, e1 in evs), 4)
+        res["full_step"] = {"value": world * a.steps / (total * 1e-3), "unit": "frames/s",
+                            "ms_per_step": total / a.steps, "p50_ms": pct(ms, 50), "p99_ms": pct(ms, 99),
+                            "network_ms": fo, "unet_error_flag": net.error_flag(),
+                            "unet_tensor_flop_per_frame": unet_flop(H, W)}
     res["clocks"] = clk.summary()
     h2d = sum(v.numel() * v.element_size() for v in host[0].values())
     res["e2e"] = {"value": world * e2e_steps / (total * 1e-3), "unit": "frames/s", "steps": e2e_steps,
@@ -514,7 +558,7 @@ def main():
                         p99_ms=r["p99_ms"], plain=r["plain"], e2e=r["e2e"], gpu_launches=r["gpu_launches"],
                         roofline=r.get("roofline"), roofline_hbm=r.get("roofline_hbm"), cpu_baseline=cpu,
                         clocks=r["clocks"], per_op_ms=r["per_op_ms"],
-                        sweep_frames_per_s=r.get("sweep_frames_per_s"))
+                        sweep_frames_per_s=r.get("sweep_frames_per_s"), full_step=r.get("full_step"))
             print(json.dumps(line))
     finally:
         if world > 1:

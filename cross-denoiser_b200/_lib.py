@@ -20,6 +20,7 @@ REPROJECT_MAX_LIST = 8
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _S = ctypes.c_size_t
+_F = ctypes.c_float
 
 # name -> (restype, argtypes); mirrors include/cd_ops.h
 SIGNATURES = {
@@ -42,6 +43,15 @@ SIGNATURES = {
     "cd_aggregation_loss": (_I, [_P] * 22 + [_I] * 3 + [_P, _S, _P]),
     "cd_filter_aggregate_workspace_size": (_S, [_I, _I, _I]),
     "cd_filter_aggregate": (_I, [_P] * 17 + [_I] * 4 + [_P, _S, _P]),
+    "cd_unet_param_count": (_S, []),
+    "cd_unet_workspace_size": (_S, [_I] * 3),
+    "cd_unet_forward": (_I, [_P] * 8 + [_I] * 3 + [_P, _S, _P]),
+    "cd_unet_backward": (_I, [_P] * 4 + [_I] * 3 + [_P, _S, _P]),
+    "cd_adam_update": (_I, [_P] * 4 + [_I, _I] + [_F] * 4 + [_P]),
+    "cd_unet_conv3x3_workspace_size": (_S, [_I, _I]),
+    "cd_unet_conv3x3": (_I, [_P] * 4 + [_I] * 6 + [_P, _S, _P]),
+    "cd_unet_conv3x3_wgrad_workspace_size": (_S, [_I] * 5),
+    "cd_unet_conv3x3_wgrad": (_I, [_P] * 3 + [_I] * 5 + [_P, _S, _P]),
     "cd_fp32_fma_probe": (_I, [_P, _I, _I, _P]),
 }
 
@@ -50,6 +60,8 @@ KERNELS_PER_CALL = {
     "cd_cross_regression": 3, "cd_cross_regression_grad": 8, "cd_spatial_filter": 1, "cd_spatial_filter_grad": 1, "cd_reproject": 1,
     "cd_erode3x3": 1, "cd_temporal_screening": 1, "cd_erode_temporal_screening": 1,
     "cd_prepare_input": 1, "cd_aggregation_loss": 2, "cd_filter_aggregate": 2,
+    "cd_unet_forward": 22, "cd_unet_backward": 42, "cd_adam_update": 1, "cd_unet_conv3x3": 2,
+    "cd_unet_conv3x3_wgrad": 2,
 }
 LAUNCHES = {"count": 0}
 

@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
+#include "unet.cuh"
 #include "../../include/cd_ops.h"
 
 namespace {
@@ -338,3 +339,109 @@ cd_status cd_filter_aggregate(const float *ols1, const float *ols2, const float 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// U-Net kernel predictor and Adam
+// ---------------------------------------------------------------------------
+static bool unet_dims_ok(int B, int H, int W)
+{
+    return dims_ok(B, H, W) && H % 4 == 0 && W % 4 == 0 && H <= 4 * 65535;
+}
+
+size_t cd_unet_param_count(void) { return (size_t)cd::unet::param_count(); }
+
+size_t cd_unet_workspace_size(int B, int H, int W)
+{
+    return unet_dims_ok(B, H, W) ? cd::unet::workspace_bytes(B, H, W) : 0;
+}
+
+cd_status cd_unet_forward(const float *ols1, const float *ols2, const float *prev_out, const float *albedo,
+                          const float *normal, const float *params, float *band, float *alpha, int B, int H, int W,
+                          void *workspace, size_t workspace_bytes, cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!ols1 || !ols2 || !prev_out || !albedo || !normal || !params || !band || !alpha)
+        return fail(CD_EINVAL, "unet_forward: null pointer");
+    if (!unet_dims_ok(B, H, W))
+        return fail(CD_EINVAL, "unet_forward: bad shape B=%d H=%d W=%d (H and W must be multiples of 4)", B, H, W);
+    const size_t need = cd::unet::workspace_bytes(B, H, W);
+    if (!workspace || workspace_bytes < need)
+        return fail(CD_ENOMEM, "unet_forward: workspace of %zu bytes needed, %zu given", need, workspace_bytes);
+    return cuda_status(cd::unet::forward(ols1, ols2, prev_out, albedo, normal, params, band, alpha, workspace, B, H,
+                                         W, stream),
+                       "unet_forward");
+}
+
+cd_status cd_unet_backward(const float *grad_band, const float *grad_alpha, const float *params, float *grad_params,
+                           int B, int H, int W, void *workspace, size_t workspace_bytes, cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!grad_band || !grad_alpha || !params || !grad_params) return fail(CD_EINVAL, "unet_backward: null pointer");
+    if (!unet_dims_ok(B, H, W))
+        return fail(CD_EINVAL, "unet_backward: bad shape B=%d H=%d W=%d (H and W must be multiples of 4)", B, H, W);
+    const size_t need = cd::unet::workspace_bytes(B, H, W);
+    if (!workspace || workspace_bytes < need)
+        return fail(CD_ENOMEM, "unet_backward: workspace of %zu bytes needed, %zu given", need, workspace_bytes);
+    return cuda_status(cd::unet::backward(grad_band, grad_alpha, params, grad_params, workspace, B, H, W, stream),
+                       "unet_backward");
+}
+
+cd_status cd_adam_update(float *params, const float *grads, float *m, float *v, int n, int step, float lr,
+                         float beta1, float beta2, float epsilon, cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!params || !grads || !m || !v) return fail(CD_EINVAL, "adam_update: null pointer");
+    if (n < 1 || step < 1) return fail(CD_EINVAL, "adam_update: n and step must be >= 1 (n=%d step=%d)", n, step);
+    return cuda_status(cd::unet::adam(params, grads, m, v, n, step, lr, beta1, beta2, epsilon, stream), "adam_update");
+}
+
+static bool conv_channels_ok(int cin, int cout)
+{
+    const bool ci = cin == 8 || cin == 15 || cin == 16 || cin == 24 || cin == 32 || cin == 48;
+    const bool co = cout == 8 || cout == 16 || cout == 32;
+    return ci && co;
+}
+
+size_t cd_unet_conv3x3_workspace_size(int cin, int cout)
+{
+    return conv_channels_ok(cin, cout) ? cd::unet::conv_layer_workspace(cin, cout) : 0;
+}
+
+cd_status cd_unet_conv3x3(const float *weight, const float *bias, const void *x, void *y, int cin, int cout,
+                          int dgrad, int B, int H, int W, void *workspace, size_t workspace_bytes, cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!weight || !x || !y || (!dgrad && !bias)) return fail(CD_EINVAL, "unet_conv3x3: null pointer");
+    if (!conv_channels_ok(cin, cout)) return fail(CD_EINVAL, "unet_conv3x3: unsupported channels %d -> %d", cin, cout);
+    if (!dims_ok(B, H, W) || H > 4 * 65535) return fail(CD_EINVAL, "unet_conv3x3: bad shape B=%d H=%d W=%d", B, H, W);
+    const size_t need = cd::unet::conv_layer_workspace(cin, cout);
+    if (!workspace || workspace_bytes < need)
+        return fail(CD_ENOMEM, "unet_conv3x3: workspace of %zu bytes needed, %zu given", need, workspace_bytes);
+    return cuda_status(cd::unet::conv_layer(weight, bias, static_cast<const __nv_bfloat16 *>(x),
+                                            static_cast<__nv_bfloat16 *>(y), cin, cout, dgrad ? 1 : 0, B, H, W,
+                                            workspace, stream),
+                       "unet_conv3x3");
+}
+
+size_t cd_unet_conv3x3_wgrad_workspace_size(int cin, int cout, int B, int H, int W)
+{
+    return conv_channels_ok(cin, cout) && dims_ok(B, H, W) ? cd::unet::wgrad_layer_workspace(cin, cout, B, H, W) : 0;
+}
+
+cd_status cd_unet_conv3x3_wgrad(const void *x, const void *dz, float *grad, int cin, int cout, int B, int H, int W,
+                                void *workspace, size_t workspace_bytes, cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!x || !dz || !grad) return fail(CD_EINVAL, "unet_conv3x3_wgrad: null pointer");
+    if (!conv_channels_ok(cin, cout))
+        return fail(CD_EINVAL, "unet_conv3x3_wgrad: unsupported channels %d -> %d", cin, cout);
+    if (!dims_ok(B, H, W) || H > 4 * 65535)
+        return fail(CD_EINVAL, "unet_conv3x3_wgrad: bad shape B=%d H=%d W=%d", B, H, W);
+    const size_t need = cd::unet::wgrad_layer_workspace(cin, cout, B, H, W);
+    if (!workspace || workspace_bytes < need)
+        return fail(CD_ENOMEM, "unet_conv3x3_wgrad: workspace of %zu bytes needed, %zu given", need, workspace_bytes);
+    return cuda_status(cd::unet::wgrad_layer(static_cast<const __nv_bfloat16 *>(x),
+                                             static_cast<const __nv_bfloat16 *>(dz), grad, cin, cout, B, H, W,
+                                             workspace, stream),
+                       "unet_conv3x3_wgrad");
+}

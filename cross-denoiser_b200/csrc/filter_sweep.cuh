@@ -36,12 +36,14 @@ CD_DEV float lo(f2 v)
 {
     float a, b;
     asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+    (void)b;
     return a;
 }
 CD_DEV float hi(f2 v)
 {
     float a, b;
     asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+    (void)a;
     return b;
 }
 CD_DEV f2 fma2(f2 a, f2 b, f2 c)

@@ -1,0 +1,420 @@
+// 3x3 convolutions of the kernel-predicting U-Net on the tensor cores
+// (tcgen05, bf16 operands, fp32 accumulation in TMEM).
+//
+// Layer semantics: Keras Conv2D(kernel_size=3, padding='same') as the
+// reference builds them (scripts/main.py:83-99): cross-correlation with zero
+// padding, kernel layout [ky][kx][cin][cout], bias, ReLU.  The same kernel
+// computes the input gradient (dgrad) of such a layer, as the convolution of
+// the output gradient with the flipped, transposed kernel.
+//
+// Implicit GEMM.  A CTA owns R output rows x 128 pixels.  Its R + 2 input
+// rows (131 pixels: x0-1 .. x0+129) are staged in shared memory as chunk
+// planes: plane c of a row holds channels 8c..8c+7 of every pixel, 16 bytes
+// per pixel.  For output row r the MMA is
+//     D_r[128 px x NOUT] += A[128 px x 16] * B_s[NOUT x 16]^T   per K step s,
+// where A is a 16-byte-shifted view of a staged row (the tap's kx shift) and
+// its 16 K columns are two chunks: either chunks c, c+1 of one tap (LBO =
+// plane size) or the same chunk of taps kx, kx+1 (LBO = 16 bytes: the second
+// chunk is the next pixel).  The host builds the K-step table; the packed B
+// operand holds the matching weights (zero where a step's half is unused).
+// One thread issues all R x steps MMAs, commits them to an mbarrier, and the
+// four warps read their 32 TMEM lanes (one pixel each) for the epilogue.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include "cd_common.cuh"
+#include "tc_sm100.cuh"
+#include "unet.cuh"
+
+namespace cd {
+namespace unet {
+namespace {
+
+constexpr int kPx = 128;                    // pixels per MMA (M)
+constexpr int kStagePx = kPx + 3;           // staged pixels per row
+constexpr int kPlane = kStagePx * 16;       // bytes per chunk plane
+constexpr int kWaitIter = 1 << 22;          // bounded mbarrier polls
+
+__host__ __device__ inline int b_bytes(int nsteps, int nout) { return nsteps * 2 * nout * 16; }
+
+// Dynamic shared memory to request so that no more CTAs share an SM than
+// its 512 TMEM columns hold (228 KB of shared memory per SM): a CTA that
+// cannot allocate would otherwise wait in tcgen05.alloc.
+inline size_t smem_for_tmem(size_t need, int cols)
+{
+    const int per_sm = 512 / cols;
+    const size_t cap = (size_t)233472 / (size_t)(per_sm + 1) + 1024;
+    return need > cap ? need : cap;
+}
+
+__host__ __device__ inline size_t conv_smem(int nsteps, int nout, int nch, int R)
+{
+    return (size_t)b_bytes(nsteps, nout) + (size_t)(R + 2) * nch * kPlane + 16;
+}
+
+template <int NOUT, int R>
+__global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    constexpr int kCols = (R * NOUT <= 32) ? 32 : (R * NOUT <= 64) ? 64 : (R * NOUT <= 128) ? 128
+                                                : (R * NOUT <= 256) ? 256 : 512;
+    static_assert(R * NOUT <= 512, "TMEM holds 512 columns");
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int x0 = blockIdx.x * kPx, y0 = blockIdx.y * R, b = blockIdx.z;
+    const int nch = P.c0 + P.c1;
+    const int bb = b_bytes(P.nsteps, NOUT);
+    uint8_t *sB = smem;
+    uint8_t *sA = smem + bb;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sA + (size_t)(R + 2) * nch * kPlane);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+
+    // stage the packed weights and the input rows (zero outside the image)
+    const uint8_t *wsrc = reinterpret_cast<const uint8_t *>(P.wpack);
+    for (int i = tid; i < bb / 16; i += 128) tc::cp16(sB + 16 * i, wsrc + 16 * i, 16);
+    const size_t HW = (size_t)P.H * P.W;
+    for (int i = tid; i < (R + 2) * nch * kStagePx; i += 128) {
+        const int px = i % kStagePx, t = i / kStagePx;
+        const int c = t % nch, r = t / nch;
+        const int gy = y0 - 1 + r, gx = x0 - 1 + px;
+        const bool in = gy >= 0 && gy < P.H && gx >= 0 && gx < P.W;
+        const size_t pix = b * HW + (size_t)(in ? gy : 0) * P.W + (in ? gx : 0);
+        const __nv_bfloat16 *src = c < P.c0 ? P.src0 + pix * (8 * P.c0) + 8 * c
+                                            : P.src1 + pix * (8 * P.c1) + 8 * (c - P.c0);
+        tc::cp16(sA + (size_t)(r * nch + c) * kPlane + 16 * px, src, in ? 16u : 0u);
+    }
+    if (warp == 0) tc::tmem_alloc(tslot, kCols);
+    if (tid == 0) tc::mbar_init(bar, 1);
+    tc::cp_wait_all();
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = *tslot;
+
+    if (tid == 0) {
+        const uint32_t idesc = tc::idesc_bf16(kPx, NOUT);
+        const uint32_t a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sB);
+        for (int r = 0; r < R; ++r)
+            for (int s = 0; s < P.nsteps; ++s) {
+                const KStep st = P.steps[s];
+                const uint64_t ad = tc::sdesc(a0 + (uint32_t)((r + st.ky) * nch) * kPlane + st.a_off, st.a_lbo, 128);
+                const uint64_t bd = tc::sdesc(b0 + (uint32_t)(s * 2 * NOUT * 16), NOUT * 16, 128);
+                tc::mma_bf16(tbase + r * NOUT, ad, bd, idesc, s > 0 ? 1u : 0u);
+            }
+        tc::commit(bar);
+    }
+    const bool done = tc::mbar_wait(bar, 0, kWaitIter);
+    tc::fence_after_sync();
+    if (!done) {
+        if (tid == 0) atomicExch(P.err, 1);
+    } else {
+        const int x = x0 + tid;
+        const uint32_t lane_base = tbase + ((uint32_t)(warp * 32) << 16);
+        float prev[NOUT];
+        for (int r = 0; r < R; ++r) {
+            float v[NOUT];
+#pragma unroll
+            for (int j = 0; j < NOUT; j += 16) tc::tmem_ld16(lane_base + r * NOUT + j, v + j);
+            const int y = y0 + r;
+            const bool inside = x < P.W && y < P.H;
+            const size_t pix = b * HW + (size_t)(inside ? y : 0) * P.W + (inside ? x : 0);
+            if (P.bias) {
+#pragma unroll
+                for (int j = 0; j < NOUT; ++j) v[j] += __ldg(P.bias + j);
+            }
+            if (P.relu) {
+#pragma unroll
+                for (int j = 0; j < NOUT; ++j) v[j] = fmaxf(v[j], 0.f);
+            }
+            if (inside) {
+                // dgrad: multiply by the ReLU derivative of the layer below
+                // (mask0 / mask1 laid out like dst0 / dst1; null = no ReLU)
+#pragma unroll
+                for (int c = 0; c < NOUT / 8; ++c) {
+                    if (c >= P.d0 + P.d1) break;
+                    const __nv_bfloat16 *m = c < P.d0 ? (P.mask0 ? P.mask0 + pix * (8 * P.d0) + 8 * c : nullptr)
+                                                      : (P.mask1 ? P.mask1 + pix * (8 * P.d1) + 8 * (c - P.d0) : nullptr);
+                    if (!m) continue;
+                    const uint4 raw = *reinterpret_cast<const uint4 *>(m);
+                    const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(&raw);
+#pragma unroll
+                    for (int e = 0; e < 8; ++e)
+                        if (!(__bfloat162float(mb[e]) > 0.f)) v[8 * c + e] = 0.f;
+                }
+            }
+            if (inside) {
+#pragma unroll
+                for (int c = 0; c < NOUT / 8; ++c) {
+                    if (c >= P.d0 + P.d1) break;
+                    uint4 o;
+                    __nv_bfloat162 *ob = reinterpret_cast<__nv_bfloat162 *>(&o);
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) ob[e] = __floats2bfloat162_rn(v[8 * c + 2 * e], v[8 * c + 2 * e + 1]);
+                    __nv_bfloat16 *d = c < P.d0 ? P.dst0 + pix * (8 * P.d0) + 8 * c
+                                                : P.dst1 + pix * (8 * P.d1) + 8 * (c - P.d0);
+                    *reinterpret_cast<uint4 *>(d) = o;
+                }
+            }
+            if (P.pool) {
+                // fused 2x2 max pooling (rows y0 + r - 1, y0 + r; lanes x, x ^ 1),
+                // on the bf16-rounded outputs, as the stored activations are
+                if (r & 1) {
+#pragma unroll
+                    for (int j = 0; j < NOUT; ++j) {
+                        float m = fmaxf(__bfloat162float(__float2bfloat16_rn(prev[j])),
+                                        __bfloat162float(__float2bfloat16_rn(v[j])));
+                        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
+                        prev[j] = m;
+                    }
+                    const int py = y / 2, px = x / 2, PH = P.H / 2, PW = P.W / 2;
+                    if (!(tid & 1) && py < PH && px < PW) {
+                        const size_t q = b * (size_t)PH * PW + (size_t)py * PW + px;
+#pragma unroll
+                        for (int c = 0; c < NOUT / 8; ++c) {
+                            if (c >= P.d0) break;
+                            uint4 o;
+                            __nv_bfloat162 *ob = reinterpret_cast<__nv_bfloat162 *>(&o);
+#pragma unroll
+                            for (int e = 0; e < 4; ++e)
+                                ob[e] = __floats2bfloat162_rn(prev[8 * c + 2 * e], prev[8 * c + 2 * e + 1]);
+                            *reinterpret_cast<uint4 *>(P.pool + q * (8 * P.d0) + 8 * c) = o;
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < NOUT; ++j) prev[j] = v[j];
+                }
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tbase, kCols);
+}
+
+template <int NOUT, int R>
+cudaError_t launch_t(const ConvParams &P, int B, cudaStream_t st)
+{
+    constexpr int kCols = (R * NOUT <= 32) ? 32 : (R * NOUT <= 64) ? 64 : (R * NOUT <= 128) ? 128
+                                                : (R * NOUT <= 256) ? 256 : 512;
+    const size_t smem = smem_for_tmem(conv_smem(P.nsteps, NOUT, P.c0 + P.c1, R), kCols);
+    cudaError_t e = cudaFuncSetAttribute(conv3x3_kernel<NOUT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid((P.W + kPx - 1) / kPx, (P.H + R - 1) / R, B);
+    conv3x3_kernel<NOUT, R><<<grid, 128, smem, st>>>(P);
+    return cudaGetLastError();
+}
+
+// Packed B operand: per step s, half h, conv output row n, element e
+// (dst[((s * 2 + h) * nout + n) * 8 + e]) the weight of tap (ky, kx) from
+// conv input channel 8 * chunk + e to conv output channel n.
+__global__ void pack_kernel(const float *__restrict__ w, __nv_bfloat16 *__restrict__ dst, const PackTable T)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.nsteps * 2 * T.nout * 8) return;
+    const int e = i & 7, n = (i >> 3) % T.nout, h = (i / (8 * T.nout)) & 1, s = i / (16 * T.nout);
+    const StepHalf hf = T.half[s][h];
+    float v = 0.f;
+    if (hf.chunk >= 0) {
+        const int ci = 8 * hf.chunk + e;
+        if (!T.dgrad) {
+            if (ci < T.cin && n < T.cout) v = w[((hf.ky * 3 + hf.kx) * T.cin + ci) * T.cout + n];
+        } else {
+            // conv of dZ: input channel = layer output ci, output channel = layer input n, flipped taps
+            if (ci < T.cout && n < T.cin) v = w[(((2 - hf.ky) * 3 + (2 - hf.kx)) * T.cin + n) * T.cout + ci];
+        }
+    }
+    dst[i] = __float2bfloat16_rn(v);
+}
+
+// Weight gradient.  D_tap[cin x cout] = sum_p X[p + tap][cin] dZ[p][cout]:
+// M = input channels (128 rows: the chunk planes of X from chunk 0 on, rows
+// past cin read other staged data and are discarded), N = output channels
+// padded to NZ, K = 16 consecutive pixels per MMA; both operands MN-major
+// (channels contiguous, pixels 16 bytes apart).  Nine accumulators, one per
+// tap.  A CTA covers R rows x 128 pixels and writes its partial sums.
+constexpr int kZPlane = kPx * 16;
+
+__host__ __device__ inline size_t wgrad_smem(int nch, int zc, int R)
+{
+    return (size_t)((R + 2) * nch + 16) * kPlane + (size_t)(R * zc + 4) * kZPlane + 16;
+}
+
+template <int NZ, int R>
+__global__ void __launch_bounds__(128) wgrad_kernel(const WgradParams P)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    constexpr int kCols = 9 * NZ <= 256 ? 256 : 512;
+    static_assert(9 * NZ <= 512, "nine accumulators of NZ columns");
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int x0 = blockIdx.x * kPx, y0 = blockIdx.y * R, b = blockIdx.z;
+    const int tile = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    const int nch = P.xc0 + P.xc1;
+    uint8_t *sX = smem;
+    uint8_t *sZ = sX + (size_t)((R + 2) * nch + 16) * kPlane;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sZ + (size_t)(R * P.zc + 4) * kZPlane);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+    const size_t HW = (size_t)P.H * P.W;
+
+    for (int i = tid; i < (R + 2) * nch * kStagePx; i += 128) {
+        const int px = i % kStagePx, t = i / kStagePx;
+        const int c = t % nch, r = t / nch;
+        const int gy = y0 - 1 + r, gx = x0 - 1 + px;
+        const bool in = gy >= 0 && gy < P.H && gx >= 0 && gx < P.W;
+        const size_t pix = b * HW + (size_t)(in ? gy : 0) * P.W + (in ? gx : 0);
+        const __nv_bfloat16 *src = c < P.xc0 ? P.x0 + pix * (8 * P.xc0) + 8 * c
+                                             : P.x1 + pix * (8 * P.xc1) + 8 * (c - P.xc0);
+        tc::cp16(sX + (size_t)(r * nch + c) * kPlane + 16 * px, src, in ? 16u : 0u);
+    }
+    for (int i = tid; i < R * P.zc * kPx; i += 128) {
+        const int px = i % kPx, t = i / kPx;
+        const int c = t % P.zc, r = t / P.zc;
+        const int gy = y0 + r, gx = x0 + px;
+        const bool in = gy < P.H && gx < P.W;
+        const size_t pix = b * HW + (size_t)(in ? gy : 0) * P.W + (in ? gx : 0);
+        tc::cp16(sZ + (size_t)(r * P.zc + c) * kZPlane + 16 * px, P.dz + pix * (8 * P.zc) + 8 * c, in ? 16u : 0u);
+    }
+    if (warp == 0) tc::tmem_alloc(tslot, kCols);
+    if (tid == 0) tc::mbar_init(bar, 1);
+    tc::cp_wait_all();
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = *tslot;
+
+    if (tid == 0) {
+        const uint32_t idesc = tc::idesc_bf16(kPx, NZ) | (1u << 15) | (1u << 16);   // A and B MN-major
+        const uint32_t ax = tc::smem_u32(sX), az = tc::smem_u32(sZ);
+        for (int r = 0; r < R; ++r)
+            for (int g = 0; g < kPx / 16; ++g) {
+                const uint64_t bd = tc::sdesc(az + (uint32_t)(r * P.zc) * kZPlane + 256u * g, 128, kZPlane);
+                for (int tap = 0; tap < 9; ++tap) {
+                    const int ky = tap / 3, kx = tap - 3 * ky;
+                    const uint32_t a = ax + (uint32_t)((r + ky) * nch) * kPlane + (uint32_t)(kx + 16 * g) * 16;
+                    tc::mma_bf16(tbase + tap * NZ, tc::sdesc(a, 128, kPlane), bd, idesc, (r | g) ? 1u : 0u);
+                }
+            }
+        tc::commit(bar);
+    }
+    const bool done = tc::mbar_wait(bar, 0, kWaitIter);
+    tc::fence_after_sync();
+    float *out = P.partial + (size_t)tile * (9 * P.cin * P.cout + P.cout);
+    if (!done) {
+        if (tid == 0) atomicExch(P.err, 1);
+    } else {
+        if (warp * 32 < P.cin) {
+            const int m = warp * 32 + (tid & 31);
+            for (int tap = 0; tap < 9; ++tap)
+#pragma unroll
+                for (int j = 0; j < NZ; j += 16) {
+                    float v[16];
+                    tc::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + tap * NZ + j, v);
+                    if (m < P.cin)
+#pragma unroll
+                        for (int q = 0; q < 16; ++q)
+                            if (j + q < P.cout) out[(tap * P.cin + m) * P.cout + j + q] = v[q];
+                }
+        }
+        if (tid < P.cout) {
+            // bias gradient: the tile's sum of dZ for channel tid
+            float s = 0.f;
+            const int c = tid >> 3, e = tid & 7;
+            for (int r = 0; r < R; ++r) {
+                const __nv_bfloat16 *row =
+                    reinterpret_cast<const __nv_bfloat16 *>(sZ + (size_t)(r * P.zc + c) * kZPlane) + e;
+                for (int px = 0; px < kPx; ++px) s += __bfloat162float(row[8 * px]);
+            }
+            out[9 * P.cin * P.cout + tid] = s;
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tbase, kCols);
+}
+
+constexpr int kWgradRows = 4;
+
+template <int NZ>
+cudaError_t launch_wgrad_t(const WgradParams &P, int B, cudaStream_t st)
+{
+    const size_t smem = smem_for_tmem(wgrad_smem(P.xc0 + P.xc1, P.zc, kWgradRows), 9 * NZ <= 256 ? 256 : 512);
+    cudaError_t e = cudaFuncSetAttribute(wgrad_kernel<NZ, kWgradRows>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid((P.W + kPx - 1) / kPx, (P.H + kWgradRows - 1) / kWgradRows, B);
+    wgrad_kernel<NZ, kWgradRows><<<grid, 128, smem, st>>>(P);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+int conv_rows(int nout, int nch) { return nout >= 32 ? 4 : (nch > 4 ? 4 : 8); }
+
+size_t conv_smem_bytes(int nsteps, int nout, int nch) { return conv_smem(nsteps, nout, nch, conv_rows(nout, nch)); }
+
+// K-step table for `nch` input chunks (8 channels each): channel pairs of
+// every tap, then, for an odd last chunk, tap pairs (kx, kx+1) with the
+// second half of (ky, 2, 3) unused.  half[h] = (ky, kx, chunk) or chunk -1.
+int build_steps(int nch, KStep *steps, StepHalf (*half)[2])
+{
+    int n = 0;
+    for (int c = 0; c + 1 < nch; c += 2)
+        for (int ky = 0; ky < 3; ++ky)
+            for (int kx = 0; kx < 3; ++kx) {
+                steps[n] = KStep{ky, c * kPlane + kx * 16, kPlane, 0};
+                half[n][0] = StepHalf{ky, kx, c};
+                half[n][1] = StepHalf{ky, kx, c + 1};
+                ++n;
+            }
+    if (nch & 1) {
+        const int c = nch - 1;
+        for (int ky = 0; ky < 3; ++ky)
+            for (int kx = 0; kx < 3; kx += 2) {
+                steps[n] = KStep{ky, c * kPlane + kx * 16, 16, 0};
+                half[n][0] = StepHalf{ky, kx, c};
+                half[n][1] = kx + 1 < 3 ? StepHalf{ky, kx + 1, c} : StepHalf{0, 0, -1};
+                ++n;
+            }
+    }
+    return n;
+}
+
+cudaError_t launch_conv3x3(const ConvParams &P, int B, int nout, cudaStream_t st)
+{
+    const int nch = P.c0 + P.c1;
+    if (nout == 16) return conv_rows(16, nch) == 8 ? launch_t<16, 8>(P, B, st) : launch_t<16, 4>(P, B, st);
+    if (nout == 32) return launch_t<32, 4>(P, B, st);
+    if (nout == 48) return launch_t<48, 4>(P, B, st);
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace unet
+}  // namespace cd
+
+namespace cd {
+namespace unet {
+
+cudaError_t launch_pack(const float *w, __nv_bfloat16 *dst, const PackTable &T, cudaStream_t st)
+{
+    const int n = T.nsteps * 2 * T.nout * 8;
+    pack_kernel<<<(n + 255) / 256, 256, 0, st>>>(w, dst, T);
+    return cudaGetLastError();
+}
+
+size_t wgrad_tiles(int B, int H, int W) { return (size_t)B * ((W + kPx - 1) / kPx) * ((H + kWgradRows - 1) / kWgradRows); }
+
+size_t wgrad_partial_floats(int B, int H, int W, int cin, int cout)
+{
+    return wgrad_tiles(B, H, W) * (size_t)(9 * cin * cout + cout);
+}
+
+cudaError_t launch_wgrad(const WgradParams &P, int B, cudaStream_t st)
+{
+    if (P.cout <= 16) return launch_wgrad_t<16>(P, B, st);
+    if (P.cout <= 32) return launch_wgrad_t<32>(P, B, st);
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace unet
+}  // namespace cd

@@ -1,0 +1,409 @@
+// The U-Net's non-convolution layers, their backward passes, the gradient
+// reductions and the optimizer (scripts/main.py:74-118, 300-303):
+//   input packing      Concatenate of the five 3-channel inputs (:101-102)
+//   Conv2DTranspose    kernel 1, stride 2, 'same' (:92, :96): out[2i,2j] =
+//                      K x[i,j] + b, every other position b; Keras kernel
+//                      layout [1][1][cout][cin]
+//   head               Conv2D(6, 1) in fp32, band = 1 / (p^2 + 1e-4),
+//                      alpha = sigmoid (:106-111)
+//   max-pool backward  the gradient goes to the first maximum of each 2x2
+//                      window (row-major), added to the skip connection's
+//                      gradient, times the ReLU derivative
+//   Adam               Keras semantics: m += (g - m)(1 - b1),
+//                      v += (g^2 - v)(1 - b2),
+//                      w -= lr sqrt(1 - b2^t) / (1 - b1^t) m / (sqrt(v) + eps)
+// Per-block partial sums of the parameter gradients are reduced in a fixed
+// order by reduce_kernel, so the gradients are deterministic.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include "cd_common.cuh"
+#include "unet_ops.cuh"
+
+namespace cd {
+namespace unet {
+namespace {
+
+CD_DEV void ld8(const __nv_bfloat16 *p, float *v)
+{
+    const uint4 raw = *reinterpret_cast<const uint4 *>(p);
+    const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&raw);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const float2 f = __bfloat1622float2(h[e]);
+        v[2 * e] = f.x;
+        v[2 * e + 1] = f.y;
+    }
+}
+CD_DEV void st8(__nv_bfloat16 *p, const float *v)
+{
+    uint4 o;
+    __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&o);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) h[e] = __floats2bfloat162_rn(v[2 * e], v[2 * e + 1]);
+    *reinterpret_cast<uint4 *>(p) = o;
+}
+
+// [ols1, ols2, prev_out, albedo, normal] (fp32, 3 channels each) -> bf16, 16 channels (15 + zero)
+__global__ void __launch_bounds__(256) pack_input_kernel(const float *__restrict__ a, const float *__restrict__ b,
+                                                         const float *__restrict__ c, const float *__restrict__ d,
+                                                         const float *__restrict__ e, __nv_bfloat16 *__restrict__ x,
+                                                         size_t n)
+{
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    float v[16];
+    const float *src[5] = {a, b, c, d, e};
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        v[3 * k] = __ldg(src[k] + 3 * p);
+        v[3 * k + 1] = __ldg(src[k] + 3 * p + 1);
+        v[3 * k + 2] = __ldg(src[k] + 3 * p + 2);
+    }
+    v[15] = 0.f;
+    st8(x + 16 * p, v);
+    st8(x + 16 * p + 8, v + 8);
+}
+
+// Conv2DTranspose(kernel 1, stride 2) forward, one thread per output pixel.
+template <int CI, int CO>
+__global__ void __launch_bounds__(256) tconv_fwd_kernel(const __nv_bfloat16 *__restrict__ in,
+                                                        const float *__restrict__ K, const float *__restrict__ bias,
+                                                        __nv_bfloat16 *__restrict__ out, int Hi, int Wi, int B)
+{
+    __shared__ float sK[CO * CI + CO];
+    for (int i = threadIdx.x; i < CO * CI + CO; i += blockDim.x) sK[i] = i < CO * CI ? K[i] : bias[i - CO * CI];
+    __syncthreads();
+    const int Ho = 2 * Hi, Wo = 2 * Wi;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (size_t)B * Ho * Wo) return;
+    const int xo = (int)(q % Wo), yo = (int)((q / Wo) % Ho), b = (int)(q / ((size_t)Wo * Ho));
+    float o[CO];
+#pragma unroll
+    for (int c = 0; c < CO; ++c) o[c] = sK[CO * CI + c];
+    if (!(xo & 1) && !(yo & 1)) {
+        const size_t p = ((size_t)b * Hi + yo / 2) * Wi + xo / 2;
+        float x[CI];
+#pragma unroll
+        for (int c = 0; c < CI; c += 8) ld8(in + p * CI + c, x + c);
+#pragma unroll
+        for (int co = 0; co < CO; ++co)
+#pragma unroll
+            for (int ci = 0; ci < CI; ++ci) o[co] = fmaf(sK[co * CI + ci], x[ci], o[co]);
+    }
+#pragma unroll
+    for (int c = 0; c < CO; c += 8) st8(out + q * CO + c, o + c);
+}
+
+// Conv2DTranspose backward: a block of kN input pixels computes
+// d_in = K^T d_out[2i,2j] (times the ReLU derivative of `in`), and the
+// block's partial sums of dK[co][ci] and db[co] (db over all four output
+// positions of each input pixel).
+template <int CI, int CO, int kN>
+__global__ void __launch_bounds__(kN) tconv_bwd_kernel(const __nv_bfloat16 *__restrict__ in,
+                                                        const __nv_bfloat16 *__restrict__ dout,
+                                                        const float *__restrict__ K,
+                                                        __nv_bfloat16 *__restrict__ dz_in, float *__restrict__ partial,
+                                                        int Hi, int Wi, int B)
+{
+    __shared__ float sK[CO * CI];
+    __shared__ float sx[kN][CI + 1], sd[kN][CO + 1], sb[kN][CO + 1];
+    for (int i = threadIdx.x; i < CO * CI; i += blockDim.x) sK[i] = K[i];
+    const size_t n = (size_t)B * Hi * Wi;
+    const size_t p = (size_t)blockIdx.x * kN + threadIdx.x;
+    const int t = threadIdx.x;
+    float x[CI], d[CO];
+#pragma unroll
+    for (int c = 0; c < CI; ++c) x[c] = 0.f;
+#pragma unroll
+    for (int c = 0; c < CO; ++c) d[c] = 0.f;
+    float bsum[CO];
+#pragma unroll
+    for (int c = 0; c < CO; ++c) bsum[c] = 0.f;
+    if (p < n) {
+        const int xi = (int)(p % Wi), yi = (int)((p / Wi) % Hi), b = (int)(p / ((size_t)Wi * Hi));
+#pragma unroll
+        for (int c = 0; c < CI; c += 8) ld8(in + p * CI + c, x + c);
+        const int Wo = 2 * Wi;
+        for (int a = 0; a < 4; ++a) {
+            const size_t q = ((size_t)b * 2 * Hi + 2 * yi + (a >> 1)) * Wo + 2 * xi + (a & 1);
+            float g[CO];
+#pragma unroll
+            for (int c = 0; c < CO; c += 8) ld8(dout + q * CO + c, g + c);
+#pragma unroll
+            for (int c = 0; c < CO; ++c) {
+                bsum[c] += g[c];
+                if (a == 0) d[c] = g[c];
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < CI; ++c) sx[t][c] = x[c];
+#pragma unroll
+    for (int c = 0; c < CO; ++c) {
+        sd[t][c] = d[c];
+        sb[t][c] = bsum[c];
+    }
+    __syncthreads();
+    if (p < n) {
+        float g[CI];
+#pragma unroll
+        for (int ci = 0; ci < CI; ++ci) {
+            float s = 0.f;
+#pragma unroll
+            for (int co = 0; co < CO; ++co) s = fmaf(sK[co * CI + ci], d[co], s);
+            g[ci] = x[ci] > 0.f ? s : 0.f;
+        }
+#pragma unroll
+        for (int c = 0; c < CI; c += 8) st8(dz_in + p * CI + c, g + c);
+    }
+    float *out = partial + (size_t)blockIdx.x * (CO * CI + CO);
+    for (int j = t; j < CO * CI + CO; j += kN) {
+        float s = 0.f;
+        if (j < CO * CI) {
+            const int co = j / CI, ci = j - co * CI;
+            for (int k = 0; k < kN; ++k) s = fmaf(sd[k][co], sx[k][ci], s);
+        } else {
+            const int co = j - CO * CI;
+            for (int k = 0; k < kN; ++k) s += sb[k][co];
+        }
+        out[j] = s;
+    }
+}
+
+// Head: param = Kh^T c5_1 + bh (Kh[ci][co], 8 x 6), band = 1 / (p^2 + 1e-4), alpha = sigmoid(p5)
+__global__ void __launch_bounds__(256) head_fwd_kernel(const __nv_bfloat16 *__restrict__ x, const float *__restrict__ K,
+                                                       const float *__restrict__ bias, float *__restrict__ band,
+                                                       float *__restrict__ alpha, size_t n)
+{
+    __shared__ float sK[54];
+    if (threadIdx.x < 54) sK[threadIdx.x] = threadIdx.x < 48 ? K[threadIdx.x] : bias[threadIdx.x - 48];
+    __syncthreads();
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    float v[8];
+    ld8(x + 8 * p, v);
+    float q[6];
+#pragma unroll
+    for (int co = 0; co < 6; ++co) {
+        float s = sK[48 + co];
+#pragma unroll
+        for (int ci = 0; ci < 8; ++ci) s = fmaf(sK[ci * 6 + co], v[ci], s);
+        q[co] = s;
+    }
+#pragma unroll
+    for (int k = 0; k < 5; ++k) band[5 * p + k] = 1.f / (q[k] * q[k] + 1e-4f);
+    alpha[p] = 1.f / (1.f + expf(-q[5]));
+}
+
+// Head backward: dZ of c5_1 (times its ReLU derivative) and the block's
+// partial sums of dKh[ci][co] and dbh[co].
+__global__ void __launch_bounds__(128) head_bwd_kernel(const __nv_bfloat16 *__restrict__ x, const float *__restrict__ K,
+                                                       const float *__restrict__ bias, const float *__restrict__ gband,
+                                                       const float *__restrict__ galpha, __nv_bfloat16 *__restrict__ dz,
+                                                       float *__restrict__ partial, size_t n)
+{
+    constexpr int kN = 128;
+    __shared__ float sK[54];
+    __shared__ float sx[kN][9], sg[kN][7];
+    if (threadIdx.x < 54) sK[threadIdx.x] = threadIdx.x < 48 ? K[threadIdx.x] : bias[threadIdx.x - 48];
+    __syncthreads();
+    const int t = threadIdx.x;
+    const size_t p = (size_t)blockIdx.x * kN + t;
+    float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, g[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (p < n) {
+        ld8(x + 8 * p, v);
+#pragma unroll
+        for (int co = 0; co < 6; ++co) {
+            float s = sK[48 + co];
+#pragma unroll
+            for (int ci = 0; ci < 8; ++ci) s = fmaf(sK[ci * 6 + co], v[ci], s);
+            if (co < 5) {
+                const float den = s * s + 1e-4f;
+                g[co] = __ldg(gband + 5 * p + co) * (-2.f * s / (den * den));
+            } else {
+                const float a = 1.f / (1.f + expf(-s));
+                g[co] = __ldg(galpha + p) * a * (1.f - a);
+            }
+        }
+        float d[8];
+#pragma unroll
+        for (int ci = 0; ci < 8; ++ci) {
+            float s = 0.f;
+#pragma unroll
+            for (int co = 0; co < 6; ++co) s = fmaf(sK[ci * 6 + co], g[co], s);
+            d[ci] = v[ci] > 0.f ? s : 0.f;
+        }
+        st8(dz + 8 * p, d);
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) sx[t][c] = v[c];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) sg[t][c] = g[c];
+    __syncthreads();
+    if (t < 54) {
+        float s = 0.f;
+        if (t < 48) {
+            const int ci = t / 6, co = t - 6 * ci;
+            for (int k = 0; k < kN; ++k) s = fmaf(sx[k][ci], sg[k][co], s);
+        } else {
+            for (int k = 0; k < kN; ++k) s += sg[k][t - 48];
+        }
+        partial[(size_t)blockIdx.x * 54 + t] = s;
+    }
+}
+
+// dZ = (maxpool backward of dpool + dskip) * [act > 0], C channels (multiple of 8)
+template <int C>
+__global__ void __launch_bounds__(256) pool_bwd_kernel(const __nv_bfloat16 *__restrict__ act,
+                                                       const __nv_bfloat16 *__restrict__ pooled,
+                                                       const __nv_bfloat16 *__restrict__ dpool,
+                                                       const __nv_bfloat16 *__restrict__ dskip,
+                                                       __nv_bfloat16 *__restrict__ dz, int H, int W, int B)
+{
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (size_t)B * H * W) return;
+    const int x = (int)(q % W), y = (int)((q / W) % H), b = (int)(q / ((size_t)W * H));
+    const int PH = H / 2, PW = W / 2;
+    float a[C], g[C];
+#pragma unroll
+    for (int c = 0; c < C; c += 8) {
+        ld8(act + q * C + c, a + c);
+        ld8(dskip + q * C + c, g + c);
+    }
+    const int py = y / 2, px = x / 2;
+    if (py < PH && px < PW) {
+        const size_t pq = ((size_t)b * PH + py) * PW + px;
+        float m[C], dp[C];
+#pragma unroll
+        for (int c = 0; c < C; c += 8) {
+            ld8(pooled + pq * C + c, m + c);
+            ld8(dpool + pq * C + c, dp + c);
+        }
+        // position of this pixel in its window and of the first maximum before it
+        const int me = (y & 1) * 2 + (x & 1);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            if (a[c] != m[c]) continue;
+            bool first = true;
+            for (int k = 0; k < me; ++k) {
+                const size_t r = ((size_t)b * H + 2 * py + (k >> 1)) * W + 2 * px + (k & 1);
+                if (__bfloat162float(act[r * C + c]) == m[c]) first = false;
+            }
+            if (first) g[c] += dp[c];
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < C; ++c)
+        if (!(a[c] > 0.f)) g[c] = 0.f;
+#pragma unroll
+    for (int c = 0; c < C; c += 8) st8(dz + q * C + c, g + c);
+}
+
+// out[j] = sum over t < tiles of partial[t * n + j], in order of t
+__global__ void __launch_bounds__(256) reduce_kernel(const float *__restrict__ partial, float *__restrict__ out,
+                                                     int n, int tiles)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    float s = 0.f;
+    for (int t = 0; t < tiles; ++t) s += partial[(size_t)t * n + j];
+    out[j] = s;
+}
+
+__global__ void __launch_bounds__(256) adam_kernel(float *__restrict__ w, const float *__restrict__ g,
+                                                   float *__restrict__ m, float *__restrict__ v, int n, float lr_t,
+                                                   float b1, float b2, float eps)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = m[i] + (gi - m[i]) * (1.f - b1);
+    const float vi = v[i] + (gi * gi - v[i]) * (1.f - b2);
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= (mi * lr_t) / (sqrtf(vi) + eps);
+}
+
+}  // namespace
+
+cudaError_t launch_pack_input(const float *a, const float *b, const float *c, const float *d, const float *e,
+                              __nv_bfloat16 *x, size_t n, cudaStream_t st)
+{
+    pack_input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, b, c, d, e, x, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tconv_fwd(int ci, int co, const __nv_bfloat16 *in, const float *K, const float *bias,
+                             __nv_bfloat16 *out, int Hi, int Wi, int B, cudaStream_t st)
+{
+    const size_t n = (size_t)B * 4 * Hi * Wi;
+    const unsigned g = (unsigned)((n + 255) / 256);
+    if (ci == 32 && co == 32) tconv_fwd_kernel<32, 32><<<g, 256, 0, st>>>(in, K, bias, out, Hi, Wi, B);
+    else if (ci == 16 && co == 16) tconv_fwd_kernel<16, 16><<<g, 256, 0, st>>>(in, K, bias, out, Hi, Wi, B);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+// pixels per block of the transposed-conv backward (static shared memory < 48 KB)
+static int tconv_bwd_px(int ci) { return ci == 32 ? 64 : 128; }
+
+size_t tconv_blocks(int ci, int Hi, int Wi, int B)
+{
+    const int k = tconv_bwd_px(ci);
+    return ((size_t)B * Hi * Wi + k - 1) / k;
+}
+
+cudaError_t launch_tconv_bwd(int ci, int co, const __nv_bfloat16 *in, const __nv_bfloat16 *dout, const float *K,
+                             __nv_bfloat16 *dz_in, float *partial, int Hi, int Wi, int B, cudaStream_t st)
+{
+    const unsigned g = (unsigned)tconv_blocks(ci, Hi, Wi, B);
+    if (ci == 32 && co == 32) tconv_bwd_kernel<32, 32, 64><<<g, 64, 0, st>>>(in, dout, K, dz_in, partial, Hi, Wi, B);
+    else if (ci == 16 && co == 16)
+        tconv_bwd_kernel<16, 16, 128><<<g, 128, 0, st>>>(in, dout, K, dz_in, partial, Hi, Wi, B);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_head_fwd(const __nv_bfloat16 *x, const float *K, const float *bias, float *band, float *alpha,
+                            size_t n, cudaStream_t st)
+{
+    head_fwd_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, K, bias, band, alpha, n);
+    return cudaGetLastError();
+}
+
+size_t head_blocks(size_t n) { return (n + 127) / 128; }
+
+cudaError_t launch_head_bwd(const __nv_bfloat16 *x, const float *K, const float *bias, const float *gband,
+                            const float *galpha, __nv_bfloat16 *dz, float *partial, size_t n, cudaStream_t st)
+{
+    head_bwd_kernel<<<(unsigned)head_blocks(n), 128, 0, st>>>(x, K, bias, gband, galpha, dz, partial, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pool_bwd(int C, const __nv_bfloat16 *act, const __nv_bfloat16 *pooled,
+                            const __nv_bfloat16 *dpool, const __nv_bfloat16 *dskip, __nv_bfloat16 *dz, int H, int W,
+                            int B, cudaStream_t st)
+{
+    const size_t n = (size_t)B * H * W;
+    const unsigned g = (unsigned)((n + 255) / 256);
+    if (C == 8) pool_bwd_kernel<8><<<g, 256, 0, st>>>(act, pooled, dpool, dskip, dz, H, W, B);
+    else if (C == 16) pool_bwd_kernel<16><<<g, 256, 0, st>>>(act, pooled, dpool, dskip, dz, H, W, B);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reduce(const float *partial, float *out, int n, int tiles, cudaStream_t st)
+{
+    reduce_kernel<<<(n + 255) / 256, 256, 0, st>>>(partial, out, n, tiles);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adam(float *w, const float *g, float *m, float *v, int n, float lr_t, float b1, float b2,
+                        float eps, cudaStream_t st)
+{
+    adam_kernel<<<(n + 255) / 256, 256, 0, st>>>(w, g, m, v, n, lr_t, b1, b2, eps);
+    return cudaGetLastError();
+}
+
+}  // namespace unet
+}  // namespace cd

@@ -297,6 +297,61 @@ CD_API cd_status cd_filter_aggregate(const float *ols1, const float *ols2, const
                                      void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* Kernel-predicting U-Net (replaces the Keras model of scripts/main.py:83-118 */
+/* and its tf.GradientTape / optimizer.apply_gradients, :289-303).            */
+/* Parameters: one flat fp32 buffer of cd_unet_param_count() = 31,414        */
+/* floats, the model's trainable variables in order, each conv kernel in     */
+/* Keras layout [kh][kw][cin][cout] (Conv2DTranspose: [1][1][cout][cin])     */
+/* followed by its bias.  The convolutions run on the tensor cores with bf16 */
+/* operands and fp32 accumulation; activations are kept in bf16 in the      */
+/* workspace; the 1x1 head is fp32.  H and W must be multiples of 4.         */
+/*  ols1, ols2, prev_out, albedo, normal : [B,H,W,3] (the concatenated input) */
+/*  band : [B,H,W,5] = 1/(p^2 + 1e-4);  alpha : [B,H,W,1] = sigmoid(p)       */
+/* cd_unet_backward needs the workspace of the cd_unet_forward of the same   */
+/* frame and parameters; it writes dL/dparams (same layout) given dL/dband   */
+/* and dL/dalpha.  The first int32 of the workspace is an error flag that a */
+/* kernel sets to 1 when a tensor-core completion wait times out (the        */
+/* caller zeroes the workspace once and may poll it; outputs are then        */
+/* invalid).                                                                  */
+/* ------------------------------------------------------------------------ */
+CD_API size_t cd_unet_param_count(void);
+CD_API size_t cd_unet_workspace_size(int B, int H, int W);
+
+CD_API cd_status cd_unet_forward(const float *ols1, const float *ols2, const float *prev_out,
+                                 const float *albedo, const float *normal, const float *params,
+                                 float *band, float *alpha, int B, int H, int W,
+                                 void *workspace, size_t workspace_bytes, cudaStream_t stream);
+
+CD_API cd_status cd_unet_backward(const float *grad_band, const float *grad_alpha,
+                                  const float *params, float *grad_params, int B, int H, int W,
+                                  void *workspace, size_t workspace_bytes, cudaStream_t stream);
+
+/* Adam with Keras semantics (scripts/main.py:81, keras.optimizers.Adam):    */
+/* m += (g - m)(1 - beta1); v += (g^2 - v)(1 - beta2);                       */
+/* p -= lr sqrt(1 - beta2^step) / (1 - beta1^step) * m / (sqrt(v) + epsilon),*/
+/* step = 1 for the first update.                                             */
+CD_API cd_status cd_adam_update(float *params, const float *grads, float *m, float *v, int n,
+                                int step, float lr, float beta1, float beta2, float epsilon,
+                                cudaStream_t stream);
+
+/* One 3x3 'same' conv layer of the network through the same tensor-core    */
+/* kernels (for layer-level checks).  x, y: NHWC bf16 with channel counts    */
+/* rounded up to multiples of 8.  dgrad = 0: y = relu(conv(x) + bias),       */
+/* x has cin channels, y cout; dgrad = 1: y = dL/dx given x = dL/dz (the     */
+/* pre-activation gradient, cout channels), no bias, no ReLU.  cin in        */
+/* {8, 15, 16, 24, 32, 48}, cout in {8, 16, 32}.                              */
+CD_API size_t cd_unet_conv3x3_workspace_size(int cin, int cout);
+CD_API cd_status cd_unet_conv3x3(const float *weight, const float *bias, const void *x, void *y,
+                                 int cin, int cout, int dgrad, int B, int H, int W,
+                                 void *workspace, size_t workspace_bytes, cudaStream_t stream);
+/* Weight and bias gradient of such a layer: grad = [dW (Keras layout), db]  */
+/* from its input x (cin channels) and dz (cout channels).                    */
+CD_API size_t cd_unet_conv3x3_wgrad_workspace_size(int cin, int cout, int B, int H, int W);
+CD_API cd_status cd_unet_conv3x3_wgrad(const void *x, const void *dz, float *grad, int cin, int cout,
+                                       int B, int H, int W, void *workspace, size_t workspace_bytes,
+                                       cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
 /* FP32 FMA throughput probe (no counterpart in the reference): `blocks`     */
 /* CTAs of 256 threads each issue iters x 128 fused multiply-adds and store  */
 /* one float per thread to out[blocks * 256].  Timed by the caller; gives    */
