@@ -47,7 +47,7 @@ SIGNATURES = {
     "cd_unet_workspace_size": (_S, [_I] * 3),
     "cd_unet_forward": (_I, [_P] * 8 + [_I] * 3 + [_P, _S, _P]),
     "cd_unet_backward": (_I, [_P] * 4 + [_I] * 3 + [_P, _S, _P]),
-    "cd_adam_update": (_I, [_P] * 4 + [_I, _I] + [_F] * 4 + [_P]),
+    "cd_adam_update": (_I, [_P] * 4 + [_I, _P] + [_F] * 4 + [_P]),
     "cd_unet_conv3x3_workspace_size": (_S, [_I, _I]),
     "cd_unet_conv3x3": (_I, [_P] * 4 + [_I] * 6 + [_P, _S, _P]),
     "cd_unet_conv3x3_wgrad_workspace_size": (_S, [_I] * 5),
@@ -60,7 +60,7 @@ KERNELS_PER_CALL = {
     "cd_cross_regression": 3, "cd_cross_regression_grad": 8, "cd_spatial_filter": 1, "cd_spatial_filter_grad": 1, "cd_reproject": 1,
     "cd_erode3x3": 1, "cd_temporal_screening": 1, "cd_erode_temporal_screening": 1,
     "cd_prepare_input": 1, "cd_aggregation_loss": 2, "cd_filter_aggregate": 2,
-    "cd_unet_forward": 22, "cd_unet_backward": 42, "cd_adam_update": 1, "cd_unet_conv3x3": 2,
+    "cd_unet_forward": 22, "cd_unet_backward": 42, "cd_adam_update": 2, "cd_unet_conv3x3": 2,
     "cd_unet_conv3x3_wgrad": 2,
 }
 LAUNCHES = {"count": 0}

@@ -386,12 +386,12 @@ cd_status cd_unet_backward(const float *grad_band, const float *grad_alpha, cons
                        "unet_backward");
 }
 
-cd_status cd_adam_update(float *params, const float *grads, float *m, float *v, int n, int step, float lr,
+cd_status cd_adam_update(float *params, const float *grads, float *m, float *v, int n, int *step, float lr,
                          float beta1, float beta2, float epsilon, cudaStream_t stream)
 {
     g_err[0] = 0;
-    if (!params || !grads || !m || !v) return fail(CD_EINVAL, "adam_update: null pointer");
-    if (n < 1 || step < 1) return fail(CD_EINVAL, "adam_update: n and step must be >= 1 (n=%d step=%d)", n, step);
+    if (!params || !grads || !m || !v || !step) return fail(CD_EINVAL, "adam_update: null pointer");
+    if (n < 1) return fail(CD_EINVAL, "adam_update: n must be >= 1 (n=%d)", n);
     return cuda_status(cd::unet::adam(params, grads, m, v, n, step, lr, beta1, beta2, epsilon, stream), "adam_update");
 }
 

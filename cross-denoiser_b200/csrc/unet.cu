@@ -330,13 +330,10 @@ cudaError_t wgrad_layer(const __nv_bfloat16 *x, const __nv_bfloat16 *dz, float *
     return launch_reduce(P.partial, grad, 9 * cin * cout + cout, (int)wgrad_tiles(B, H, W), st);
 }
 
-// lr_t = lr sqrt(1 - b2^t) / (1 - b1^t), in float as Keras computes it
-cudaError_t adam(float *w, const float *g, float *m, float *v, int n, int step, float lr, float b1, float b2,
+cudaError_t adam(float *w, const float *g, float *m, float *v, int n, int *step, float lr, float b1, float b2,
                  float eps, cudaStream_t st)
 {
-    const float b1p = powf(b1, (float)step), b2p = powf(b2, (float)step);
-    const float lr_t = lr * sqrtf(1.f - b2p) / (1.f - b1p);
-    return launch_adam(w, g, m, v, n, lr_t, b1, b2, eps, st);
+    return launch_adam(w, g, m, v, n, step, lr, b1, b2, eps, st);
 }
 
 }  // namespace unet

@@ -79,7 +79,7 @@ cudaError_t forward(const float *ols1, const float *ols2, const float *prev, con
                     int W, cudaStream_t st);
 cudaError_t backward(const float *gband, const float *galpha, const float *params, float *grads, void *ws, int B,
                      int H, int W, cudaStream_t st);
-cudaError_t adam(float *w, const float *g, float *m, float *v, int n, int step, float lr, float b1, float b2,
+cudaError_t adam(float *w, const float *g, float *m, float *v, int n, int *step, float lr, float b1, float b2,
                  float eps, cudaStream_t st);
 
 // Single 3x3 conv layer through the same kernels (layer tests): forward

@@ -310,12 +310,18 @@ __global__ void __launch_bounds__(256) reduce_kernel(const float *__restrict__ p
     out[j] = s;
 }
 
+// The update count lives in device memory (so a captured graph replays
+// correct steps): t = *step + 1, lr_t = lr sqrt(1 - b2^t) / (1 - b1^t) in
+// float as Keras computes it; step_kernel then advances the counter.
 __global__ void __launch_bounds__(256) adam_kernel(float *__restrict__ w, const float *__restrict__ g,
-                                                   float *__restrict__ m, float *__restrict__ v, int n, float lr_t,
-                                                   float b1, float b2, float eps)
+                                                   float *__restrict__ m, float *__restrict__ v, int n,
+                                                   const int *__restrict__ step, float lr, float b1, float b2,
+                                                   float eps)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const float t = (float)(*step + 1);
+    const float lr_t = lr * sqrtf(1.f - powf(b2, t)) / (1.f - powf(b1, t));
     const float gi = g[i];
     const float mi = m[i] + (gi - m[i]) * (1.f - b1);
     const float vi = v[i] + (gi * gi - v[i]) * (1.f - b2);
@@ -323,6 +329,8 @@ __global__ void __launch_bounds__(256) adam_kernel(float *__restrict__ w, const 
     v[i] = vi;
     w[i] -= (mi * lr_t) / (sqrtf(vi) + eps);
 }
+
+__global__ void step_kernel(int *step) { *step += 1; }
 
 }  // namespace
 
@@ -398,10 +406,11 @@ cudaError_t launch_reduce(const float *partial, float *out, int n, int tiles, cu
     return cudaGetLastError();
 }
 
-cudaError_t launch_adam(float *w, const float *g, float *m, float *v, int n, float lr_t, float b1, float b2,
+cudaError_t launch_adam(float *w, const float *g, float *m, float *v, int n, int *step, float lr, float b1, float b2,
                         float eps, cudaStream_t st)
 {
-    adam_kernel<<<(n + 255) / 256, 256, 0, st>>>(w, g, m, v, n, lr_t, b1, b2, eps);
+    adam_kernel<<<(n + 255) / 256, 256, 0, st>>>(w, g, m, v, n, step, lr, b1, b2, eps);
+    step_kernel<<<1, 1, 0, st>>>(step);
     return cudaGetLastError();
 }
 

@@ -23,7 +23,7 @@ cudaError_t launch_pool_bwd(int C, const __nv_bfloat16 *act, const __nv_bfloat16
                             const __nv_bfloat16 *dpool, const __nv_bfloat16 *dskip, __nv_bfloat16 *dz, int H, int W,
                             int B, cudaStream_t st);
 cudaError_t launch_reduce(const float *partial, float *out, int n, int tiles, cudaStream_t st);
-cudaError_t launch_adam(float *w, const float *g, float *m, float *v, int n, float lr_t, float b1, float b2,
+cudaError_t launch_adam(float *w, const float *g, float *m, float *v, int n, int *step, float lr, float b1, float b2,
                         float eps, cudaStream_t st);
 
 }  // namespace unet

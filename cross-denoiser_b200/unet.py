@@ -97,7 +97,7 @@ class UNet:
         self.m = torch.zeros_like(self.params)
         self.v = torch.zeros_like(self.params)
         self.lr = float(lr)
-        self.step = 0
+        self.step = torch.zeros((1,), dtype=torch.int32, device=self.device)   # optimizer iterations
         self._shape = None
         self.ws = None
 
@@ -135,9 +135,8 @@ class UNet:
         return self.grads
 
     def apply_gradients(self):
-        self.step += 1
         _lib.check(_lib.lib().cd_adam_update(_ptr(self.params), _ptr(self.grads), _ptr(self.m), _ptr(self.v),
-                                             self.n, self.step, self.lr, BETA1, BETA2, EPSILON, _stream()),
+                                             self.n, _ptr(self.step), self.lr, BETA1, BETA2, EPSILON, _stream()),
                    "adam_update")
 
     def on_gradients(self, g_band, g_alpha):

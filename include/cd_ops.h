@@ -328,10 +328,12 @@ CD_API cd_status cd_unet_backward(const float *grad_band, const float *grad_alph
 
 /* Adam with Keras semantics (scripts/main.py:81, keras.optimizers.Adam):    */
 /* m += (g - m)(1 - beta1); v += (g^2 - v)(1 - beta2);                       */
-/* p -= lr sqrt(1 - beta2^step) / (1 - beta1^step) * m / (sqrt(v) + epsilon),*/
-/* step = 1 for the first update.                                             */
+/* p -= lr sqrt(1 - beta2^t) / (1 - beta1^t) * m / (sqrt(v) + epsilon),     */
+/* with t = *step + 1; *step is a device int32 (the optimizer's iteration    */
+/* count, 0 before the first update) that the call then increments, so a    */
+/* captured CUDA graph replays successive steps.                              */
 CD_API cd_status cd_adam_update(float *params, const float *grads, float *m, float *v, int n,
-                                int step, float lr, float beta1, float beta2, float epsilon,
+                                int *step, float lr, float beta1, float beta2, float epsilon,
                                 cudaStream_t stream);
 
 /* One 3x3 'same' conv layer of the network through the same tensor-core    */
