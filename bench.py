@@ -78,8 +78,9 @@ def args_parse():
     ap.add_argument("--serve", action="store_true",
                     help="serving run: 16 mixed-resolution streams (4x720p, 8x1080p, 3x1440p, 1x2160p)")
     ap.add_argument("--serve-frames", type=int, default=60, help="frames per stream in the serving run")
-    ap.add_argument("--ncu-region", action="store_true",
-                    help="bracket the fused phase with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
+    ap.add_argument("--ncu-region", choices=["fused", "full"], default=None,
+                    help="bracket the timed steps of the fused ops step or of the full step (with the U-Net) "
+                         "with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     return ap.parse_args()
 
 
@@ -354,11 +355,11 @@ def run_mine(a, rank, world, device):
         fn = stepper(True, a.win)
         if world > 1:
             torch.distributed.barrier()
-        if a.ncu_region:
+        if a.ncu_region == "fused":
             torch.cuda.profiler.start()
         with op_timer(fn, stream) as store:
             total, ms = timed_steps(fn, frames, a.warmup, a.steps, stream)
-        if a.ncu_region:
+        if a.ncu_region == "fused":
             torch.cuda.profiler.stop()
         launches = cd._lib.LAUNCHES["count"] * a.steps // (a.steps + a.warmup)
         total = max_over_ranks(total, world)
@@ -418,7 +419,11 @@ def run_mine(a, rank, world, device):
         full.predictor = net.forward
         if world > 1:
             torch.distributed.barrier()
+        if a.ncu_region == "full":
+            torch.cuda.profiler.start()
         total, ms = timed_steps(lambda f, t: full(f), frames, a.warmup, a.steps, stream)
+        if a.ncu_region == "full":
+            torch.cuda.profiler.stop()
         total = max_over_ranks(total, world)
         fo = {}
         for k, evs in net_ev.items():

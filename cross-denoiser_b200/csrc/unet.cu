@@ -76,8 +76,8 @@ size_t partial_floats(int B, int H, int W)
         const int h = H >> kLvl[l], w = W >> kLvl[l];
         size_t n = 0;
         if (d.kind == CONV) n = wgrad_partial_floats(B, h, w, d.cin, d.cout);
-        else if (d.kind == TCONV) n = tconv_blocks(d.cin, h, w, B) * (size_t)(d.cin * d.cout + d.cout);
-        else n = head_blocks((size_t)B * H * W) * 54;
+        else if (d.kind == TCONV) n = reduce_floats(d.cin * d.cout + d.cout, (int)tconv_blocks(d.cin, h, w, B));
+        else n = reduce_floats(54, (int)head_blocks((size_t)B * H * W));
         m = n > m ? n : m;
     }
     return m;

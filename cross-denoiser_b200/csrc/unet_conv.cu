@@ -24,6 +24,7 @@
 #include "cd_common.cuh"
 #include "tc_sm100.cuh"
 #include "unet.cuh"
+#include "unet_ops.cuh"
 
 namespace cd {
 namespace unet {
@@ -228,16 +229,19 @@ __global__ void pack_kernel(const float *__restrict__ w, __nv_bfloat16 *__restri
 }
 
 // Weight gradient.  D_tap[cin x cout] = sum_p X[p + tap][cin] dZ[p][cout]:
-// M = input channels (128 rows: the chunk planes of X from chunk 0 on, rows
-// past cin read other staged data and are discarded), N = output channels
-// padded to NZ, K = 16 consecutive pixels per MMA; both operands MN-major
-// (channels contiguous, pixels 16 bytes apart).  Nine accumulators, one per
-// tap.  A CTA covers R rows x 128 pixels and writes its partial sums.
+// M = input channels (128 rows: the chunk planes of X from chunk 0 on), N =
+// output channels padded to NZ, K = 16 consecutive pixels per MMA; both
+// operands MN-major (channels contiguous, pixels 16 bytes apart).  Nine
+// accumulators, one per tap.  Each staged row carries, after its nch chunk
+// planes, a plane of ones, so row 8 * nch of the centre tap's accumulator is
+// sum_p dZ[p][cout], the bias gradient; rows past it read other staged data
+// and are discarded.  A CTA covers R rows x 128 pixels and writes its
+// partial sums [9 * cin * cout weights, cout biases].
 constexpr int kZPlane = kPx * 16;
 
 __host__ __device__ inline size_t wgrad_smem(int nch, int zc, int R)
 {
-    return (size_t)((R + 2) * nch + 16) * kPlane + (size_t)(R * zc + 4) * kZPlane + 16;
+    return (size_t)((R + 2) * (nch + 1) + 16) * kPlane + (size_t)(R * zc + 4) * kZPlane + 16;
 }
 
 template <int NZ, int R>
@@ -249,9 +253,9 @@ __global__ void __launch_bounds__(128) wgrad_kernel(const WgradParams P)
     const int tid = threadIdx.x, warp = tid >> 5;
     const int x0 = blockIdx.x * kPx, y0 = blockIdx.y * R, b = blockIdx.z;
     const int tile = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-    const int nch = P.xc0 + P.xc1;
+    const int nch = P.xc0 + P.xc1, rs = nch + 1;   // planes per staged row (with the ones plane)
     uint8_t *sX = smem;
-    uint8_t *sZ = sX + (size_t)((R + 2) * nch + 16) * kPlane;
+    uint8_t *sZ = sX + (size_t)((R + 2) * rs + 16) * kPlane;
     uint64_t *bar = reinterpret_cast<uint64_t *>(sZ + (size_t)(R * P.zc + 4) * kZPlane);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
     const size_t HW = (size_t)P.H * P.W;
@@ -264,7 +268,12 @@ __global__ void __launch_bounds__(128) wgrad_kernel(const WgradParams P)
         const size_t pix = b * HW + (size_t)(in ? gy : 0) * P.W + (in ? gx : 0);
         const __nv_bfloat16 *src = c < P.xc0 ? P.x0 + pix * (8 * P.xc0) + 8 * c
                                              : P.x1 + pix * (8 * P.xc1) + 8 * (c - P.xc0);
-        tc::cp16(sX + (size_t)(r * nch + c) * kPlane + 16 * px, src, in ? 16u : 0u);
+        tc::cp16(sX + (size_t)(r * rs + c) * kPlane + 16 * px, src, in ? 16u : 0u);
+    }
+    const uint4 ones = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);   // bf16 1.0 x 8
+    for (int i = tid; i < (R + 2) * kStagePx; i += 128) {
+        const int px = i % kStagePx, r = i / kStagePx;
+        *reinterpret_cast<uint4 *>(sX + (size_t)(r * rs + nch) * kPlane + 16 * px) = ones;
     }
     for (int i = tid; i < R * P.zc * kPx; i += 128) {
         const int px = i % kPx, t = i / kPx;
@@ -291,7 +300,7 @@ __global__ void __launch_bounds__(128) wgrad_kernel(const WgradParams P)
                 const uint64_t bd = tc::sdesc(az + (uint32_t)(r * P.zc) * kZPlane + 256u * g, 128, kZPlane);
                 for (int tap = 0; tap < 9; ++tap) {
                     const int ky = tap / 3, kx = tap - 3 * ky;
-                    const uint32_t a = ax + (uint32_t)((r + ky) * nch) * kPlane + (uint32_t)(kx + 16 * g) * 16;
+                    const uint32_t a = ax + (uint32_t)((r + ky) * rs) * kPlane + (uint32_t)(kx + 16 * g) * 16;
                     tc::mma_bf16(tbase + tap * NZ, tc::sdesc(a, 128, kPlane), bd, idesc, (r | g) ? 1u : 0u);
                 }
             }
@@ -302,31 +311,23 @@ __global__ void __launch_bounds__(128) wgrad_kernel(const WgradParams P)
     float *out = P.partial + (size_t)tile * (9 * P.cin * P.cout + P.cout);
     if (!done) {
         if (tid == 0) atomicExch(P.err, 1);
-    } else {
-        if (warp * 32 < P.cin) {
-            const int m = warp * 32 + (tid & 31);
-            for (int tap = 0; tap < 9; ++tap)
+    } else if (warp * 32 <= 8 * nch) {
+        const int m = warp * 32 + (tid & 31);
+        for (int tap = 0; tap < 9; ++tap)
 #pragma unroll
-                for (int j = 0; j < NZ; j += 16) {
-                    float v[16];
-                    tc::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + tap * NZ + j, v);
-                    if (m < P.cin)
+            for (int j = 0; j < NZ; j += 16) {
+                float v[16];
+                tc::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + tap * NZ + j, v);
+                if (m < P.cin) {
 #pragma unroll
-                        for (int q = 0; q < 16; ++q)
-                            if (j + q < P.cout) out[(tap * P.cin + m) * P.cout + j + q] = v[q];
+                    for (int q = 0; q < 16; ++q)
+                        if (j + q < P.cout) out[(tap * P.cin + m) * P.cout + j + q] = v[q];
+                } else if (m == 8 * nch && tap == 4) {
+#pragma unroll
+                    for (int q = 0; q < 16; ++q)
+                        if (j + q < P.cout) out[9 * P.cin * P.cout + j + q] = v[q];
                 }
-        }
-        if (tid < P.cout) {
-            // bias gradient: the tile's sum of dZ for channel tid
-            float s = 0.f;
-            const int c = tid >> 3, e = tid & 7;
-            for (int r = 0; r < R; ++r) {
-                const __nv_bfloat16 *row =
-                    reinterpret_cast<const __nv_bfloat16 *>(sZ + (size_t)(r * P.zc + c) * kZPlane) + e;
-                for (int px = 0; px < kPx; ++px) s += __bfloat162float(row[8 * px]);
             }
-            out[9 * P.cin * P.cout + tid] = s;
-        }
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -406,7 +407,7 @@ size_t wgrad_tiles(int B, int H, int W) { return (size_t)B * ((W + kPx - 1) / kP
 
 size_t wgrad_partial_floats(int B, int H, int W, int cin, int cout)
 {
-    return wgrad_tiles(B, H, W) * (size_t)(9 * cin * cout + cout);
+    return reduce_floats(9 * cin * cout + cout, (int)wgrad_tiles(B, H, W));
 }
 
 cudaError_t launch_wgrad(const WgradParams &P, int B, cudaStream_t st)

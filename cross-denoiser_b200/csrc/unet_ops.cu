@@ -299,6 +299,21 @@ __global__ void __launch_bounds__(256) pool_bwd_kernel(const __nv_bfloat16 *__re
     for (int c = 0; c < C; c += 8) st8(dz + q * C + c, g + c);
 }
 
+// Two-stage fixed-order reduction of per-tile partial sums: stage 1 sums
+// groups of kGroup consecutive tiles (grid y = group), stage 2 sums the groups.
+constexpr int kGroup = 64;
+
+__global__ void __launch_bounds__(256) reduce_group_kernel(const float *__restrict__ partial,
+                                                           float *__restrict__ out, int n, int tiles)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int t0 = blockIdx.y * kGroup, t1 = min(tiles, t0 + kGroup);
+    float s = 0.f;
+    for (int t = t0; t < t1; ++t) s += partial[(size_t)t * n + j];
+    out[(size_t)blockIdx.y * n + j] = s;
+}
+
 // out[j] = sum over t < tiles of partial[t * n + j], in order of t
 __global__ void __launch_bounds__(256) reduce_kernel(const float *__restrict__ partial, float *__restrict__ out,
                                                      int n, int tiles)
@@ -400,9 +415,18 @@ cudaError_t launch_pool_bwd(int C, const __nv_bfloat16 *act, const __nv_bfloat16
     return cudaGetLastError();
 }
 
-cudaError_t launch_reduce(const float *partial, float *out, int n, int tiles, cudaStream_t st)
+size_t reduce_floats(int n, int tiles) { return (size_t)n * tiles + (size_t)n * ((tiles + kGroup - 1) / kGroup); }
+
+cudaError_t launch_reduce(float *partial, float *out, int n, int tiles, cudaStream_t st)
 {
-    reduce_kernel<<<(n + 255) / 256, 256, 0, st>>>(partial, out, n, tiles);
+    if (tiles <= kGroup) {
+        reduce_kernel<<<(n + 255) / 256, 256, 0, st>>>(partial, out, n, tiles);
+        return cudaGetLastError();
+    }
+    const int groups = (tiles + kGroup - 1) / kGroup;
+    float *mid = partial + (size_t)n * tiles;
+    reduce_group_kernel<<<dim3((n + 255) / 256, groups), 256, 0, st>>>(partial, mid, n, tiles);
+    reduce_kernel<<<(n + 255) / 256, 256, 0, st>>>(mid, out, n, groups);
     return cudaGetLastError();
 }
 

@@ -22,7 +22,11 @@ cudaError_t launch_head_bwd(const __nv_bfloat16 *x, const float *K, const float 
 cudaError_t launch_pool_bwd(int C, const __nv_bfloat16 *act, const __nv_bfloat16 *pooled,
                             const __nv_bfloat16 *dpool, const __nv_bfloat16 *dskip, __nv_bfloat16 *dz, int H, int W,
                             int B, cudaStream_t st);
-cudaError_t launch_reduce(const float *partial, float *out, int n, int tiles, cudaStream_t st);
+// Sum per-tile partials partial[t * n + j] over t into out[j] (fixed order).
+// The partial buffer must hold reduce_floats(n, tiles) floats: the tiles'
+// sums followed by room for the per-group sums.
+size_t reduce_floats(int n, int tiles);
+cudaError_t launch_reduce(float *partial, float *out, int n, int tiles, cudaStream_t st);
 cudaError_t launch_adam(float *w, const float *g, float *m, float *v, int n, int *step, float lr, float b1, float b2,
                         float eps, cudaStream_t st);
 
