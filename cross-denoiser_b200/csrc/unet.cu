@@ -187,7 +187,7 @@ cudaError_t wgrad(const Ctx &c, float *grads, int l, int lvl, Buf x0, int xc0, B
     P.W = c.W >> lvl;
     P.err = c.err();
     CD_TRY(launch_wgrad(P, c.B, c.st));
-    return launch_reduce(c.partial(), grads + param_offset(l), param_size(d), (int)wgrad_tiles(c.B, P.H, P.W), c.st);
+    return launch_reduce(c.partial(), grads + param_offset(l), param_size(d), wgrad_partial_rows(P, c.B), c.st);
 }
 
 constexpr Buf NONE = NBUF;
@@ -327,7 +327,7 @@ cudaError_t wgrad_layer(const __nv_bfloat16 *x, const __nv_bfloat16 *dz, float *
     P.W = W;
     P.err = reinterpret_cast<int *>(base);
     CD_TRY(launch_wgrad(P, B, st));
-    return launch_reduce(P.partial, grad, 9 * cin * cout + cout, (int)wgrad_tiles(B, H, W), st);
+    return launch_reduce(P.partial, grad, 9 * cin * cout + cout, wgrad_partial_rows(P, B), st);
 }
 
 cudaError_t adam(float *w, const float *g, float *m, float *v, int n, int *step, float lr, float b1, float b2,

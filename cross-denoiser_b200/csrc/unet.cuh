@@ -67,6 +67,7 @@ struct WgradParams {
     int *err;
 };
 size_t wgrad_tiles(int B, int H, int W);
+int wgrad_partial_rows(const WgradParams &P, int B);
 size_t wgrad_partial_floats(int B, int H, int W, int cin, int cout);
 cudaError_t launch_wgrad(const WgradParams &P, int B, cudaStream_t st);
 

@@ -72,15 +72,18 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P)
     const uint8_t *wsrc = reinterpret_cast<const uint8_t *>(P.wpack);
     for (int i = tid; i < bb / 16; i += 128) tc::cp16(sB + 16 * i, wsrc + 16 * i, 16);
     const size_t HW = (size_t)P.H * P.W;
-    for (int i = tid; i < (R + 2) * nch * kStagePx; i += 128) {
-        const int px = i % kStagePx, t = i / kStagePx;
-        const int c = t % nch, r = t / nch;
+    for (int i = tid; i < (R + 2) * kStagePx; i += 128) {
+        const int r = i / kStagePx, px = i - r * kStagePx;
         const int gy = y0 - 1 + r, gx = x0 - 1 + px;
         const bool in = gy >= 0 && gy < P.H && gx >= 0 && gx < P.W;
         const size_t pix = b * HW + (size_t)(in ? gy : 0) * P.W + (in ? gx : 0);
-        const __nv_bfloat16 *src = c < P.c0 ? P.src0 + pix * (8 * P.c0) + 8 * c
-                                            : P.src1 + pix * (8 * P.c1) + 8 * (c - P.c0);
-        tc::cp16(sA + (size_t)(r * nch + c) * kPlane + 16 * px, src, in ? 16u : 0u);
+        uint8_t *d = sA + (size_t)r * nch * kPlane + 16 * px;
+        const __nv_bfloat16 *s0 = P.src0 + pix * (8 * P.c0);
+        for (int c = 0; c < P.c0; ++c) tc::cp16(d + (size_t)c * kPlane, s0 + 8 * c, in ? 16u : 0u);
+        if (P.c1) {
+            const __nv_bfloat16 *s1 = P.src1 + pix * (8 * P.c1);
+            for (int c = 0; c < P.c1; ++c) tc::cp16(d + (size_t)(P.c0 + c) * kPlane, s1 + 8 * c, in ? 16u : 0u);
+        }
     }
     if (warp == 0) tc::tmem_alloc(tslot, kCols);
     if (tid == 0) tc::mbar_init(bar, 1);
@@ -103,7 +106,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P)
             }
         tc::commit(bar);
     }
-    const bool done = tc::mbar_wait(bar, 0, kWaitIter);
+    const bool done = __syncthreads_and(tc::mbar_wait(bar, 0, kWaitIter)) != 0;   // uniform across the CTA
     tc::fence_after_sync();
     if (!done) {
         if (tid == 0) atomicExch(P.err, 1);
@@ -306,7 +309,7 @@ __global__ void __launch_bounds__(128) wgrad_kernel(const WgradParams P)
             }
         tc::commit(bar);
     }
-    const bool done = tc::mbar_wait(bar, 0, kWaitIter);
+    const bool done = __syncthreads_and(tc::mbar_wait(bar, 0, kWaitIter)) != 0;   // uniform across the CTA
     tc::fence_after_sync();
     float *out = P.partial + (size_t)tile * (9 * P.cin * P.cout + P.cout);
     if (!done) {
@@ -332,6 +335,164 @@ __global__ void __launch_bounds__(128) wgrad_kernel(const WgradParams P)
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) tc::tmem_dealloc(tbase, kCols);
+}
+
+// Persistent weight gradient with the three horizontal taps folded into M.
+// Each staged input row holds three copies shifted by kx = 0, 1, 2 pixels
+// (planes [kx][chunk], 128 pixels each) and a plane of ones, so for a
+// kernel row ky one MMA computes
+//   D_ky[(kx, cin) x cout] += X_ky^T[(kx, cin) x 16 px] dZ[16 px x cout]
+// and row 8 * 3 * nch of D_1 is the bias gradient.  M = 128 rows cover
+// 3 * nch + 1 chunk groups (nch <= 5); rows past them read other staged data
+// and are discarded.  CTAs are persistent (one per SM) and keep their three
+// accumulators in TMEM over all their tiles; tile i + 1 is copied in
+// (cp.async, second stage) while the tensor cores work on tile i.  One
+// partial sum per CTA.
+constexpr int kWgradPlanes = 108;   // 2 KB planes of dynamic shared memory
+
+__host__ __device__ inline int wgrad2_rows(int nch, int zc)
+{
+    const int rowp = 3 * nch + 1;
+    return (kWgradPlanes / 2 - 8 - 2 * rowp) / (rowp + zc);
+}
+
+constexpr int kWgradThreads = 256;
+
+template <int NZ>
+__global__ void __launch_bounds__(kWgradThreads, 1) wgrad2_kernel(const WgradParams P, int R, int ntx, int nty,
+                                                                  int ntiles)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    constexpr int kCols = 3 * NZ <= 64 ? 64 : 128;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int nch = P.xc0 + P.xc1, zc = P.zc, rowp = 3 * nch + 1;
+    const int stage_planes = (R + 2) * rowp + R * zc;
+    uint8_t *stage[2] = {smem, smem + (size_t)stage_planes * kZPlane};
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + (size_t)(2 * stage_planes + 16) * kZPlane);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
+    const size_t HW = (size_t)P.H * P.W;
+
+    const uint4 ones = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);   // bf16 1.0 x 8
+    for (int s = 0; s < 2; ++s)
+        for (int i = tid; i < (R + 2) * kPx; i += kWgradThreads)
+            *reinterpret_cast<uint4 *>(stage[s] + (size_t)((i / kPx) * rowp + 3 * nch) * kZPlane + 16 * (i % kPx)) =
+                ones;
+
+    // thread -> pixel px of the tile row; the two halves take alternate (row, tap) pairs
+    const int px = tid & (kPx - 1), half = tid >> 7;
+    auto load_tile = [&](int tile, uint8_t *st) {
+        const int tx = tile % ntx, ty = (tile / ntx) % nty, b = tile / (ntx * nty);
+        const int x0 = tx * kPx, y0 = ty * R;
+        for (int q = half; q < (R + 2) * 3; q += kWgradThreads / kPx) {
+            const int rr = q / 3, kx = q - 3 * rr;
+            const int gy = y0 - 1 + rr, gx = x0 - 1 + kx + px;
+            const bool in = gy >= 0 && gy < P.H && gx >= 0 && gx < P.W;
+            const size_t pix = b * HW + (size_t)(in ? gy : 0) * P.W + (in ? gx : 0);
+            uint8_t *d = st + (size_t)(rr * rowp + kx * nch) * kZPlane + 16 * px;
+            const __nv_bfloat16 *s0 = P.x0 + pix * (8 * P.xc0);
+            for (int c = 0; c < P.xc0; ++c) tc::cp16(d + (size_t)c * kZPlane, s0 + 8 * c, in ? 16u : 0u);
+            if (P.xc1) {
+                const __nv_bfloat16 *s1 = P.x1 + pix * (8 * P.xc1);
+                for (int c = 0; c < P.xc1; ++c)
+                    tc::cp16(d + (size_t)(P.xc0 + c) * kZPlane, s1 + 8 * c, in ? 16u : 0u);
+            }
+        }
+        for (int r = half; r < R; r += kWgradThreads / kPx) {
+            const int gy = y0 + r, gx = x0 + px;
+            const bool in = gy < P.H && gx < P.W;
+            const size_t pix = b * HW + (size_t)(in ? gy : 0) * P.W + (in ? gx : 0);
+            uint8_t *d = st + (size_t)((R + 2) * rowp + r * zc) * kZPlane + 16 * px;
+            for (int c = 0; c < zc; ++c) tc::cp16(d + (size_t)c * kZPlane, P.dz + pix * (8 * zc) + 8 * c, in ? 16u : 0u);
+        }
+    };
+
+    if (warp == 0) tc::tmem_alloc(tslot, kCols);
+    if (tid == 0) {
+        tc::mbar_init(&bar[0], 1);
+        tc::mbar_init(&bar[1], 1);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = *tslot;
+    const uint32_t idesc = tc::idesc_bf16(kPx, NZ) | (1u << 15) | (1u << 16);   // A and B MN-major
+
+    const int first = blockIdx.x, stride = gridDim.x;
+    if (first < ntiles) load_tile(first, stage[0]);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    uint32_t phase[2] = {0u, 0u};
+    bool ok = true;
+    int it = 0;
+    for (int tile = first; tile < ntiles && ok; tile += stride, ++it) {
+        const int s = it & 1;
+        if (it >= 1) {
+            // the other stage is free once the MMAs of the previous tile are done
+            ok = tc::mbar_wait(&bar[s ^ 1], phase[s ^ 1], kWaitIter);
+            phase[s ^ 1] ^= 1u;
+        }
+        if (ok && tile + stride < ntiles) load_tile(tile + stride, stage[s ^ 1]);
+        asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 1;" ::: "memory");
+        tc::fence_async_smem();
+        tc::fence_before_sync();
+        ok = __syncthreads_and(ok) != 0;   // one decision for the whole CTA
+        tc::fence_after_sync();
+        if (tid == 0 && ok) {
+            const uint32_t sa = tc::smem_u32(stage[s]);
+            const uint32_t sz = sa + (uint32_t)((R + 2) * rowp) * kZPlane;
+            for (int r = 0; r < R; ++r)
+                for (int g = 0; g < kPx / 16; ++g) {
+                    const uint64_t bd = tc::sdesc(sz + (uint32_t)(r * zc) * kZPlane + 256u * g, 128, kZPlane);
+                    for (int ky = 0; ky < 3; ++ky) {
+                        const uint32_t a = sa + (uint32_t)((r + ky) * rowp) * kZPlane + 256u * g;
+                        tc::mma_bf16(tbase + ky * NZ, tc::sdesc(a, 128, kZPlane), bd, idesc,
+                                     (it | r | g) ? 1u : 0u);
+                    }
+                }
+            tc::commit(&bar[s]);
+        }
+    }
+    // the last tile's MMAs (if the loop ended early, its stage's commit may be missing: bounded wait)
+    if (it >= 1 && ok) ok = tc::mbar_wait(&bar[(it - 1) & 1], phase[(it - 1) & 1], kWaitIter);
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    ok = __syncthreads_and(ok) != 0;
+    tc::fence_after_sync();
+    float *out = P.partial + (size_t)blockIdx.x * (9 * P.cin * P.cout + P.cout);
+    if (!ok) {
+        if (tid == 0) atomicExch(P.err, 1);
+    } else if (it >= 1 && warp < 4) {
+        const int m = warp * 32 + (tid & 31);
+        const int kx = m / (8 * nch), c = m - kx * 8 * nch;
+        for (int ky = 0; ky < 3; ++ky)
+#pragma unroll
+            for (int j = 0; j < NZ; j += 16) {
+                float v[16];
+                tc::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + ky * NZ + j, v);
+                if (kx < 3 && c < P.cin) {
+#pragma unroll
+                    for (int q = 0; q < 16; ++q)
+                        if (j + q < P.cout) out[((ky * 3 + kx) * P.cin + c) * P.cout + j + q] = v[q];
+                } else if (kx == 3 && c == 0 && ky == 1) {
+#pragma unroll
+                    for (int q = 0; q < 16; ++q)
+                        if (j + q < P.cout) out[9 * P.cin * P.cout + j + q] = v[q];
+                }
+            }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tbase, kCols);
+}
+
+template <int NZ>
+cudaError_t launch_wgrad2_t(const WgradParams &P, int B, int R, int grid, cudaStream_t st)
+{
+    const int nch = P.xc0 + P.xc1, rowp = 3 * nch + 1;
+    const size_t smem = (size_t)(2 * ((R + 2) * rowp + R * P.zc) + 16) * kZPlane + 64;
+    cudaError_t e = cudaFuncSetAttribute(wgrad2_kernel<NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int ntx = (P.W + kPx - 1) / kPx, nty = (P.H + R - 1) / R;
+    wgrad2_kernel<NZ><<<grid, kWgradThreads, smem, st>>>(P, R, ntx, nty, B * ntx * nty);
+    return cudaGetLastError();
 }
 
 constexpr int kWgradRows = 4;
@@ -405,16 +566,39 @@ cudaError_t launch_pack(const float *w, __nv_bfloat16 *dst, const PackTable &T, 
 
 size_t wgrad_tiles(int B, int H, int W) { return (size_t)B * ((W + kPx - 1) / kPx) * ((H + kWgradRows - 1) / kWgradRows); }
 
+// Partial-sum rows the weight gradient of this layer writes: one per CTA of
+// the persistent kernel (nch <= 5), one per tile otherwise.
+static bool wgrad_persistent(const WgradParams &P) { return P.xc0 + P.xc1 <= 5 && wgrad2_rows(P.xc0 + P.xc1, P.zc) >= 1; }
+
+static int sm_count()
+{
+    int dev = 0, n = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n;
+}
+
+int wgrad_partial_rows(const WgradParams &P, int B)
+{
+    if (!wgrad_persistent(P)) return (int)wgrad_tiles(B, P.H, P.W);
+    const int R = wgrad2_rows(P.xc0 + P.xc1, P.zc);
+    const int tiles = B * ((P.W + kPx - 1) / kPx) * ((P.H + R - 1) / R);
+    return tiles < sm_count() ? tiles : sm_count();
+}
+
 size_t wgrad_partial_floats(int B, int H, int W, int cin, int cout)
 {
-    return reduce_floats(9 * cin * cout + cout, (int)wgrad_tiles(B, H, W));
+    const size_t t = wgrad_tiles(B, H, W);
+    return reduce_floats(9 * cin * cout + cout, (int)(t > 1024 ? t : 1024));
 }
 
 cudaError_t launch_wgrad(const WgradParams &P, int B, cudaStream_t st)
 {
-    if (P.cout <= 16) return launch_wgrad_t<16>(P, B, st);
-    if (P.cout <= 32) return launch_wgrad_t<32>(P, B, st);
-    return cudaErrorInvalidValue;
+    if (P.cout > 32) return cudaErrorInvalidValue;
+    if (wgrad_persistent(P)) {
+        const int R = wgrad2_rows(P.xc0 + P.xc1, P.zc), grid = wgrad_partial_rows(P, B);
+        return P.cout <= 16 ? launch_wgrad2_t<16>(P, B, R, grid, st) : launch_wgrad2_t<32>(P, B, R, grid, st);
+    }
+    return P.cout <= 16 ? launch_wgrad_t<16>(P, B, st) : launch_wgrad_t<32>(P, B, st);
 }
 
 }  // namespace unet
