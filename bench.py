@@ -204,11 +204,8 @@ def pct(xs, q):
 
 
 def max_over_ranks(x, world):
-    if world > 1:
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
-    return x
+    from cross_denoiser_b200 import replicas
+    return replicas.max_over_ranks(x) if world > 1 else x
 
 
 # ---------------------------------------------------------------------------
