@@ -427,7 +427,20 @@ def run_mine(a, rank, world, device):
             evs = evs[a.warmup:]
             if evs:
                 fo[k] = round(statistics.mean(e0.elapsed_time(e1) for e0, e1 in evs), 4)
-        res["full_step"] = {"value": world * a.steps / (total * 1e-3), "unit": "frames/s",
+        # the same full step with the FP64 Cholesky fallback (condition estimate > 1e6):
+        # fallbacks per frame and its time
+        net2 = cd.unet.UNet(device, seed=a.seed)
+        fb = stepmod.FrameStep(stepmod.StepConfig(regression_width=a.win, filter_width=a.filter_win, fused=True,
+                                                  fp64_cond_limit=1e6),
+                               predictor=net2, on_gradients=net2.on_gradients)
+        counts = []
+        kf = max(1, min(a.steps, 20))
+        totf, _ = timed_steps(lambda f, t: counts.append(fb(f)["fp64_fallbacks"]), frames, 2, kf, stream)
+        counts = [int(c.item()) for c in counts[2:]]
+        fp64_fb = {"cond_limit": 1e6, "ms_per_step": totf / kf, "fallbacks_per_frame_mean": statistics.mean(counts),
+                   "fallbacks_per_frame_max": max(counts),
+                   "solves_per_frame": 2 * 3 * (H // 4) * (W // 4)}
+        res["full_step"] = {"value": world * a.steps / (total * 1e-3), "unit": "frames/s", "fp64_fallback": fp64_fb,
                             "ms_per_step": total / a.steps, "p50_ms": pct(ms, 50), "p99_ms": pct(ms, 99),
                             "network_ms": fo, "unet_error_flag": net.error_flag(),
                             "unet_tensor_flop_per_frame": unet_flop(H, W)}

@@ -28,6 +28,7 @@ SIGNATURES = {
     "cd_get_last_error": (ctypes.c_char_p, []),
     "cd_cross_regression_workspace_size": (_S, [_I, _I, _I, _I]),
     "cd_cross_regression": (_I, [_P] * 8 + [_I] * 6 + [_P, _S, _P]),
+    "cd_cross_regression_fp64_fallback": (_I, [_P] * 8 + [_I] * 6 + [_F, _P, _P, _S, _P]),
     "cd_cross_regression_grad_workspace_size": (_S, [_I] * 5),
     "cd_cross_regression_grad": (_I, [_P] * 12 + [_I] * 6 + [_P, _S, _P]),
     "cd_cross_regression_noalloc_capacity": (_S, []),
@@ -57,7 +58,7 @@ SIGNATURES = {
 
 # kernels each entry point launches (for the launch count of bench.py)
 KERNELS_PER_CALL = {
-    "cd_cross_regression": 3, "cd_cross_regression_grad": 8, "cd_spatial_filter": 1, "cd_spatial_filter_grad": 1, "cd_reproject": 1,
+    "cd_cross_regression": 3, "cd_cross_regression_fp64_fallback": 3, "cd_cross_regression_grad": 8, "cd_spatial_filter": 1, "cd_spatial_filter_grad": 1, "cd_reproject": 1,
     "cd_erode3x3": 1, "cd_temporal_screening": 1, "cd_erode_temporal_screening": 1,
     "cd_prepare_input": 1, "cd_aggregation_loss": 2, "cd_filter_aggregate": 2,
     "cd_unet_forward": 22, "cd_unet_backward": 42, "cd_adam_update": 2, "cd_unet_conv3x3": 2,

@@ -85,20 +85,20 @@ static cd_status check_regression(const char *op, int B, int H, int W, int win_s
     return CD_OK;
 }
 
-cd_status cd_cross_regression(const float *imga, const float *imgb, const float *albedo,
-                              const float *normal, float *outa, float *outb, float *vara,
-                              float *varb, int B, int H, int W, int win_size, int sparsity,
-                              int recon_scale, void *workspace, size_t workspace_bytes,
-                              cudaStream_t stream)
+static cd_status cross_regression_impl(const char *op, const float *imga, const float *imgb, const float *albedo,
+                                       const float *normal, float *outa, float *outb, float *vara, float *varb,
+                                       int B, int H, int W, int win_size, int sparsity, int recon_scale,
+                                       float cond_limit, unsigned *fallbacks, void *workspace,
+                                       size_t workspace_bytes, cudaStream_t stream)
 {
     g_err[0] = 0;
     if (!imga || !imgb || !albedo || !normal || !outa || !outb || !vara || !varb)
-        return fail(CD_EINVAL, "cross_regression: null tensor pointer");
-    cd_status s = check_regression("cross_regression", B, H, W, win_size, sparsity, recon_scale);
+        return fail(CD_EINVAL, "%s: null tensor pointer", op);
+    cd_status s = check_regression(op, B, H, W, win_size, sparsity, recon_scale);
     if (s != CD_OK) return s;
     const size_t need = cd_cross_regression_workspace_size(B, H, W, sparsity);
     if (workspace_bytes < need || (need > 0 && !workspace))
-        return fail(CD_ENOMEM, "cross_regression: workspace of %zu bytes needed, %zu given", need, workspace_bytes);
+        return fail(CD_ENOMEM, "%s: workspace of %zu bytes needed, %zu given", op, need, workspace_bytes);
 
     float *beta = static_cast<float *>(workspace);
     float *sda = beta + (size_t)2 * B * (H / sparsity) * (W / sparsity) * 18;
@@ -106,10 +106,36 @@ cd_status cd_cross_regression(const float *imga, const float *imgb, const float 
     if ((s = cuda_status(cd::launch_variance(imga, imgb, vara, varb, sda, sdb, B, H, W, stream), "variance")) != CD_OK)
         return s;
     if ((s = cuda_status(cd::launch_regression(imga, imgb, albedo, normal, vara, varb, sda, sdb, beta, B, H, W,
-                                               win_size, sparsity, stream), "regression")) != CD_OK)
+                                               win_size, sparsity, stream, nullptr, cond_limit, fallbacks),
+                         "regression")) != CD_OK)
         return s;
     return cuda_status(cd::launch_recon(imga, imgb, albedo, normal, vara, varb, sda, sdb, beta, outa, outb, B,
                                         H, W, win_size, sparsity, recon_scale, stream), "recon");
+}
+
+cd_status cd_cross_regression(const float *imga, const float *imgb, const float *albedo,
+                              const float *normal, float *outa, float *outb, float *vara,
+                              float *varb, int B, int H, int W, int win_size, int sparsity,
+                              int recon_scale, void *workspace, size_t workspace_bytes,
+                              cudaStream_t stream)
+{
+    return cross_regression_impl("cross_regression", imga, imgb, albedo, normal, outa, outb, vara, varb, B, H, W,
+                                 win_size, sparsity, recon_scale, 0.f, nullptr, workspace, workspace_bytes, stream);
+}
+
+cd_status cd_cross_regression_fp64_fallback(const float *imga, const float *imgb, const float *albedo,
+                                             const float *normal, float *outa, float *outb, float *vara,
+                                             float *varb, int B, int H, int W, int win_size, int sparsity,
+                                             int recon_scale, float cond_limit, unsigned int *fallback_count,
+                                             void *workspace, size_t workspace_bytes, cudaStream_t stream)
+{
+    if (!(cond_limit > 0.f)) {
+        g_err[0] = 0;
+        return fail(CD_EINVAL, "cross_regression_fp64_fallback: cond_limit must be > 0");
+    }
+    return cross_regression_impl("cross_regression_fp64_fallback", imga, imgb, albedo, normal, outa, outb, vara,
+                                 varb, B, H, W, win_size, sparsity, recon_scale, cond_limit, fallback_count,
+                                 workspace, workspace_bytes, stream);
 }
 
 size_t cd_cross_regression_grad_workspace_size(int B, int H, int W, int sparsity, int recon_scale)

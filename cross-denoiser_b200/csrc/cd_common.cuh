@@ -43,7 +43,8 @@ cudaError_t launch_variance(const float *imga, const float *imgb, float *vara, f
 cudaError_t launch_regression(const float *imga, const float *imgb, const float *albedo,
                               const float *normal, const float *vara, const float *varb,
                               const float *sda, const float *sdb, float *beta, int B, int H, int W,
-                              int win, int sparsity, cudaStream_t st, float *chol = nullptr);
+                              int win, int sparsity, cudaStream_t st, float *chol = nullptr,
+                              float cond_limit = 0.f, unsigned *fallbacks = nullptr);
 cudaError_t launch_recon(const float *imga, const float *imgb, const float *albedo,
                          const float *normal, const float *vara, const float *varb,
                          const float *sda, const float *sdb, const float *beta, float *outa,

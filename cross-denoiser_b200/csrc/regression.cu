@@ -143,7 +143,49 @@ CD_DEV void normal_tap(Normal &n, float3 ft, float3 fc, float3 y, float vt, floa
 // sqrt(max(1e-5, a_ii - s)), off-diagonals (1/L_jj) * (a_ji - s).
 // Lo (nullable) receives the factor, row-major packed lower triangle
 // (21 floats per channel), for the backward pass.
-CD_DEV void solve_channel(const Normal &n, int k, float *beta, float *Lo)
+//
+// FP64 fallback (cond_limit > 0, off by default): when the factor's pivots
+// give a condition estimate (max L_ii / min L_ii)^2 above cond_limit, the
+// same FP32 normal equations are factored and solved again in double and
+// *fallbacks is incremented.  The reference has no such path; with the
+// fallback off the result is the reference's.
+CD_DEV void solve_fp64(const float (*A)[kP], const float *X, int k, float *beta)
+{
+    double L[kP][kP];
+#pragma unroll
+    for (int i = 0; i < kP; ++i) {
+#pragma unroll
+        for (int j = 0; j <= i; ++j) {
+            double s = 0.0;
+#pragma unroll
+            for (int q = 0; q < j; ++q) s = fma(L[i][q], L[j][q], s);
+            if (i == j)
+                L[i][i] = sqrt(fmax(1e-12, (double)A[i][i] - s));
+            else
+                L[i][j] = ((double)A[j][i] - s) / L[j][j];
+        }
+    }
+    double Y[kP], bt[kP];
+#pragma unroll
+    for (int i = 0; i < kP; ++i) {
+        double s = X[i];
+#pragma unroll
+        for (int q = 0; q < i; ++q) s -= L[i][q] * Y[q];
+        Y[i] = s / L[i][i];
+    }
+#pragma unroll
+    for (int i = kP - 1; i >= 0; --i) {
+        double s = Y[i];
+#pragma unroll
+        for (int q = i + 1; q < kP; ++q) s -= L[q][i] * bt[q];
+        bt[i] = s / L[i][i];
+    }
+#pragma unroll
+    for (int r = 0; r < kP; ++r) beta[r * 3 + k] = (float)bt[r];
+}
+
+CD_DEV void solve_channel(const Normal &n, int k, float *beta, float *Lo, float cond_limit = 0.f,
+                          unsigned *fallbacks = nullptr)
 {
     float A[kP][kP];
     A[0][0] = n.a00; A[0][1] = n.a01[k]; A[0][2] = n.a02[k]; A[0][3] = n.a03; A[0][4] = n.a04; A[0][5] = n.a05;
@@ -174,6 +216,19 @@ CD_DEV void solve_channel(const Normal &n, int k, float *beta, float *Lo)
         for (int i = 0; i < kP; ++i)
 #pragma unroll
             for (int j = 0; j <= i; ++j) Lo[21 * k + i * (i + 1) / 2 + j] = L[i][j];
+    }
+    if (cond_limit > 0.f) {
+        float dmin = L[0][0], dmax = L[0][0];
+#pragma unroll
+        for (int i = 1; i < kP; ++i) {
+            dmin = fminf(dmin, L[i][i]);
+            dmax = fmaxf(dmax, L[i][i]);
+        }
+        if (dmax * dmax > cond_limit * (dmin * dmin)) {
+            solve_fp64(A, X, k, beta);
+            if (fallbacks) atomicAdd(fallbacks, 1u);
+            return;
+        }
     }
     float Y[kP];
     Y[0] = X[0] / L[0][0];
@@ -252,7 +307,7 @@ __global__ void __launch_bounds__(kThreads) regression_kernel(
     const float *__restrict__ albedo, const float *__restrict__ normal,
     const float *__restrict__ vara, const float *__restrict__ varb,
     const float *__restrict__ sda, const float *__restrict__ sdb, float *__restrict__ beta,
-    float *__restrict__ chol, int H, int W, int hw, int sp)
+    float *__restrict__ chol, float cond_limit, unsigned *__restrict__ fallbacks, int H, int W, int hw, int sp)
 {
     extern __shared__ float4 sm4[];
     const RowGeom g = row_geom(hw, sp);
@@ -353,9 +408,9 @@ __global__ void __launch_bounds__(kThreads) regression_kernel(
     const size_t cidx = (size_t)b * nb_img + (size_t)blockIdx.y * Ws + (i0 + lane);
     float *bo = beta + (size_t)buf * gridDim.z * nb_img * kBeta + cidx * kBeta;
     float *lo = chol ? chol + ((size_t)buf * gridDim.z * nb_img + cidx) * 63 : nullptr;
-    solve_channel(nm, 0, bo, lo);
-    solve_channel(nm, 1, bo, lo);
-    solve_channel(nm, 2, bo, lo);
+    solve_channel(nm, 0, bo, lo, cond_limit, fallbacks);
+    solve_channel(nm, 1, bo, lo, cond_limit, fallbacks);
+    solve_channel(nm, 2, bo, lo, cond_limit, fallbacks);
 }
 
 // ---------------------------------------------------------------------------
@@ -550,7 +605,8 @@ size_t recon_smem_bytes(int win, int sp, int rs) { return recon_smem(win / 2, sp
 cudaError_t launch_regression(const float *imga, const float *imgb, const float *albedo,
                               const float *normal, const float *vara, const float *varb,
                               const float *sda, const float *sdb, float *beta, int B, int H, int W,
-                              int win, int sp, cudaStream_t st, float *chol)
+                              int win, int sp, cudaStream_t st, float *chol, float cond_limit,
+                              unsigned *fallbacks)
 {
     const int hw = win / 2;
     const size_t smem = regression_smem(hw, sp);
@@ -560,7 +616,7 @@ cudaError_t launch_regression(const float *imga, const float *imgb, const float 
     const int Ws = W / sp, Hs = H / sp;
     dim3 grid((Ws + kCX - 1) / kCX, Hs, B);
     regression_kernel<<<grid, kThreads, smem, st>>>(imga, imgb, albedo, normal, vara, varb, sda, sdb, beta,
-                                                    chol, H, W, hw, sp);
+                                                    chol, cond_limit, fallbacks, H, W, hw, sp);
     return cudaGetLastError();
 }
 

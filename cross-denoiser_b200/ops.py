@@ -80,7 +80,8 @@ def _regression_args(imga, imgb, albedo, normal, win_size, sparsity, recon_scale
     return imga, imgb, albedo, normal, rs
 
 
-def _cross_regression_raw(imga, imgb, albedo, normal, win_size, sparsity, recon_scale):
+def _cross_regression_raw(imga, imgb, albedo, normal, win_size, sparsity, recon_scale, fp64_cond_limit=0.0,
+                          fallback_count=None):
     imga, imgb, albedo, normal, rs = _regression_args(imga, imgb, albedo, normal, win_size, sparsity,
                                                       recon_scale)
     B, H, W, _ = imga.shape
@@ -91,10 +92,16 @@ def _cross_regression_raw(imga, imgb, albedo, normal, win_size, sparsity, recon_
     varb = torch.empty_like(vara)
     nbytes = L.cd_cross_regression_workspace_size(B, H, W, int(sparsity))
     ws = torch.empty((max(nbytes, 1),), dtype=torch.uint8, device=imga.device)
-    _lib.check(L.cd_cross_regression(_ptr(imga), _ptr(imgb), _ptr(albedo), _ptr(normal),
-                                     _ptr(outa), _ptr(outb), _ptr(vara), _ptr(varb),
-                                     B, H, W, int(win_size), int(sparsity), rs,
-                                     _ptr(ws), nbytes, _stream()), "cross_regression")
+    common = (_ptr(imga), _ptr(imgb), _ptr(albedo), _ptr(normal), _ptr(outa), _ptr(outb), _ptr(vara), _ptr(varb),
+              B, H, W, int(win_size), int(sparsity), rs)
+    if fp64_cond_limit and fp64_cond_limit > 0:
+        if fallback_count is not None and (fallback_count.dtype != torch.int32 or not fallback_count.is_cuda):
+            raise ValueError("fallback_count must be a CUDA int32 tensor")
+        _lib.check(L.cd_cross_regression_fp64_fallback(*common, float(fp64_cond_limit),
+                                                       None if fallback_count is None else _ptr(fallback_count),
+                                                       _ptr(ws), nbytes, _stream()), "cross_regression_fp64_fallback")
+    else:
+        _lib.check(L.cd_cross_regression(*common, _ptr(ws), nbytes, _stream()), "cross_regression")
     return outa, outb, vara, varb
 
 
@@ -160,7 +167,7 @@ class _CrossRegressionFn(torch.autograd.Function):
 
 
 def cross_regression(imga, imgb, albedo, normal, win_size: int, sparsity: int,
-                     recon_scale: int = 1, name=None):
+                     recon_scale: int = 1, name=None, fp64_cond_limit: float = 0.0, fallback_count=None):
     """(outa, outb, out_vara, out_varb) = cross_regression(imga, imgb, albedo, normal, ...).
 
     Reference: REGISTER_OP("CrossRegression") ops/regression.cc:25-57 and
@@ -168,12 +175,18 @@ def cross_regression(imga, imgb, albedo, normal, win_size: int, sparsity: int,
     from imga's features, outb imga from imgb's; out_vara/out_varb are the
     3x3 variance estimates of imga/imgb.  Differentiable with respect to the
     four images through cross_regression_grad when any of them requires grad.
+
+    fp64_cond_limit > 0 (not in the reference) re-solves, in double, every
+    centre whose FP32 Cholesky pivots give a condition estimate above it and
+    adds the number of such (centre, channel) solves to `fallback_count` (a
+    CUDA int32 tensor) when given.
     """
     if torch.is_grad_enabled() and any(isinstance(t, torch.Tensor) and t.requires_grad
                                        for t in (imga, imgb, albedo, normal)):
         return _CrossRegressionFn.apply(imga, imgb, albedo, normal, int(win_size), int(sparsity),
                                         int(recon_scale))
-    return _cross_regression_raw(imga, imgb, albedo, normal, win_size, sparsity, recon_scale)
+    return _cross_regression_raw(imga, imgb, albedo, normal, win_size, sparsity, recon_scale, fp64_cond_limit,
+                                 fallback_count)
 
 
 # ---------------------------------------------------------------------------

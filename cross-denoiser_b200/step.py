@@ -50,6 +50,10 @@ class StepConfig:
     win_curr: int = WIN_CURR
     win_prev: int = WIN_PREV
     fused: bool = False
+    # > 0: re-solve ill-conditioned regression centres in FP64 (condition
+    # estimate above this value); the count per frame is returned as
+    # "fp64_fallbacks".  0 keeps the reference's FP32 solve.
+    fp64_cond_limit: float = 0.0
 
 
 @dataclass
@@ -84,7 +88,7 @@ def aggregation_forward_backward(sum1, sumw1, sum2, sumw2, alpha, success, succe
     o1s = sum1 / d1
     o2s = sum2 / d2
     out = (sum1 + sum2) / (sumw1 + sumw2 + e)
-    op = torch.where(opacity > 0, 1.0, 0.0)
+    op = torch.where(opacity > 0, 1.0, 0.0).to(sum1.dtype)
     s = success * success_prev
     a = s * alpha + (1 - s)
     out = (a * out + (1 - a) * prev_out) * op
@@ -135,8 +139,12 @@ class FrameStep:
         h = self.history
         y1, y2 = ops.prepare_input(color, f["color2"])
         albedo, normal = f["albedo"], f["normal"]
+        fallbacks = None
+        if cfg.fp64_cond_limit > 0:
+            fallbacks = torch.zeros((1,), dtype=torch.int32, device=color.device)
         ols1, ols2, _, _ = ops.cross_regression(y1, y2, albedo, normal, win_size=cfg.regression_width,
-                                                sparsity=cfg.sparsity)
+                                                sparsity=cfg.sparsity, fp64_cond_limit=cfg.fp64_cond_limit,
+                                                fallback_count=fallbacks)
         ones1 = torch.ones((B, H, W, 1), dtype=torch.float32, device=color.device)
         success, rep = ops.Reproject(f["mvec"], [h.out_log, h.ols1, h.ols2], f["linearZ"], h.linearZ, normal,
                                      h.normal, f["pnFwidth"], ones1, ones1)
@@ -169,4 +177,5 @@ class FrameStep:
             self.on_gradients(g_band, g_alpha)
         self.history = History(out_log, ols1, ols2, f["linearZ"], normal)
         return {"out": out, "out_log": out_log, "loss": loss, "avg_loss": avg, "ols1": ols1, "ols2": ols2,
-                "g_band": g_band, "g_alpha": g_alpha, "success": success}
+                "g_band": g_band, "g_alpha": g_alpha, "success": success, "band": band, "alpha": alpha,
+                "fp64_fallbacks": fallbacks}

@@ -82,6 +82,23 @@ CD_API cd_status cd_cross_regression(const float *imga, const float *imgb,
                               void *workspace, size_t workspace_bytes,
                               cudaStream_t stream);
 
+/* CrossRegression with an FP64 fallback for ill-conditioned centres (no     */
+/* counterpart in the reference).  Same as cd_cross_regression, except that  */
+/* a centre/channel whose FP32 Cholesky pivots give a condition estimate     */
+/* (max L_ii / min L_ii)^2 above cond_limit (> 0; 1e6 is the intended value) */
+/* is factored and solved again in double from the same FP32 normal         */
+/* equations, and *fallback_count (a device uint32, may be NULL) is          */
+/* incremented once per such centre and channel.  Outputs differ from the   */
+/* reference only at those centres.                                           */
+CD_API cd_status cd_cross_regression_fp64_fallback(const float *imga, const float *imgb,
+                              const float *albedo, const float *normal,
+                              float *outa, float *outb, float *vara, float *varb,
+                              int B, int H, int W,
+                              int win_size, int sparsity, int recon_scale,
+                              float cond_limit, unsigned int *fallback_count,
+                              void *workspace, size_t workspace_bytes,
+                              cudaStream_t stream);
+
 /* ------------------------------------------------------------------------ */
 /* CrossRegression backward (no counterpart in the reference, which          */
 /* registers a gradient only for SpatialFilter, scripts/ops.py:23-32; the     */

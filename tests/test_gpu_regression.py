@@ -93,3 +93,32 @@ def test_argument_errors(cd, cuda):
         cd.ops.cross_regression(x[:, :62], x[:, :62], x[:, :62], x[:, :62], win_size=15, sparsity=4)
     with pytest.raises(ValueError):
         cd.ops.cross_regression(x[:, :8, :8], x[:, :8, :8], x[:, :8, :8], x[:, :8, :8], win_size=17, sparsity=4)
+
+
+def test_fp64_fallback(cd, cuda):
+    """cd_cross_regression_fp64_fallback: with an unreachable limit nothing
+    falls back and the outputs are the reference path's bit for bit; with a
+    limit of 1 every (centre, channel, buffer) is re-solved in double, and
+    the outputs stay within the op tolerance of the FP64 restatement."""
+    from oracle import regression_fp64 as r64
+    y1, y2, alb, nrm = inputs(cd, 32, 48, seed=5)
+    win, sp = 9, 4
+    base = run(cd, y1, y2, alb, nrm, win, sp)
+    cnt = torch.zeros((1,), dtype=torch.int32, device="cuda:0")
+    o = cd.ops.cross_regression(T(y1), T(y2), T(alb), T(nrm), win_size=win, sparsity=sp, fp64_cond_limit=1e30,
+                                fallback_count=cnt)
+    torch.cuda.synchronize()
+    assert int(cnt.item()) == 0
+    for a, b in zip(o, base):
+        np.testing.assert_array_equal(N(a), b)
+    cnt.zero_()
+    o = cd.ops.cross_regression(T(y1), T(y2), T(alb), T(nrm), win_size=win, sparsity=sp, fp64_cond_limit=1.0,
+                                fallback_count=cnt)
+    torch.cuda.synchronize()
+    assert int(cnt.item()) == (32 // sp) * (48 // sp) * 3 * 2
+    ref = r64.cross_regression(*[torch.from_numpy(a).double() for a in (y1, y2, alb, nrm)], win, sp, 1)
+    for a, b, nm in zip(o, ref, ("outa", "outb", "vara", "varb")):
+        assert_close(N(a), b.numpy().astype(np.float32), f"fp64 fallback {nm}", atol=ATOL)
+    with pytest.raises(ValueError):
+        cd.ops._lib.check(cd.ops._lib.lib().cd_cross_regression_fp64_fallback(
+            *[None] * 8, 1, 32, 48, win, sp, 1, 0.0, None, None, 0, None), "cross_regression_fp64_fallback")

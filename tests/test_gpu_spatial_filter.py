@@ -10,6 +10,8 @@ from helpers import assert_close, golden, golden_names
 from oracle import oracle as orc
 from oracle import reference as ref
 
+from oracle.step_fp64 import filter_fp64  # noqa: E402
+
 pytestmark = pytest.mark.gpu
 
 
@@ -80,32 +82,6 @@ def test_autograd_matches_grad_op(cd, cuda):
     direct = cd.ops.spatial_filter_grad(*gs, *x, win_size=9)
     torch.cuda.synchronize()
     np.testing.assert_array_equal(N(band.grad), N(direct))
-
-
-def filter_fp64(imga, imgb, alb, nrm, band, win):
-    """Plain PyTorch FP64 restatement of the filter (ops/regression.cu.cc:84-195)
-    used for finite differences."""
-    B, H, W, _ = imga.shape
-    r = win // 2
-    idx_y = torch.arange(H).view(H, 1) + torch.arange(-r, r + 1).view(1, -1)
-    idx_x = torch.arange(W).view(W, 1) + torch.arange(-r, r + 1).view(1, -1)
-    mir = lambda i, n: torch.where(i >= n, 2 * n - 2 - i, i.abs())
-    iy, ix = mir(idx_y, H), mir(idx_x, W)
-
-    def win_of(img):  # [B,H,W,C] -> [B,H,W,win,win,C]
-        return img[:, iy][:, :, :, ix].permute(0, 1, 3, 2, 4, 5)
-
-    d = torch.arange(-r, r + 1, dtype=torch.float64) / r
-    pd = d.view(-1, 1) ** 2 + d.view(1, -1) ** 2
-    dist = lambda img: ((img[:, :, :, None, None, :] - win_of(img)) ** 2).sum(-1)
-    dA, dB, dAl, dN = dist(imga), dist(imgb), dist(alb), dist(nrm)
-    b = band[:, :, :, None, None, :]
-    eA = -b[..., 0] * dA - b[..., 2] * dAl - b[..., 3] * dN - b[..., 4] * pd
-    eB = -b[..., 1] * dB - b[..., 2] * dAl - b[..., 3] * dN - b[..., 4] * pd
-    wA, wB = eA.exp(), eB.exp()
-    acca = (wA[..., None] * win_of(imga)).sum((3, 4))
-    accb = (wB[..., None] * win_of(imgb)).sum((3, 4))
-    return acca, accb, wA.sum((3, 4))[..., None], wB.sum((3, 4))[..., None]
 
 
 def test_gradient_vs_fp64_finite_differences(cd, cuda):
