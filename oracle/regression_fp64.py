@@ -10,7 +10,8 @@ differences).  It follows the same formulas as oracle/cd_oracle.c:
   regression    ops/regression.cu.cc:367-475  (reflect-101 window, ridge 1e-3)
   block recon   ops/regression.cu.cc:289-365  (centre range with the iDivUp rule)
 
-Dense over all (pixel, centre) pairs with a mask, so only for small images.
+The reconstruction gathers, per output pixel, the centres of its clamped
+range (at most ceil((2 hw + 1) / s) + 1 per axis); small and medium images.
 The Cholesky pivot clamp max(1e-5, .) of the reference never binds for the
 ridge-regularised systems (their Schur complements are >= 1e-3) and is left
 out; the solve is torch.linalg.solve.
@@ -80,39 +81,44 @@ def _branch(y, f, v, alb, nrm, win, sp, rs):
     b = torch.einsum("bhwtki,bhwt,bhwtk->bhwki", X, w[..., 0], yt)
     beta = torch.linalg.solve(A, b.unsqueeze(-1)).squeeze(-1)   # [B,Hs,Ws,3,6]
 
-    # block reconstruction over all (output pixel, centre) pairs in range
+    # block reconstruction: for every output pixel, the centres of its clamped
+    # iDivUp range along each axis (at most K per axis), gathered with a mask
     Hr, Wr = H // rs, W // rs
+
+    def ranges(n_out, n, ncen):
+        lo = [max(0, idivup_c(p * rs - hw, sp)) for p in range(n_out)]
+        hi = [min((n - 1) // sp, (p * rs + hw) // sp) for p in range(n_out)]
+        K = max(h - l + 1 for l, h in zip(lo, hi))
+        idx = torch.tensor([[min(l + k, ncen - 1) for k in range(K)] for l in lo], device=dev)
+        ok = torch.tensor([[l + k <= h for k in range(K)] for l, h in zip(lo, hi)], device=dev)
+        return idx, ok                                       # [n_out, K]
+
+    jy, oky = ranges(Hr, H, Hs)
+    ix, okx = ranges(Wr, W, Ws)
+    Ky, Kx = jy.shape[1], ix.shape[1]
     py = torch.arange(Hr, device=dev) * rs
     px = torch.arange(Wr, device=dev) * rs
 
-    def in_range(pos, n, ncen):
-        lo = [max(0, idivup_c(int(p) - hw, sp)) for p in pos]
-        hi = [min((n - 1) // sp, (int(p) + hw) // sp) for p in pos]
-        i = torch.arange(ncen, device=dev)
-        return (i[None] >= torch.tensor(lo, device=dev)[:, None]) & (i[None] <= torch.tensor(hi, device=dev)[:, None])
+    def at_out(img):                                        # [B,Hr,Wr,1,1,C]
+        return img[:, py][:, :, px][:, :, :, None, None, :]
 
-    my = in_range(py, H, Hs)                                # [Hr,Hs]
-    mx = in_range(px, W, Ws)                                # [Wr,Ws]
-    mask = (my[:, None, :, None] & mx[None, :, None, :]).to(f.dtype)   # [Hr,Wr,Hs,Ws]
-
-    def at_out(img):
-        return img[:, py][:, :, px]                        # [B,Hr,Wr,C]
+    def at_cen(img):                                        # [B,Hr,Wr,Ky,Kx,C]
+        g = img[:, cy][:, :, cx]                            # [B,Hs,Ws,C]
+        return g[:, jy][:, :, :, ix].permute(0, 1, 3, 2, 4, 5)
 
     fp, ap, np_, vp, sp_ = at_out(f), at_out(alb), at_out(nrm), at_out(v), at_out(s)
-    fcc, acc, ncc = f[:, cy][:, :, cx], alb[:, cy][:, :, cx], nrm[:, cy][:, :, cx]
-    vcc, scc = v[:, cy][:, :, cx], s[:, cy][:, :, cx]
-    E = lambda t: t[:, :, :, None, None, :]                 # pixel side  [B,Hr,Wr,1,1,C]
-    C = lambda t: t[:, None, None, :, :, :]                 # centre side [B,1,1,Hs,Ws,C]
-    den2 = E(sp_) + C(scc) + 1e-2
-    dfp = E(fp) - C(fcc)
+    fcc, acc, ncc, vcc, scc = at_cen(f), at_cen(alb), at_cen(nrm), at_cen(v), at_cen(s)
+    den2 = sp_ + scc + 1e-2
+    dfp = fp - fcc
     d1p = dfp / den2
-    dap = E(ap) - C(acc)
-    dnp = E(np_) - C(ncc)
-    Bc = beta[:, None, None]                                # [B,1,1,Hs,Ws,3,6]
+    dap = ap - acc
+    dnp = np_ - ncc
+    Bc = beta[:, jy][:, :, :, ix].permute(0, 1, 3, 2, 4, 5, 6)   # [B,Hr,Wr,Ky,Kx,3,6]
     pred = (Bc[..., 0] + Bc[..., 1] * d1p + Bc[..., 2] * dap + Bc[..., 3] * dnp[..., 0:1]
             + Bc[..., 4] * dnp[..., 1:2] + Bc[..., 5] * dnp[..., 2:3])
-    distp = (dfp ** 2).sum(-1, keepdim=True) / (E(vp) + C(vcc) + 1e-4)
-    wp = (torch.exp(-distp) + 1e-7) * mask[None, :, :, :, :, None]
+    distp = (dfp ** 2).sum(-1, keepdim=True) / (vp + vcc + 1e-4)
+    mask = (oky[:, None, :, None] & okx[None, :, None, :]).to(f.dtype)[None, ..., None]   # [1,Hr,Wr,Ky,Kx,1]
+    wp = (torch.exp(-distp) + 1e-7) * mask
     num = (wp * pred).sum((3, 4))
     den_sum = wp.sum((3, 4))
     return torch.relu(num / torch.clamp(den_sum, min=1e-7))
