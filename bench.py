@@ -277,6 +277,51 @@ def regression_flop(H, W, win, sp):
     return taps * FLOP["regression_tap"] + pairs * FLOP["recon_pair"] + 2 * H * W * FLOP["variance_px"]
 
 
+def differentiation_costs(device, stream):
+    """512x512, batch 4, radius 7: the spatial filter's band gradient by
+    recomputation (this repository's design) against the reference's design
+    (the forward stores 128 B/px of partials, the gradient reads them), and
+    the regression backward: time per call and the extra device memory each
+    needs beyond the op's inputs and outputs."""
+    B, H, W, win = 4, 512, 512, 15
+    frames = make_frames(H, W, 2, 77, device)
+    f = frames[1]
+    ia, ib = torch.log1p(f["color"]), torch.log1p(f["color2"])
+    ia, ib, al, nr = [t.expand(B, -1, -1, -1).contiguous() for t in (ia, ib, f["albedo"], f["normal"])]
+    g = torch.Generator(device=device).manual_seed(78)
+    band = synth.random_band((B, H, W), g, device=device)
+    gs = [torch.randn((B, H, W, c), generator=g, device=device) for c in (3, 3, 1, 1)]
+
+    def timed(fn, n=20):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    out = {"shape": [B, H, W], "window": win}
+    fwd = timed(lambda: ops.spatial_filter(ia, ib, al, nr, band, win_size=win))
+    grd = timed(lambda: ops.spatial_filter_grad(*gs, ia, ib, al, nr, band, win_size=win))
+    part = ops.spatial_filter_stored(ia, ib, al, nr, band, win_size=win)[4]
+    fwd_s = timed(lambda: ops.spatial_filter_stored(ia, ib, al, nr, band, win_size=win))
+    grd_s = timed(lambda: ops.spatial_filter_grad_stored(*gs, part))
+    out["filter_recompute"] = {"forward_ms": round(fwd, 4), "grad_ms": round(grd, 4), "extra_bytes": 0}
+    out["filter_stored"] = {"forward_ms": round(fwd_s, 4), "grad_ms": round(grd_s, 4),
+                            "extra_bytes": part.numel() * 4}
+    y = [ia, ib, al, nr]
+    rf = timed(lambda: ops.cross_regression(*y, win_size=win, sparsity=4), n=10)
+    gu = [torch.randn((B, H, W, c), generator=g, device=device) for c in (3, 3, 1, 1)]
+    rb = timed(lambda: ops.cross_regression_grad(*gu, *y, win, 4, 1), n=10)
+    ws = cd._lib.lib().cd_cross_regression_grad_workspace_size(B, H, W, 4, 1)
+    out["regression"] = {"forward_ms": round(rf, 4), "backward_ms": round(rb, 4), "backward_workspace_bytes": int(ws)}
+    return out
+
+
 def unet_flop(H, W):
     """Tensor-core FLOP of one training step of the U-Net (forward + input and
     weight gradients of the 3x3 convolutions) at H x W, counting only the
@@ -449,6 +494,8 @@ def run_mine(a, rank, world, device):
     res["e2e"] = {"value": world * e2e_steps / (total * 1e-3), "unit": "frames/s", "steps": e2e_steps,
                   "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(out_host.numel() * 4 + 4),
                   "p50_ms": pct(ms, 50), "p99_ms": pct(ms, 99)}
+
+    res["differentiation"] = differentiation_costs(device, stream)
 
     # regression-width sweep (radius 5 / 7 / 9)
     if not a.no_sweep:
@@ -649,7 +696,8 @@ def main():
                         p99_ms=r["p99_ms"], plain=r["plain"], e2e=r["e2e"], gpu_launches=r["gpu_launches"],
                         roofline=r.get("roofline"), roofline_hbm=r.get("roofline_hbm"), cpu_baseline=cpu,
                         clocks=r["clocks"], per_op_ms=r["per_op_ms"],
-                        sweep_frames_per_s=r.get("sweep_frames_per_s"), full_step=r.get("full_step"))
+                        sweep_frames_per_s=r.get("sweep_frames_per_s"), full_step=r.get("full_step"),
+                        differentiation=r.get("differentiation"))
             print(json.dumps(line))
     finally:
         if world > 1:

@@ -35,6 +35,8 @@ SIGNATURES = {
     "cd_cross_regression_noalloc": (_I, [_P] * 8 + [_I] * 6 + [_P]),
     "cd_spatial_filter": (_I, [_P] * 9 + [_I] * 4 + [_P]),
     "cd_spatial_filter_grad": (_I, [_P] * 10 + [_I] * 4 + [_P]),
+    "cd_spatial_filter_stored": (_I, [_P] * 10 + [_I] * 4 + [_P]),
+    "cd_spatial_filter_grad_stored": (_I, [_P] * 6 + [_I] * 3 + [_P]),
     "cd_reproject": (_I, [_P, _I, _P, _P, _P] + [_P] * 8 + [_I] * 3 + [_P]),
     "cd_erode3x3": (_I, [_P, _P, _I, _I, _I, _P]),
     "cd_temporal_screening": (_I, [_P] * 10 + [_I] * 5 + [_P]),
@@ -58,7 +60,8 @@ SIGNATURES = {
 
 # kernels each entry point launches (for the launch count of bench.py)
 KERNELS_PER_CALL = {
-    "cd_cross_regression": 3, "cd_cross_regression_fp64_fallback": 3, "cd_cross_regression_grad": 8, "cd_spatial_filter": 1, "cd_spatial_filter_grad": 1, "cd_reproject": 1,
+    "cd_cross_regression": 3, "cd_cross_regression_fp64_fallback": 3, "cd_cross_regression_grad": 8, "cd_spatial_filter": 1, "cd_spatial_filter_grad": 1, "cd_spatial_filter_stored": 1, "cd_spatial_filter_grad_stored": 1,
+    "cd_reproject": 1,
     "cd_erode3x3": 1, "cd_temporal_screening": 1, "cd_erode_temporal_screening": 1,
     "cd_prepare_input": 1, "cd_aggregation_loss": 2, "cd_filter_aggregate": 2,
     "cd_unet_forward": 22, "cd_unet_backward": 42, "cd_adam_update": 2, "cd_unet_conv3x3": 2,

@@ -188,6 +188,42 @@ cd_status cd_spatial_filter(const float *imga, const float *imgb, const float *a
                        "spatial_filter");
 }
 
+cd_status cd_spatial_filter_stored(const float *imga, const float *imgb, const float *albedo, const float *normal,
+                                   const float *band, float *out_acca, float *out_accb, float *out_wgtsuma,
+                                   float *out_wgtsumb, float *partials, int B, int H, int W, int win_size,
+                                   cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!imga || !imgb || !albedo || !normal || !band || !out_acca || !out_accb || !out_wgtsuma || !out_wgtsumb ||
+        !partials)
+        return fail(CD_EINVAL, "spatial_filter_stored: null tensor pointer");
+    if (!dims_ok(B, H, W)) return fail(CD_EINVAL, "spatial_filter_stored: bad shape B=%d H=%d W=%d", B, H, W);
+    if (win_size < 1) return fail(CD_EINVAL, "spatial_filter_stored: win_size must be >= 1");
+    const int hw = win_size / 2;
+    if (hw >= H || hw >= W)
+        return fail(CD_EINVAL, "spatial_filter_stored: window radius %d must be smaller than the image (%dx%d)", hw,
+                    H, W);
+    if (cd::spatial_filter_smem_bytes(win_size) > kSmemLimit)
+        return fail(CD_EINVAL, "spatial_filter_stored: win_size %d exceeds the shared-memory tile", win_size);
+    return cuda_status(cd::launch_spatial_filter_store(imga, imgb, albedo, normal, band, out_acca, out_accb,
+                                                       out_wgtsuma, out_wgtsumb, partials, B, H, W, win_size,
+                                                       stream),
+                       "spatial_filter_stored");
+}
+
+cd_status cd_spatial_filter_grad_stored(const float *grad_acca, const float *grad_accb, const float *grad_wgtsuma,
+                                        const float *grad_wgtsumb, const float *partials, float *out_grad_band,
+                                        int B, int H, int W, cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!grad_acca || !grad_accb || !grad_wgtsuma || !grad_wgtsumb || !partials || !out_grad_band)
+        return fail(CD_EINVAL, "spatial_filter_grad_stored: null tensor pointer");
+    if (!dims_ok(B, H, W)) return fail(CD_EINVAL, "spatial_filter_grad_stored: bad shape B=%d H=%d W=%d", B, H, W);
+    return cuda_status(cd::launch_spatial_filter_grad_stored(grad_acca, grad_accb, grad_wgtsuma, grad_wgtsumb,
+                                                             partials, out_grad_band, B, H, W, stream),
+                       "spatial_filter_grad_stored");
+}
+
 cd_status cd_spatial_filter_grad(const float *grad_acca, const float *grad_accb,
                                  const float *grad_wgtsuma, const float *grad_wgtsumb,
                                  const float *imga, const float *imgb, const float *albedo,

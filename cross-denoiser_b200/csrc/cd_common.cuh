@@ -73,6 +73,14 @@ cudaError_t launch_spatial_filter_grad(const float *gacca, const float *gaccb, c
                                        const float *band, float *gband, int B, int H, int W,
                                        int win, cudaStream_t st);
 
+cudaError_t launch_spatial_filter_store(const float *imga, const float *imgb, const float *albedo,
+                                        const float *normal, const float *band, float *acca, float *accb,
+                                        float *wsa, float *wsb, float *partials, int B, int H, int W, int win,
+                                        cudaStream_t st);
+cudaError_t launch_spatial_filter_grad_stored(const float *gacca, const float *gaccb, const float *gwsa,
+                                              const float *gwsb, const float *partials, float *gband, int B, int H,
+                                              int W, cudaStream_t st);
+
 struct ReprojectList {
     const float *in[8];
     float *out[8];

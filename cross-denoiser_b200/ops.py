@@ -273,6 +273,42 @@ def spatial_filter(imga, imgb, albedo, normal, band, win_size: int, name=None):
     return _spatial_filter_raw(imga, imgb, albedo, normal, band, win_size)
 
 
+def spatial_filter_stored(imga, imgb, albedo, normal, band, win_size: int):
+    """(out_acca, out_accb, out_wgtsuma, out_wgtsumb, partials): the forward of
+    the reference's design, which keeps the band partials ([B,H,W,32] floats,
+    ops/regression.cc:218-225) for the gradient; see spatial_filter_grad_stored.
+    Same outputs as spatial_filter."""
+    imga = _img(imga, "imga", 3)
+    imgb = _img(imgb, "imgb", 3, imga)
+    albedo = _img(albedo, "albedo", 3, imga)
+    normal = _img(normal, "normal", 3, imga)
+    band = _img(band, "band", 5, imga)
+    B, H, W, _ = imga.shape
+    acca, accb = torch.empty_like(imga), torch.empty_like(imga)
+    wsa = imga.new_empty((B, H, W, 1))
+    wsb = torch.empty_like(wsa)
+    part = imga.new_empty((B, H, W, 32))
+    _lib.check(_lib.lib().cd_spatial_filter_stored(_ptr(imga), _ptr(imgb), _ptr(albedo), _ptr(normal), _ptr(band),
+                                                   _ptr(acca), _ptr(accb), _ptr(wsa), _ptr(wsb), _ptr(part), B, H,
+                                                   W, int(win_size), _stream()), "spatial_filter_stored")
+    return acca, accb, wsa, wsb, part
+
+
+def spatial_filter_grad_stored(grad_acca, grad_accb, grad_wgtsuma, grad_wgtsumb, partials):
+    """dL/dband from the partials stored by spatial_filter_stored (the
+    reference's SpatialFilterGradKernel data flow); equals spatial_filter_grad."""
+    ga = _img(grad_acca, "grad_acca", 3)
+    gb = _img(grad_accb, "grad_accb", 3, ga)
+    gwa = _img(grad_wgtsuma, "grad_wgtsuma", 1, ga)
+    gwb = _img(grad_wgtsumb, "grad_wgtsumb", 1, ga)
+    part = _img(partials, "partials", 32, ga)
+    B, H, W, _ = ga.shape
+    out = ga.new_empty((B, H, W, 5))
+    _lib.check(_lib.lib().cd_spatial_filter_grad_stored(_ptr(ga), _ptr(gb), _ptr(gwa), _ptr(gwb), _ptr(part),
+                                                        _ptr(out), B, H, W, _stream()), "spatial_filter_grad_stored")
+    return out
+
+
 # ---------------------------------------------------------------------------
 # Reproject
 # ---------------------------------------------------------------------------

@@ -195,6 +195,26 @@ CD_API cd_status cd_spatial_filter_grad(const float *grad_acca, const float *gra
                                  cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* SpatialFilter with stored partials: the reference's design (its forward   */
+/* keeps 2 x [B,H,W,16] floats of band partials for the gradient op,         */
+/* ops/regression.cc:218-225), kept for the recompute-vs-store measurement.  */
+/* partials: [B,H,W,32] floats (128 B/px) written by the forward and read by */
+/* the gradient; results are those of cd_spatial_filter and                  */
+/* cd_spatial_filter_grad bit for bit.                                        */
+/* ------------------------------------------------------------------------ */
+CD_API cd_status cd_spatial_filter_stored(const float *imga, const float *imgb,
+                                          const float *albedo, const float *normal,
+                                          const float *band,
+                                          float *out_acca, float *out_accb,
+                                          float *out_wgtsuma, float *out_wgtsumb,
+                                          float *partials, int B, int H, int W, int win_size,
+                                          cudaStream_t stream);
+CD_API cd_status cd_spatial_filter_grad_stored(const float *grad_acca, const float *grad_accb,
+                                               const float *grad_wgtsuma, const float *grad_wgtsumb,
+                                               const float *partials, float *out_grad_band,
+                                               int B, int H, int W, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
 /* Reproject                                                                  */
 /* Replaces REGISTER_OP("Reproject") + ReprojectOp::Compute                   */
 /* (ops/reproject.cc:34-69, 93-171) and ReprojectFunc                         */

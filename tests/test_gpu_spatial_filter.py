@@ -126,3 +126,19 @@ def test_argument_errors(cd, cuda):
         cd.ops.spatial_filter(x, x, x, x, b, win_size=17)          # radius 8 >= H
     with pytest.raises(ValueError):
         cd.ops.spatial_filter(x, x, x, x, b[..., :4], win_size=3)
+
+
+def test_stored_partials_variant_is_identical(cd, cuda):
+    """The stored-partials design (the reference's) gives the recomputing
+    kernels' results bit for bit."""
+    x = [T(a) for a in inputs(cd, 40, 72, seed=21, B=2)]
+    gs = [T(a) for a in upstream(2, 40, 72, seed=22)]
+    for win in (7, 15):
+        o = cd.ops.spatial_filter(*x, win_size=win)
+        gb = cd.ops.spatial_filter_grad(*gs, *x, win_size=win)
+        o2 = cd.ops.spatial_filter_stored(*x, win_size=win)
+        gb2 = cd.ops.spatial_filter_grad_stored(*gs, o2[4])
+        torch.cuda.synchronize()
+        for a, b in zip(o, o2[:4]):
+            np.testing.assert_array_equal(N(a), N(b))
+        np.testing.assert_array_equal(N(gb), N(gb2))
