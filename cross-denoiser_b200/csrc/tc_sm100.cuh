@@ -11,6 +11,7 @@
 // matrix by one pixel, which is how the convolutions address their taps.
 #pragma once
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace cd {
@@ -126,6 +127,39 @@ __device__ __forceinline__ void cp16(void *dst, const void *src, uint32_t src_by
 __device__ __forceinline__ void cp_wait_all()
 {
     asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Bulk and tensor (TMA) copies global -> shared, completing on an mbarrier
+// whose transaction count the issuing thread raised with mbar_expect_tx.
+// Loads only, no multicast.
+// ---------------------------------------------------------------------------
+bool make_rows_map(CUtensorMap *map, const void *base, int chunks, int W, int H, int B, int box_px, int box_rows);
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// `bytes` (multiple of 16) from 16-byte aligned global memory
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// one box of a 5-D tensor map at coordinates (c0 innermost .. c4)
+__device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3, int c4,
+                                            uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
+        "[%7];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+        : "memory");
 }
 
 }  // namespace tc

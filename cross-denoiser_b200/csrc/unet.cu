@@ -65,6 +65,11 @@ struct Layout {
     int steps_fwd[kLayers], steps_dg[kLayers];
 };
 
+// forward input split over the two sources of a concatenation (chunks of 8
+// channels): L7 reads [c3_3 | c2_2], L10 reads [c4_3 | c1_2]
+constexpr int kSrc0[kLayers] = {2, 1, 1, 2, 2, 4, 0, 4, 2, 0, 2, 0};
+constexpr int kSrc1[kLayers] = {0, 0, 0, 0, 0, 0, 0, 2, 0, 0, 1, 0};
+
 // pyramid level of each layer's input (0 full, 1 half, 2 quarter)
 constexpr int kLvl[kLayers] = {0, 0, 1, 1, 2, 2, 2, 1, 1, 1, 0, 0};
 
@@ -92,10 +97,10 @@ Layout layout(int B, int H, int W)
     for (int l = 0; l < kLayers; ++l) {
         const LayerDef &d = kDef[l];
         if (d.kind != CONV) continue;
-        L.steps_fwd[l] = build_steps(chunks(d.cin), st, hf);
+        L.steps_fwd[l] = build_steps(kSrc0[l], kSrc1[l], st, hf);
         L.pack_fwd[l] = o;
         o += align256((size_t)L.steps_fwd[l] * 2 * nout_of(d.cout) * 16);
-        L.steps_dg[l] = build_steps(chunks(d.cout), st, hf);
+        L.steps_dg[l] = build_steps(chunks(d.cout), 0, st, hf);
         L.pack_dg[l] = o;
         o += align256((size_t)L.steps_dg[l] * 2 * nout_of(d.cin) * 16);
     }
@@ -133,7 +138,7 @@ cudaError_t pack(const Ctx &c, int l, bool dgrad)
     const LayerDef &d = kDef[l];
     PackTable T{};
     KStep st[kMaxSteps];
-    T.nsteps = build_steps(chunks(dgrad ? d.cout : d.cin), st, T.half);
+    T.nsteps = dgrad ? build_steps(chunks(d.cout), 0, st, T.half) : build_steps(kSrc0[l], kSrc1[l], st, T.half);
     T.nout = nout_of(dgrad ? d.cin : d.cout);
     T.cin = d.cin;
     T.cout = d.cout;
@@ -149,7 +154,7 @@ cudaError_t conv(const Ctx &c, int l, bool dgrad, int lvl, Buf s0, int c0, Buf s
     const LayerDef &d = kDef[l];
     ConvParams P{};
     StepHalf hf[kMaxSteps][2];
-    P.nsteps = build_steps(c0 + c1, P.steps, hf);
+    P.nsteps = build_steps(c0, c1, P.steps, hf);
     P.src0 = c.buf(s0);
     P.src1 = c1 ? c.buf(s1) : nullptr;
     P.c0 = c0;
@@ -271,7 +276,7 @@ size_t conv_layer_workspace(int cin, int cout)
 {
     KStep st[kMaxSteps];
     StepHalf hf[kMaxSteps][2];
-    const int a = build_steps(chunks(cin), st, hf), b = build_steps(chunks(cout), st, hf);
+    const int a = build_steps(chunks(cin), 0, st, hf), b = build_steps(chunks(cout), 0, st, hf);
     const size_t fw = (size_t)a * 2 * nout_of(cout) * 16, dg = (size_t)b * 2 * nout_of(cin) * 16;
     return 256 + align256(fw > dg ? fw : dg);
 }
@@ -284,7 +289,7 @@ cudaError_t conv_layer(const float *w, const float *bias, const __nv_bfloat16 *x
     const int in_ch = dgrad ? cout : cin, out_ch = dgrad ? cin : cout;
     PackTable T{};
     KStep st_[kMaxSteps];
-    T.nsteps = build_steps(chunks(in_ch), st_, T.half);
+    T.nsteps = build_steps(chunks(in_ch), 0, st_, T.half);
     T.nout = nout_of(out_ch);
     T.cin = cin;
     T.cout = cout;
@@ -292,7 +297,7 @@ cudaError_t conv_layer(const float *w, const float *bias, const __nv_bfloat16 *x
     CD_TRY(launch_pack(w, wp, T, st));
     ConvParams P{};
     StepHalf hf[kMaxSteps][2];
-    P.nsteps = build_steps(chunks(in_ch), P.steps, hf);
+    P.nsteps = build_steps(chunks(in_ch), 0, P.steps, hf);
     P.src0 = x;
     P.c0 = chunks(in_ch);
     P.wpack = wp;

@@ -17,7 +17,7 @@ constexpr int kMaxSteps = 32;
 // the A view inside that row block (chunk plane + kx shift) and the byte
 // distance to its second 16-channel half.
 struct KStep {
-    int ky, a_off, a_lbo, pad;
+    int ky, a_off, a_lbo, src;   // src: which input source's staged rows
 };
 // What each half of a K step multiplies: tap (ky, kx) of input chunk `chunk`
 // (-1: unused, zero weights).
@@ -40,7 +40,7 @@ struct ConvParams {
     KStep steps[kMaxSteps];
 };
 
-int build_steps(int nch, KStep *steps, StepHalf (*half)[2]);
+int build_steps(int c0, int c1, KStep *steps, StepHalf (*half)[2]);
 int conv_rows(int nout, int nch);
 size_t conv_smem_bytes(int nsteps, int nout, int nch);
 cudaError_t launch_conv3x3(const ConvParams &P, int B, int nout, cudaStream_t st);

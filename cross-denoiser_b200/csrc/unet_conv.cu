@@ -47,13 +47,17 @@ inline size_t smem_for_tmem(size_t need, int cols)
     return need > cap ? need : cap;
 }
 
-__host__ __device__ inline size_t conv_smem(int nsteps, int nout, int nch, int R)
+__host__ __device__ inline size_t align128(size_t n) { return (n + 127) & ~(size_t)127; }
+
+__host__ __device__ inline size_t conv_smem(int nsteps, int nout, int c0, int c1, int R)
 {
-    return (size_t)b_bytes(nsteps, nout) + (size_t)(R + 2) * nch * kPlane + 16;
+    return (size_t)b_bytes(nsteps, nout) + align128((size_t)(R + 2) * c0 * kPlane) +
+           align128((size_t)(R + 2) * c1 * kPlane) + 16;
 }
 
 template <int NOUT, int R>
-__global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P)
+__global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P, const __grid_constant__ CUtensorMap m0,
+                                                      const __grid_constant__ CUtensorMap m1)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     constexpr int kCols = (R * NOUT <= 32) ? 32 : (R * NOUT <= 64) ? 64 : (R * NOUT <= 128) ? 128
@@ -61,55 +65,63 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P)
     static_assert(R * NOUT <= 512, "TMEM holds 512 columns");
     const int tid = threadIdx.x, warp = tid >> 5;
     const int x0 = blockIdx.x * kPx, y0 = blockIdx.y * R, b = blockIdx.z;
-    const int nch = P.c0 + P.c1;
     const int bb = b_bytes(P.nsteps, NOUT);
+    // [packed weights][source 0 rows][source 1 rows], blocks 128-byte aligned
+    const size_t blk0 = align128((size_t)(R + 2) * P.c0 * kPlane), blk1 = align128((size_t)(R + 2) * P.c1 * kPlane);
     uint8_t *sB = smem;
-    uint8_t *sA = smem + bb;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sA + (size_t)(R + 2) * nch * kPlane);
+    uint8_t *sA0 = smem + bb;
+    uint8_t *sA1 = sA0 + blk0;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sA1 + blk1);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
 
-    // stage the packed weights and the input rows (zero outside the image)
-    const uint8_t *wsrc = reinterpret_cast<const uint8_t *>(P.wpack);
-    for (int i = tid; i < bb / 16; i += 128) tc::cp16(sB + 16 * i, wsrc + 16 * i, 16);
-    const size_t HW = (size_t)P.H * P.W;
-    for (int i = tid; i < (R + 2) * kStagePx; i += 128) {
-        const int r = i / kStagePx, px = i - r * kStagePx;
-        const int gy = y0 - 1 + r, gx = x0 - 1 + px;
-        const bool in = gy >= 0 && gy < P.H && gx >= 0 && gx < P.W;
-        const size_t pix = b * HW + (size_t)(in ? gy : 0) * P.W + (in ? gx : 0);
-        uint8_t *d = sA + (size_t)r * nch * kPlane + 16 * px;
-        const __nv_bfloat16 *s0 = P.src0 + pix * (8 * P.c0);
-        for (int c = 0; c < P.c0; ++c) tc::cp16(d + (size_t)c * kPlane, s0 + 8 * c, in ? 16u : 0u);
-        if (P.c1) {
-            const __nv_bfloat16 *s1 = P.src1 + pix * (8 * P.c1);
-            for (int c = 0; c < P.c1; ++c) tc::cp16(d + (size_t)(P.c0 + c) * kPlane, s1 + 8 * c, in ? 16u : 0u);
-        }
-    }
+    // one TMA box per input source ([row][chunk][131 px][8 ch], zeros outside
+    // the image) and one bulk copy of the packed weights, on one mbarrier
     if (warp == 0) tc::tmem_alloc(tslot, kCols);
-    if (tid == 0) tc::mbar_init(bar, 1);
-    tc::cp_wait_all();
-    tc::fence_async_smem();
+    if (tid == 0) {
+        tc::mbar_init(bar, 1);
+        tc::fence_async_smem();
+    }
+    __syncthreads();   // barrier initialised before the copies are issued and waited on
+    if (tid == 0) {
+        const uint32_t bytes = (uint32_t)bb + (uint32_t)((R + 2) * (P.c0 + P.c1) * kPlane);
+        tc::mbar_expect_tx(bar, bytes);
+        tc::bulk_load(sB, P.wpack, (uint32_t)bb, bar);
+        tc::tma_load_5d(sA0, &m0, 0, x0 - 1, 0, y0 - 1, b, bar);
+        if (P.c1) tc::tma_load_5d(sA1, &m1, 0, x0 - 1, 0, y0 - 1, b, bar);
+    }
     tc::fence_before_sync();
     __syncthreads();
+    const bool staged = __syncthreads_and(tc::mbar_wait(bar, 0, kWaitIter)) != 0;
     tc::fence_after_sync();
     const uint32_t tbase = *tslot;
+    if (!staged) {
+        if (tid == 0) atomicExch(P.err, 1);
+        tc::fence_before_sync();
+        __syncthreads();
+        if (warp == 0) tc::tmem_dealloc(tbase, kCols);
+        return;
+    }
+    const size_t HW = (size_t)P.H * P.W;
 
     if (tid == 0) {
         const uint32_t idesc = tc::idesc_bf16(kPx, NOUT);
-        const uint32_t a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sB);
+        const uint32_t a0 = tc::smem_u32(sA0), a1 = tc::smem_u32(sA1), b0 = tc::smem_u32(sB);
         for (int r = 0; r < R; ++r)
             for (int s = 0; s < P.nsteps; ++s) {
                 const KStep st = P.steps[s];
-                const uint64_t ad = tc::sdesc(a0 + (uint32_t)((r + st.ky) * nch) * kPlane + st.a_off, st.a_lbo, 128);
+                const uint32_t base = st.src ? a1 + (uint32_t)((r + st.ky) * P.c1) * kPlane
+                                             : a0 + (uint32_t)((r + st.ky) * P.c0) * kPlane;
+                const uint64_t ad = tc::sdesc(base + st.a_off, st.a_lbo, 128);
                 const uint64_t bd = tc::sdesc(b0 + (uint32_t)(s * 2 * NOUT * 16), NOUT * 16, 128);
                 tc::mma_bf16(tbase + r * NOUT, ad, bd, idesc, s > 0 ? 1u : 0u);
             }
         tc::commit(bar);
     }
-    const bool done = __syncthreads_and(tc::mbar_wait(bar, 0, kWaitIter)) != 0;   // uniform across the CTA
+    // the commit completes the barrier's second phase (parity 1)
+    const bool done = __syncthreads_and(tc::mbar_wait(bar, 1, kWaitIter)) != 0;   // uniform across the CTA
     tc::fence_after_sync();
     if (!done) {
-        if (tid == 0) atomicExch(P.err, 1);
+        if (tid == 0) atomicExch(P.err, 2);
     } else {
         const int x = x0 + tid;
         const uint32_t lane_base = tbase + ((uint32_t)(warp * 32) << 16);
@@ -200,12 +212,19 @@ cudaError_t launch_t(const ConvParams &P, int B, cudaStream_t st)
 {
     constexpr int kCols = (R * NOUT <= 32) ? 32 : (R * NOUT <= 64) ? 64 : (R * NOUT <= 128) ? 128
                                                 : (R * NOUT <= 256) ? 256 : 512;
-    const size_t smem = smem_for_tmem(conv_smem(P.nsteps, NOUT, P.c0 + P.c1, R), kCols);
+    CUtensorMap m0, m1;
+    if (!tc::make_rows_map(&m0, P.src0, P.c0, P.W, P.H, B, kStagePx, R + 2)) return cudaErrorInvalidValue;
+    if (P.c1) {
+        if (!tc::make_rows_map(&m1, P.src1, P.c1, P.W, P.H, B, kStagePx, R + 2)) return cudaErrorInvalidValue;
+    } else {
+        m1 = m0;
+    }
+    const size_t smem = smem_for_tmem(conv_smem(P.nsteps, NOUT, P.c0, P.c1, R), kCols);
     cudaError_t e = cudaFuncSetAttribute(conv3x3_kernel<NOUT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid((P.W + kPx - 1) / kPx, (P.H + R - 1) / R, B);
-    conv3x3_kernel<NOUT, R><<<grid, 128, smem, st>>>(P);
+    conv3x3_kernel<NOUT, R><<<grid, 128, smem, st>>>(P, m0, m1);
     return cudaGetLastError();
 }
 
@@ -513,31 +532,36 @@ cudaError_t launch_wgrad_t(const WgradParams &P, int B, cudaStream_t st)
 
 int conv_rows(int nout, int nch) { return nout >= 32 ? 4 : (nch > 4 ? 4 : 8); }
 
-size_t conv_smem_bytes(int nsteps, int nout, int nch) { return conv_smem(nsteps, nout, nch, conv_rows(nout, nch)); }
+size_t conv_smem_bytes(int nsteps, int nout, int nch) { return conv_smem(nsteps, nout, nch, 0, conv_rows(nout, nch)); }
 
-// K-step table for `nch` input chunks (8 channels each): channel pairs of
+// K-step table for input chunks split over two sources (c0 chunks of source
+// 0, then c1 of source 1; 8 channels each), per source: channel pairs of
 // every tap, then, for an odd last chunk, tap pairs (kx, kx+1) with the
-// second half of (ky, 2, 3) unused.  half[h] = (ky, kx, chunk) or chunk -1.
-int build_steps(int nch, KStep *steps, StepHalf (*half)[2])
+// second half of (ky, 2, 3) unused.  half[h] = (ky, kx, chunk) with chunk the
+// conv input chunk over both sources, or chunk -1.
+int build_steps(int c0, int c1, KStep *steps, StepHalf (*half)[2])
 {
     int n = 0;
-    for (int c = 0; c + 1 < nch; c += 2)
-        for (int ky = 0; ky < 3; ++ky)
-            for (int kx = 0; kx < 3; ++kx) {
-                steps[n] = KStep{ky, c * kPlane + kx * 16, kPlane, 0};
-                half[n][0] = StepHalf{ky, kx, c};
-                half[n][1] = StepHalf{ky, kx, c + 1};
-                ++n;
-            }
-    if (nch & 1) {
-        const int c = nch - 1;
-        for (int ky = 0; ky < 3; ++ky)
-            for (int kx = 0; kx < 3; kx += 2) {
-                steps[n] = KStep{ky, c * kPlane + kx * 16, 16, 0};
-                half[n][0] = StepHalf{ky, kx, c};
-                half[n][1] = kx + 1 < 3 ? StepHalf{ky, kx + 1, c} : StepHalf{0, 0, -1};
-                ++n;
-            }
+    for (int src = 0; src < 2; ++src) {
+        const int nc = src ? c1 : c0, g0 = src ? c0 : 0;
+        for (int c = 0; c + 1 < nc; c += 2)
+            for (int ky = 0; ky < 3; ++ky)
+                for (int kx = 0; kx < 3; ++kx) {
+                    steps[n] = KStep{ky, c * kPlane + kx * 16, kPlane, src};
+                    half[n][0] = StepHalf{ky, kx, g0 + c};
+                    half[n][1] = StepHalf{ky, kx, g0 + c + 1};
+                    ++n;
+                }
+        if (nc & 1) {
+            const int c = nc - 1;
+            for (int ky = 0; ky < 3; ++ky)
+                for (int kx = 0; kx < 3; kx += 2) {
+                    steps[n] = KStep{ky, c * kPlane + kx * 16, 16, src};
+                    half[n][0] = StepHalf{ky, kx, g0 + c};
+                    half[n][1] = kx + 1 < 3 ? StepHalf{ky, kx + 1, g0 + c} : StepHalf{0, 0, -1};
+                    ++n;
+                }
+        }
     }
     return n;
 }
@@ -602,4 +626,48 @@ cudaError_t launch_wgrad(const WgradParams &P, int B, cudaStream_t st)
 }
 
 }  // namespace unet
+}  // namespace cd
+
+namespace cd {
+namespace tc {
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// NHWC bf16 tensor with `chunks` x 8 channels viewed as 5-D {8 channels, W
+// pixels, chunks, H rows, B} (the chunk dimension's stride, 16 bytes, is
+// inside a pixel), boxes of {8, box_px, chunks, box_rows, 1}: a box lands in
+// shared memory as [row][chunk][pixel][8 channels], one 16-byte-per-pixel
+// chunk plane per (row, chunk).
+bool make_rows_map(CUtensorMap *map, const void *base, int chunks, int W, int H, int B, int box_px, int box_rows)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn || chunks < 1 || box_px > 256 || box_rows > 256 || chunks > 256) return false;
+    const cuuint64_t C = (cuuint64_t)chunks * 8;
+    const cuuint64_t dims[5] = {8, (cuuint64_t)W, (cuuint64_t)chunks, (cuuint64_t)H, (cuuint64_t)B};
+    const cuuint64_t strides[4] = {C * 2, 16, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+    const cuuint32_t box[5] = {8, (cuuint32_t)box_px, (cuuint32_t)chunks, (cuuint32_t)box_rows, 1};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void *>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace tc
 }  // namespace cd
