@@ -13,6 +13,8 @@
 // 31,414 parameters.  Activations and activation gradients are bf16 NHWC
 // in the workspace; the forward keeps every activation for the backward.
 #include <cstring>
+#include <mutex>
+#include <unordered_map>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
@@ -61,7 +63,7 @@ size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
 // Workspace: [error flag][packed weights per conv: fwd, dgrad][buffers][partials]
 struct Layout {
-    size_t pack_fwd[kLayers], pack_dg[kLayers], buf[NBUF], partial, total;
+    size_t pack_fwd[kLayers], pack_dg[kLayers], buf[NBUF], partial, partial2, total;
     int steps_fwd[kLayers], steps_dg[kLayers];
 };
 
@@ -110,6 +112,8 @@ Layout layout(int B, int H, int W)
     }
     L.partial = o;
     o += align256(partial_floats(B, H, W) * sizeof(float));
+    L.partial2 = o;   // the weight gradients' partials (companion stream)
+    o += align256(partial_floats(B, H, W) * sizeof(float));
     L.total = o;
     return L;
 }
@@ -123,6 +127,7 @@ struct Ctx {
     __nv_bfloat16 *buf(Buf b) const { return reinterpret_cast<__nv_bfloat16 *>(ws + L.buf[b]); }
     int *err() const { return reinterpret_cast<int *>(ws); }
     float *partial() const { return reinterpret_cast<float *>(ws + L.partial); }
+    float *partial2() const { return reinterpret_cast<float *>(ws + L.partial2); }
     const float *w(int l) const { return params + param_offset(l); }
     const float *b(int l) const { return params + param_offset(l) + weight_count(l); }
 };
@@ -175,7 +180,9 @@ cudaError_t conv(const Ctx &c, int l, bool dgrad, int lvl, Buf s0, int c0, Buf s
     return launch_conv3x3(P, c.B, nout_of(dgrad ? d.cin : d.cout), c.st);
 }
 
-cudaError_t wgrad(const Ctx &c, float *grads, int l, int lvl, Buf x0, int xc0, Buf x1, int xc1, Buf dz)
+// Weight and bias gradient of layer l on stream `st` with partial buffer `part`.
+cudaError_t wgrad(const Ctx &c, float *grads, int l, int lvl, Buf x0, int xc0, Buf x1, int xc1, Buf dz,
+                  cudaStream_t st, float *part)
 {
     const LayerDef &d = kDef[l];
     WgradParams P{};
@@ -187,12 +194,44 @@ cudaError_t wgrad(const Ctx &c, float *grads, int l, int lvl, Buf x0, int xc0, B
     P.zc = chunks(d.cout);
     P.cin = d.cin;
     P.cout = d.cout;
-    P.partial = c.partial();
+    P.partial = part;
     P.H = c.H >> lvl;
     P.W = c.W >> lvl;
     P.err = c.err();
-    CD_TRY(launch_wgrad(P, c.B, c.st));
-    return launch_reduce(c.partial(), grads + param_offset(l), param_size(d), wgrad_partial_rows(P, c.B), c.st);
+    CD_TRY(launch_wgrad(P, c.B, st));
+    return launch_reduce(part, grads + param_offset(l), param_size(d), wgrad_partial_rows(P, c.B), st);
+}
+
+// A companion stream per caller stream (and device) for the weight
+// gradients, which depend only on their layer's dZ and the forward
+// activations: each is forked after the kernel that writes its dZ (event
+// record / wait, which stream capture records as graph edges) and overlaps
+// the rest of the input-gradient chain; backward() joins it before
+// returning.  Companions are created on first use outside stream capture;
+// inside a capture without one, the gradients stay on the caller's stream.
+struct Side {
+    cudaStream_t s = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+Side *side_stream(cudaStream_t main)
+{
+    static std::mutex mu;
+    static std::unordered_map<uint64_t, Side> sides;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    const uint64_t key = (reinterpret_cast<uint64_t>(main) << 8) ^ (uint64_t)dev;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = sides.find(key);
+    if (it != sides.end()) return &it->second;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(main, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return nullptr;
+    Side sd;
+    if (cudaStreamCreateWithFlags(&sd.s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+    if (cudaEventCreateWithFlags(&sd.fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sd.join, cudaEventDisableTiming) != cudaSuccess)
+        return nullptr;
+    return &(sides[key] = sd);
 }
 
 constexpr Buf NONE = NBUF;
@@ -230,46 +269,67 @@ cudaError_t backward(const float *gband, const float *galpha, const float *param
 {
     Ctx c{static_cast<uint8_t *>(ws), layout(B, H, W), B, H, W, st, params};
     const size_t n0 = (size_t)B * H * W;
-    for (int l = 1; l < kLayers; ++l)
-        if (kDef[l].kind == CONV) CD_TRY(pack(c, l, true));
-    // head
-    CD_TRY(launch_head_bwd(c.buf(C51), c.w(11), c.b(11), gband, galpha, c.buf(DZ10), c.partial(), n0, st));
-    CD_TRY(launch_reduce(c.partial(), grads + param_offset(11), 54, (int)head_blocks(n0), st));
-    // L10: 24 -> 8 at full resolution; input gradient splits into c4_3 and the c1_2 skip
-    CD_TRY(conv(c, 10, true, 0, DZ10, 1, NONE, 0, DC43, 2, DSK1, 1, NONE, NONE, NONE));
-    CD_TRY(wgrad(c, grads, 10, 0, C43, 2, C12, 1, DZ10));
-    // L9: transposed conv half -> full
-    CD_TRY(launch_tconv_bwd(16, 16, c.buf(C42), c.buf(DC43), c.w(9), c.buf(DZ8), c.partial(), H >> 1, W >> 1, B, st));
-    CD_TRY(launch_reduce(c.partial(), grads + param_offset(9), param_size(kDef[9]),
-                         (int)tconv_blocks(16, H >> 1, W >> 1, B), st));
-    // L8
-    CD_TRY(conv(c, 8, true, 1, DZ8, 2, NONE, 0, DZ7, 2, NONE, 0, C41, NONE, NONE));
-    CD_TRY(wgrad(c, grads, 8, 1, C41, 2, NONE, 0, DZ8));
-    // L7: 48 -> 16; input gradient splits into c3_3 and the c2_2 skip
-    CD_TRY(conv(c, 7, true, 1, DZ7, 2, NONE, 0, DC33, 4, DSK2, 2, NONE, NONE, NONE));
-    CD_TRY(wgrad(c, grads, 7, 1, C33, 4, C22, 2, DZ7));
-    // L6: transposed conv quarter -> half
-    CD_TRY(launch_tconv_bwd(32, 32, c.buf(C32), c.buf(DC33), c.w(6), c.buf(DZ5), c.partial(), H >> 2, W >> 2, B, st));
-    CD_TRY(launch_reduce(c.partial(), grads + param_offset(6), param_size(kDef[6]),
-                         (int)tconv_blocks(32, H >> 2, W >> 2, B), st));
-    // L5, L4
-    CD_TRY(conv(c, 5, true, 2, DZ5, 4, NONE, 0, DZ4, 4, NONE, 0, C31, NONE, NONE));
-    CD_TRY(wgrad(c, grads, 5, 2, C31, 4, NONE, 0, DZ5));
-    CD_TRY(conv(c, 4, true, 2, DZ4, 4, NONE, 0, DC23, 2, NONE, 0, NONE, NONE, NONE));
-    CD_TRY(wgrad(c, grads, 4, 2, C23, 2, NONE, 0, DZ4));
-    // pool of c2_2 + skip, ReLU of c2_2
-    CD_TRY(launch_pool_bwd(16, c.buf(C22), c.buf(C23), c.buf(DC23), c.buf(DSK2), c.buf(DZ3), H >> 1, W >> 1, B, st));
-    // L3, L2
-    CD_TRY(conv(c, 3, true, 1, DZ3, 2, NONE, 0, DZ2, 2, NONE, 0, C21, NONE, NONE));
-    CD_TRY(wgrad(c, grads, 3, 1, C21, 2, NONE, 0, DZ3));
-    CD_TRY(conv(c, 2, true, 1, DZ2, 2, NONE, 0, DC13, 1, NONE, 0, NONE, NONE, NONE));
-    CD_TRY(wgrad(c, grads, 2, 1, C13, 1, NONE, 0, DZ2));
-    // pool of c1_2 + skip, ReLU of c1_2
-    CD_TRY(launch_pool_bwd(8, c.buf(C12), c.buf(C13), c.buf(DC13), c.buf(DSK1), c.buf(DZ1), H, W, B, st));
-    // L1, L0
-    CD_TRY(conv(c, 1, true, 0, DZ1, 1, NONE, 0, DZ0, 1, NONE, 0, C11, NONE, NONE));
-    CD_TRY(wgrad(c, grads, 1, 0, C11, 1, NONE, 0, DZ1));
-    return wgrad(c, grads, 0, 0, X0, 2, NONE, 0, DZ0);
+    Side *side = side_stream(st);
+    // weight gradient of layer l, forked onto the companion stream when there is one
+    auto wg = [&](int l, int lvl, Buf x0, int xc0, Buf x1, int xc1, Buf dz) -> cudaError_t {
+        if (!side) return wgrad(c, grads, l, lvl, x0, xc0, x1, xc1, dz, st, c.partial2());
+        CD_TRY(cudaEventRecord(side->fork, st));
+        CD_TRY(cudaStreamWaitEvent(side->s, side->fork, 0));
+        return wgrad(c, grads, l, lvl, x0, xc0, x1, xc1, dz, side->s, c.partial2());
+    };
+    auto body = [&]() -> cudaError_t {
+        for (int l = 1; l < kLayers; ++l)
+            if (kDef[l].kind == CONV) CD_TRY(pack(c, l, true));
+        // head
+        CD_TRY(launch_head_bwd(c.buf(C51), c.w(11), c.b(11), gband, galpha, c.buf(DZ10), c.partial(), n0, st));
+        CD_TRY(launch_reduce(c.partial(), grads + param_offset(11), 54, (int)head_blocks(n0), st));
+        // L10: 24 -> 8 at full resolution; input gradient splits into c4_3 and the c1_2 skip
+        CD_TRY(wg(10, 0, C43, 2, C12, 1, DZ10));
+        CD_TRY(conv(c, 10, true, 0, DZ10, 1, NONE, 0, DC43, 2, DSK1, 1, NONE, NONE, NONE));
+        // L9: transposed conv half -> full
+        CD_TRY(launch_tconv_bwd(16, 16, c.buf(C42), c.buf(DC43), c.w(9), c.buf(DZ8), c.partial(), H >> 1, W >> 1, B,
+                                st));
+        CD_TRY(launch_reduce(c.partial(), grads + param_offset(9), param_size(kDef[9]),
+                             (int)tconv_blocks(16, H >> 1, W >> 1, B), st));
+        // L8
+        CD_TRY(wg(8, 1, C41, 2, NONE, 0, DZ8));
+        CD_TRY(conv(c, 8, true, 1, DZ8, 2, NONE, 0, DZ7, 2, NONE, 0, C41, NONE, NONE));
+        // L7: 48 -> 16; input gradient splits into c3_3 and the c2_2 skip
+        CD_TRY(wg(7, 1, C33, 4, C22, 2, DZ7));
+        CD_TRY(conv(c, 7, true, 1, DZ7, 2, NONE, 0, DC33, 4, DSK2, 2, NONE, NONE, NONE));
+        // L6: transposed conv quarter -> half
+        CD_TRY(launch_tconv_bwd(32, 32, c.buf(C32), c.buf(DC33), c.w(6), c.buf(DZ5), c.partial(), H >> 2, W >> 2, B,
+                                st));
+        CD_TRY(launch_reduce(c.partial(), grads + param_offset(6), param_size(kDef[6]),
+                             (int)tconv_blocks(32, H >> 2, W >> 2, B), st));
+        // L5, L4
+        CD_TRY(wg(5, 2, C31, 4, NONE, 0, DZ5));
+        CD_TRY(conv(c, 5, true, 2, DZ5, 4, NONE, 0, DZ4, 4, NONE, 0, C31, NONE, NONE));
+        CD_TRY(wg(4, 2, C23, 2, NONE, 0, DZ4));
+        CD_TRY(conv(c, 4, true, 2, DZ4, 4, NONE, 0, DC23, 2, NONE, 0, NONE, NONE, NONE));
+        // pool of c2_2 + skip, ReLU of c2_2
+        CD_TRY(launch_pool_bwd(16, c.buf(C22), c.buf(C23), c.buf(DC23), c.buf(DSK2), c.buf(DZ3), H >> 1, W >> 1, B,
+                               st));
+        // L3, L2
+        CD_TRY(wg(3, 1, C21, 2, NONE, 0, DZ3));
+        CD_TRY(conv(c, 3, true, 1, DZ3, 2, NONE, 0, DZ2, 2, NONE, 0, C21, NONE, NONE));
+        CD_TRY(wg(2, 1, C13, 1, NONE, 0, DZ2));
+        CD_TRY(conv(c, 2, true, 1, DZ2, 2, NONE, 0, DC13, 1, NONE, 0, NONE, NONE, NONE));
+        // pool of c1_2 + skip, ReLU of c1_2
+        CD_TRY(launch_pool_bwd(8, c.buf(C12), c.buf(C13), c.buf(DC13), c.buf(DSK1), c.buf(DZ1), H, W, B, st));
+        // L1, L0
+        CD_TRY(wg(1, 0, C11, 1, NONE, 0, DZ1));
+        CD_TRY(conv(c, 1, true, 0, DZ1, 1, NONE, 0, DZ0, 1, NONE, 0, C11, NONE, NONE));
+        return wg(0, 0, X0, 2, NONE, 0, DZ0);
+    };
+    const cudaError_t e = body();
+    if (side) {   // join, also after a failed launch, so no fork is left open
+        const cudaError_t e1 = cudaEventRecord(side->join, side->s);
+        const cudaError_t e2 = cudaStreamWaitEvent(st, side->join, 0);
+        if (e == cudaSuccess && e1 != cudaSuccess) return e1;
+        if (e == cudaSuccess && e2 != cudaSuccess) return e2;
+    }
+    return e;
 }
 
 size_t conv_layer_workspace(int cin, int cout)
