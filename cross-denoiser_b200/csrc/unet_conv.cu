@@ -528,6 +528,238 @@ cudaError_t launch_wgrad_t(const WgradParams &P, int B, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// Persistent weight gradient with the input rows staged once.  For input row
+// i and horizontal tap kx, per input source,
+//   D_{kx}[(ky, cout) x cin] += dZ_i^T[(ky, cout) x 16 px] X_i[16 px x cin]
+// where dZ_i stacks the output-gradient rows i + 1, i, i - 1 (ky = 0, 1, 2)
+// and X_i is input row i shifted by kx - 1 pixels.  Those three gradient rows
+// are consecutive staged rows, so the M groups (ky, chunk) of A sit one 2 KB
+// plane apart and one MMA covers all three kernel rows; the horizontal tap
+// is a 16-byte (one pixel) shift of the B view.  M = 128 rows cover 3 * ZC
+// chunk groups and B has cin rounded up to 16 columns: rows and columns past
+// them read other staged data and are discarded.  Both operands MN-major
+// (channels contiguous, pixels 16 bytes apart).
+//
+// A tile is R input rows x 128 pixels: one TMA box of output gradient (R + 2
+// rows from y0 - 1, 128 pixels) and one per input source (R rows, 131 pixels
+// from x0 - 1), zeros outside the image, land in a ring of S stages.  One
+// thread issues the MMAs of a stage and commits them to the stage's "empty"
+// barrier, then refills the previous stage; all threads sum the bias
+// gradient (the output gradient over the tile's R centre rows) from the
+// staged planes meanwhile.  CTAs are persistent and keep 3 x nsrc
+// accumulators in TMEM over all their tiles; one partial sum per CTA.
+constexpr int kWgrad3Smem = 225 * 1024;
+
+__host__ __device__ inline size_t align1k(size_t n) { return (n + 1023) & ~(size_t)1023; }
+
+struct Wgrad3Plan {
+    int R, S;
+    size_t zbytes, x0bytes, x1bytes, stage, smem;
+};
+
+inline Wgrad3Plan wgrad3_plan(int xc0, int xc1, int zc)
+{
+    Wgrad3Plan p{};
+    for (int R = 8; R >= 1; R >>= 1) {
+        p.R = R;
+        p.zbytes = (size_t)(R + 2) * zc * kZPlane;
+        p.x0bytes = (size_t)R * xc0 * kPlane;
+        p.x1bytes = (size_t)R * xc1 * kPlane;
+        p.stage = align1k(p.zbytes) + align1k(p.x0bytes) + align1k(p.x1bytes);
+        // tail: discarded A rows read up to 16 planes past a row's start
+        const size_t tail = 16 * (size_t)kZPlane + 2048;
+        const int S = (int)((kWgrad3Smem - tail) / p.stage);
+        p.S = S > 6 ? 6 : S;
+        p.smem = p.S * p.stage + tail;
+        if (p.S >= 3) break;
+    }
+    return p;
+}
+
+__host__ __device__ inline int pow2_cols(int n)
+{
+    int c = 32;
+    while (c < n) c <<= 1;
+    return c;
+}
+
+template <int ZC>
+__global__ void __launch_bounds__(kWgradThreads, 1)
+    wgrad3_kernel(const WgradParams P, const __grid_constant__ CUtensorMap mz, const __grid_constant__ CUtensorMap mx0,
+                  const __grid_constant__ CUtensorMap mx1, int R, int S, int stage_bytes, int ntx, int nty, int ntiles)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int xc0 = P.xc0, xc1 = P.xc1;
+    const int n0 = (8 * xc0 + 15) & ~15, n1 = (8 * xc1 + 15) & ~15, nacc = n0 + n1;
+    const uint32_t cols = (uint32_t)pow2_cols(3 * nacc);
+    const uint32_t zbytes = (uint32_t)((R + 2) * ZC * kZPlane), x0bytes = (uint32_t)(R * xc0 * kPlane),
+                   x1bytes = (uint32_t)(R * xc1 * kPlane);
+    const uint32_t x0off = (zbytes + 1023u) & ~1023u, x1off = x0off + ((x0bytes + 1023u) & ~1023u);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)S * stage_bytes + 16 * kZPlane);
+    uint64_t *empty = full + S;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(empty + S);
+    float *red = reinterpret_cast<float *>(smem + (size_t)S * stage_bytes + 16 * kZPlane + 1024);   // [8][8 * ZC]
+
+    auto issue = [&](int tile, int s) {
+        const int tx = tile % ntx, ty = (tile / ntx) % nty, b = tile / (ntx * nty);
+        const int x0 = tx * kPx, y0 = ty * R;
+        uint8_t *st = smem + (size_t)s * stage_bytes;
+        tc::mbar_expect_tx(&full[s], zbytes + x0bytes + x1bytes);
+        tc::tma_load_5d(st, &mz, 0, x0, 0, y0 - 1, b, &full[s]);
+        tc::tma_load_5d(st + x0off, &mx0, 0, x0 - 1, 0, y0, b, &full[s]);
+        if (xc1) tc::tma_load_5d(st + x1off, &mx1, 0, x0 - 1, 0, y0, b, &full[s]);
+    };
+
+    if (warp == 0) tc::tmem_alloc(tslot, cols);
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        tc::fence_async_smem();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = *tslot;
+    const uint32_t id0 = tc::idesc_bf16(kPx, n0) | (1u << 15) | (1u << 16);   // A and B MN-major
+    const uint32_t id1 = tc::idesc_bf16(kPx, n1 > 0 ? n1 : 16) | (1u << 15) | (1u << 16);
+
+    const int first = blockIdx.x, stride = gridDim.x;
+    int issued = 0;   // thread 0: loads issued, by iteration index
+    if (tid == 0)
+        for (; issued < S && first + issued * stride < ntiles; ++issued) issue(first + issued * stride, issued);
+
+    float bsum[8 * ZC];
+#pragma unroll
+    for (int j = 0; j < 8 * ZC; ++j) bsum[j] = 0.f;
+    const int px = tid & (kPx - 1), half = tid >> 7;
+    bool ok = true;
+    int it = 0;
+    for (int tile = first; tile < ntiles; tile += stride, ++it) {
+        const int s = it % S;
+        const bool got = tc::mbar_wait(&full[s], (uint32_t)(it / S) & 1u, kWaitIter);
+        ok = __syncthreads_and(ok && got) != 0;   // one decision for the whole CTA
+        if (!ok) break;
+        tc::fence_after_sync();
+        const uint8_t *st = smem + (size_t)s * stage_bytes;
+        if (tid == 0) {
+            const uint32_t sb = tc::smem_u32(st);
+            for (int r = 0; r < R; ++r)
+                for (int g = 0; g < kPx / 16; ++g) {
+                    const uint64_t ad = tc::sdesc(sb + (uint32_t)(r * ZC) * kZPlane + 256u * g, 128, kZPlane);
+                    const uint32_t acc = (it | r | g) ? 1u : 0u;
+                    for (int kx = 0; kx < 3; ++kx) {
+                        const uint32_t b0 = sb + x0off + (uint32_t)(r * xc0) * kPlane + 16u * kx + 256u * g;
+                        tc::mma_bf16(tbase + kx * nacc, ad, tc::sdesc(b0, 128, kPlane), id0, acc);
+                        if (xc1) {
+                            const uint32_t b1 = sb + x1off + (uint32_t)(r * xc1) * kPlane + 16u * kx + 256u * g;
+                            tc::mma_bf16(tbase + kx * nacc + n0, ad, tc::sdesc(b1, 128, kPlane), id1, acc);
+                        }
+                    }
+                }
+            tc::commit(&empty[s]);
+        }
+        // bias gradient: the tile's centre gradient rows (staged rows 1..R)
+        for (int r = 1 + half; r <= R; r += 2)
+#pragma unroll
+            for (int c = 0; c < ZC; ++c) {
+                const uint4 raw = *reinterpret_cast<const uint4 *>(st + (size_t)(r * ZC + c) * kZPlane + 16 * px);
+                const __nv_bfloat162 *h2 = reinterpret_cast<const __nv_bfloat162 *>(&raw);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const float2 f = __bfloat1622float2(h2[e]);
+                    bsum[8 * c + 2 * e] += f.x;
+                    bsum[8 * c + 2 * e + 1] += f.y;
+                }
+            }
+        // refill the previous iteration's stage once its MMAs are done
+        if (tid == 0 && it >= 1) {
+            const int pit = it - 1, ps = pit % S, nt = first + (pit + S) * stride;
+            if (nt < ntiles) {
+                if (tc::mbar_wait(&empty[ps], (uint32_t)(pit / S) & 1u, kWaitIter)) {
+                    issue(nt, ps);
+                    ++issued;
+                } else {
+                    ok = false;
+                }
+            }
+        }
+    }
+    // the last MMAs, and (after an early exit) the loads still in flight
+    bool fin = true;
+    if (tid == 0) {
+        if (it >= 1) fin = tc::mbar_wait(&empty[(it - 1) % S], (uint32_t)((it - 1) / S) & 1u, kWaitIter);
+        for (int j = it; j < issued; ++j) tc::mbar_wait(&full[j % S], (uint32_t)(j / S) & 1u, kWaitIter);
+    }
+    ok = __syncthreads_and(ok && fin) != 0;
+    tc::fence_after_sync();
+    float *out = P.partial + (size_t)blockIdx.x * (9 * P.cin * P.cout + P.cout);
+    if (!ok) {
+        if (tid == 0) atomicExch(P.err, 1);
+    } else if (it >= 1) {
+        // bias: lanes, then warps in a fixed order
+#pragma unroll
+        for (int j = 0; j < 8 * ZC; ++j) {
+            float v = bsum[j];
+#pragma unroll
+            for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) red[warp * 8 * ZC + j] = v;
+        }
+        __syncthreads();
+        if (tid < P.cout) {
+            float v = 0.f;
+            for (int w = 0; w < kWgradThreads / 32; ++w) v += red[w * 8 * ZC + tid];
+            out[9 * P.cin * P.cout + tid] = v;
+        }
+        if (warp < 4) {
+            const int m = warp * 32 + lane, kyp = m / (8 * ZC), co = m - kyp * 8 * ZC;
+            const bool valid = kyp < 3 && co < P.cout;
+            const int ky = 2 - kyp;
+            for (int kx = 0; kx < 3; ++kx)
+                for (int src = 0; src < (xc1 ? 2 : 1); ++src) {
+                    const int ns = src ? n1 : n0, creal = 8 * (src ? xc1 : xc0), cbase = src ? 8 * xc0 : 0;
+                    for (int j = 0; j < ns; j += 16) {
+                        float v[16];
+                        tc::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + kx * nacc + (src ? n0 : 0) + j, v);
+                        if (valid) {
+#pragma unroll
+                            for (int q = 0; q < 16; ++q) {
+                                const int ci = cbase + j + q;
+                                if (j + q < creal && ci < P.cin) out[((ky * 3 + kx) * P.cin + ci) * P.cout + co] = v[q];
+                            }
+                        }
+                    }
+                }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tbase, cols);
+}
+
+template <int ZC>
+cudaError_t launch_wgrad3_t(const WgradParams &P, int B, int grid, cudaStream_t st)
+{
+    const Wgrad3Plan p = wgrad3_plan(P.xc0, P.xc1, ZC);
+    if (p.S < 2) return cudaErrorInvalidValue;
+    CUtensorMap mz, mx0, mx1;
+    if (!tc::make_rows_map(&mz, P.dz, ZC, P.W, P.H, B, kPx, p.R + 2)) return cudaErrorInvalidValue;
+    if (!tc::make_rows_map(&mx0, P.x0, P.xc0, P.W, P.H, B, kStagePx, p.R)) return cudaErrorInvalidValue;
+    if (P.xc1) {
+        if (!tc::make_rows_map(&mx1, P.x1, P.xc1, P.W, P.H, B, kStagePx, p.R)) return cudaErrorInvalidValue;
+    } else {
+        mx1 = mx0;
+    }
+    cudaError_t e = cudaFuncSetAttribute(wgrad3_kernel<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+    if (e != cudaSuccess) return e;
+    const int ntx = (P.W + kPx - 1) / kPx, nty = (P.H + p.R - 1) / p.R;
+    wgrad3_kernel<ZC><<<grid, kWgradThreads, p.smem, st>>>(P, mz, mx0, mx1, p.R, p.S, (int)p.stage, ntx, nty,
+                                                            B * ntx * nty);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 int conv_rows(int nout, int nch) { return nout >= 32 ? 4 : (nch > 4 ? 4 : 8); }
@@ -601,8 +833,21 @@ static int sm_count()
     return n;
 }
 
+// The TMA-staged persistent kernel takes every layer whose output gradient
+// fits M (3 x 8 x zc <= 128) and whose accumulators fit TMEM.
+static bool wgrad3_fits(const WgradParams &P)
+{
+    const int n0 = (8 * P.xc0 + 15) & ~15, n1 = (8 * P.xc1 + 15) & ~15;
+    return P.zc >= 1 && P.zc <= 4 && 3 * (n0 + n1) <= 512 && wgrad3_plan(P.xc0, P.xc1, P.zc).S >= 2;
+}
+
 int wgrad_partial_rows(const WgradParams &P, int B)
 {
+    if (wgrad3_fits(P)) {
+        const int R = wgrad3_plan(P.xc0, P.xc1, P.zc).R;
+        const int tiles = B * ((P.W + kPx - 1) / kPx) * ((P.H + R - 1) / R);
+        return tiles < sm_count() ? tiles : sm_count();
+    }
     if (!wgrad_persistent(P)) return (int)wgrad_tiles(B, P.H, P.W);
     const int R = wgrad2_rows(P.xc0 + P.xc1, P.zc);
     const int tiles = B * ((P.W + kPx - 1) / kPx) * ((P.H + R - 1) / R);
@@ -618,6 +863,15 @@ size_t wgrad_partial_floats(int B, int H, int W, int cin, int cout)
 cudaError_t launch_wgrad(const WgradParams &P, int B, cudaStream_t st)
 {
     if (P.cout > 32) return cudaErrorInvalidValue;
+    if (wgrad3_fits(P)) {
+        const int grid = wgrad_partial_rows(P, B);
+        switch (P.zc) {
+        case 1: return launch_wgrad3_t<1>(P, B, grid, st);
+        case 2: return launch_wgrad3_t<2>(P, B, grid, st);
+        case 3: return launch_wgrad3_t<3>(P, B, grid, st);
+        default: return launch_wgrad3_t<4>(P, B, grid, st);
+        }
+    }
     if (wgrad_persistent(P)) {
         const int R = wgrad2_rows(P.xc0 + P.xc1, P.zc), grid = wgrad_partial_rows(P, B);
         return P.cout <= 16 ? launch_wgrad2_t<16>(P, B, R, grid, st) : launch_wgrad2_t<32>(P, B, R, grid, st);

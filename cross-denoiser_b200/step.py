@@ -54,6 +54,11 @@ class StepConfig:
     # estimate above this value); the count per frame is returned as
     # "fp64_fallbacks".  0 keeps the reference's FP32 solve.
     fp64_cond_limit: float = 0.0
+    # True: the predictor's training update (on_gradients: the U-Net
+    # backward and Adam) runs on a training stream of its own, overlapping
+    # the next frame's regression, reprojection and screening; the next
+    # prediction waits for it.  Same results as the serial order.
+    overlap_training: bool = False
 
 
 @dataclass
@@ -123,9 +128,40 @@ class FrameStep:
         self.history: Optional[History] = None
         self.fixed_band: Optional[torch.Tensor] = None
         self.fixed_alpha: Optional[torch.Tensor] = None
+        self._train_stream: Optional[torch.cuda.Stream] = None
+        self._trained: Optional[torch.cuda.Event] = None
+        self._held = None   # gradients the training stream may still be reading
 
     def reset(self):
         self.history = None
+
+    def wait_training(self, stream: Optional[torch.cuda.Stream] = None):
+        """Make `stream` (default: the current one) wait for the last training
+        update enqueued with overlap_training; call it before reading the
+        predictor's parameters."""
+        if self._trained is not None:
+            st = stream or torch.cuda.current_stream()
+            st.wait_event(self._trained)
+            if st == torch.cuda.current_stream():
+                # later allocations on this stream are ordered after the update,
+                # so the gradients' memory may be reused from here on
+                self._held = None
+
+    def _train(self, g_band, g_alpha, device):
+        if not self.cfg.overlap_training:
+            self.on_gradients(g_band, g_alpha)
+            return
+        if self._train_stream is None:
+            self._train_stream = torch.cuda.Stream(device)
+            self._trained = torch.cuda.Event()
+        ts = self._train_stream
+        ts.wait_stream(torch.cuda.current_stream(device))
+        with torch.cuda.stream(ts):
+            self.on_gradients(g_band, g_alpha)
+        self._trained.record(ts)
+        # the gradients were allocated on the compute stream: keep them alive
+        # until that stream has waited for this update (next prediction)
+        self._held = (g_band, g_alpha)
 
     def set_fixed_prediction(self, band: torch.Tensor, alpha: torch.Tensor):
         self.fixed_band, self.fixed_alpha = band, alpha
@@ -156,6 +192,7 @@ class FrameStep:
             prev_out, prev_ols1, prev_ols2, success_prev = ops.temporal_screening(
                 ols1, ols2, rep[0], rep[1], rep[2], success_f, win_curr=cfg.win_curr, win_prev=cfg.win_prev)
         if self.predictor is not None:
+            self.wait_training()
             band, alpha = self.predictor(ols1, ols2, prev_out, albedo, normal)
         else:
             band, alpha = self.fixed_band, self.fixed_alpha
@@ -174,8 +211,91 @@ class FrameStep:
             g_band = ops.spatial_filter_grad(g1, g2, gw1, gw2, ols1, ols2, albedo, normal, band,
                                              win_size=cfg.filter_width)
         if self.on_gradients is not None:
-            self.on_gradients(g_band, g_alpha)
+            self._train(g_band, g_alpha, color.device)
         self.history = History(out_log, ols1, ols2, f["linearZ"], normal)
         return {"out": out, "out_log": out_log, "loss": loss, "avg_loss": avg, "ols1": ols1, "ols2": ols2,
                 "g_band": g_band, "g_alpha": g_alpha, "success": success, "band": band, "alpha": alpha,
                 "fp64_fallbacks": fallbacks}
+
+
+class HostFramePipeline:
+    """Denoises frames held in host memory with the copies off the critical path.
+
+    ``pipe(host_frame)`` enqueues frame t: its inputs are copied to the device
+    on an upload stream, the step runs on the caller's current stream, and the
+    denoised frame (and the average loss) are read back on a download stream.
+    PCIe is full duplex and the copy engines run beside the SMs, so frame t+1
+    uploads and frame t-1 downloads while frame t computes; the frame rate is
+    bound by the slower of the upload and the step instead of their sum.
+
+    Frames of one stream keep their order: frame t+1 reads frame t's history,
+    and its linearZ and normal stay in frame t's input slot, so three slots
+    rotate (the slot of frame t+1 is free once frame t has finished reading
+    frame t-1's history).  Returns (out, avg_loss, event): pinned host tensors
+    that hold the result once ``event`` has completed, valid until the call
+    two frames later reuses them.  Host frames should be pinned for the
+    copies to be asynchronous.
+    """
+
+    SLOTS = 3
+
+    def __init__(self, step: FrameStep, device=None):
+        self.step = step
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.up = torch.cuda.Stream(self.device)
+        self.down = torch.cuda.Stream(self.device)
+        self.slots = None
+        self.t = 0
+        self.released = [torch.cuda.Event() for _ in range(self.SLOTS)]
+        self.uploaded = [torch.cuda.Event() for _ in range(self.SLOTS)]
+        self.computed = torch.cuda.Event()
+        self.read_back = [torch.cuda.Event() for _ in range(2)]
+        self.out_host = None
+        self.loss_host = None
+        self.pending = [None, None]   # device results being read back
+
+    def _alloc(self, host_frame):
+        self.slots = [{k: torch.empty(v.shape, dtype=v.dtype, device=self.device) for k, v in host_frame.items()}
+                      for _ in range(self.SLOTS)]
+        B, H, W, _ = host_frame["color"].shape
+        self.out_host = [torch.empty((B, H, W, 3), dtype=torch.float32).pin_memory() for _ in range(2)]
+        self.loss_host = [torch.empty((), dtype=torch.float32).pin_memory() for _ in range(2)]
+
+    def __call__(self, host_frame: Dict[str, torch.Tensor]):
+        if self.slots is None:
+            self._alloc(host_frame)
+        t, s, o = self.t, self.t % self.SLOTS, self.t % 2
+        compute = torch.cuda.current_stream(self.device)
+        if self.pending[o] is not None:
+            # frame t-2's results were allocated on the compute stream and read
+            # on the download stream: order later allocations after that read
+            compute.wait_event(self.read_back[o])
+            self.pending[o] = None
+        # slot s last held frame t-3, which frame t-2 read as history
+        if t >= self.SLOTS:
+            self.up.wait_event(self.released[s])
+        with torch.cuda.stream(self.up):
+            for k, v in host_frame.items():
+                self.slots[s][k].copy_(v, non_blocking=True)
+            self.uploaded[s].record(self.up)
+        compute.wait_event(self.uploaded[s])
+        r = self.step(self.slots[s])
+        if t >= 1:
+            # frame t has read frame t-1's linearZ/normal (its history)
+            self.released[(t - 1) % self.SLOTS].record(compute)
+        self.computed.record(compute)
+        # the host buffers of frame t-2 must have been read back before reuse
+        self.down.wait_event(self.computed)
+        with torch.cuda.stream(self.down):
+            self.out_host[o].copy_(r["out"], non_blocking=True)
+            self.loss_host[o].copy_(r["avg_loss"], non_blocking=True)
+            self.read_back[o].record(self.down)
+        self.pending[o] = (r["out"], r["avg_loss"])
+        self.t += 1
+        return self.out_host[o], self.loss_host[o], self.read_back[o]
+
+    def drain(self, stream=None):
+        """Make `stream` (default: the current one) wait for every enqueued copy."""
+        st = stream or torch.cuda.current_stream(self.device)
+        st.wait_stream(self.up)
+        st.wait_stream(self.down)

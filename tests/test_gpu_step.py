@@ -122,3 +122,65 @@ def test_frames_vs_cpu_oracle(cd, cuda):
         bad = ~np.isclose(N(o["out_log"]), ol, rtol=1e-4, atol=1e-5)
         assert bad.mean() < 2e-3, f"frame {t}: {bad.mean():.2e} of values differ"
         hist = dict(out_log=ol, ols1=o1, ols2=o2, linz=fr["linearZ"], nrm=fr["normal"])
+
+
+def _unet_frames(cd, H, W, seed, n, cuda):
+    seq = cd.synth.make_sequence(H, W, seed=seed, object_motion=2.0)
+    return [{k: v.to(cuda) for k, v in seq.frame(t).items() if k in cd.synth.FRAME_INPUTS} for t in range(n)]
+
+
+def test_overlapped_training_equals_serial(cd, cuda):
+    """The training update on its own stream, overlapping the next frame's
+    pre-network ops, gives the same frames, losses and network parameters as
+    the serial order (bit-identical: every kernel is deterministic)."""
+    H, W = 96, 128
+    fr = _unet_frames(cd, H, W, 21, 5, cuda)
+    runs = []
+    for overlap in (False, True):
+        net = cd.unet.UNet(cuda, seed=3)
+        st = cd.step.FrameStep(cd.step.StepConfig(regression_width=9, filter_width=7, fused=True,
+                                                  overlap_training=overlap),
+                               predictor=net, on_gradients=net.on_gradients)
+        outs = [st(f) for f in fr]
+        st.wait_training()
+        torch.cuda.synchronize()
+        runs.append(([N(o["out"]) for o in outs], [float(o["avg_loss"]) for o in outs], N(net.params)))
+    (o0, l0, p0), (o1, l1, p1) = runs
+    for t, (a, b) in enumerate(zip(o0, o1)):
+        assert_equal(a, b, f"frame {t} out")
+    assert l0 == l1
+    assert_equal(p0, p1, "parameters after 5 updates")
+
+
+def test_host_pipeline_equals_device_step(cd, cuda):
+    """Frames from pinned host memory through HostFramePipeline (uploads and
+    read-backs on copy streams) give the same denoised frames and losses as
+    the step on device-resident inputs."""
+    H, W = 64, 96
+    fr = _unet_frames(cd, H, W, 22, 6, cuda)
+    band = cd.synth.random_band((1, H, W), torch.Generator().manual_seed(5)).to(cuda)
+    alpha = torch.full((1, H, W, 1), 0.6, device=cuda)
+    cfg = cd.step.StepConfig(regression_width=9, filter_width=7, fused=True)
+    ref = cd.step.FrameStep(cfg)
+    ref.set_fixed_prediction(band, alpha)
+    want = [ref(f) for f in fr]
+    want = [(N(o["out"]), float(o["avg_loss"])) for o in want]
+    st = cd.step.FrameStep(cfg)
+    st.set_fixed_prediction(band, alpha)
+    pipe = cd.step.HostFramePipeline(st, cuda)
+    host = [{k: v.cpu().pin_memory() for k, v in f.items()} for f in fr]
+    for t, h in enumerate(host):
+        out, loss, ev = pipe(h)
+        ev.synchronize()
+        assert_equal(out.numpy(), want[t][0], f"frame {t} out")
+        assert float(loss) == want[t][1]
+    # back to back (copies overlapping the steps): the last two results
+    st2 = cd.step.FrameStep(cfg)
+    st2.set_fixed_prediction(band, alpha)
+    pipe2 = cd.step.HostFramePipeline(st2, cuda)
+    got = [pipe2(h) for h in host]
+    torch.cuda.synchronize()
+    for t in (len(host) - 2, len(host) - 1):
+        got[t][2].synchronize()
+        assert_equal(got[t][0].numpy(), want[t][0], f"frame {t} out (overlapped)")
+        assert float(got[t][1]) == want[t][1]

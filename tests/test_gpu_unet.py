@@ -100,6 +100,26 @@ def test_conv3x3_wgrad(cd, cuda, cin, cout):
     close_to_max(db.cpu(), bb.grad.float(), 2e-3, f"bgrad {cin}->{cout}")
 
 
+@pytest.mark.parametrize("cin,cout", [(8, 8), (15, 8), (32, 32), (48, 16)])
+def test_conv3x3_wgrad_many_tiles(cd, cuda, cin, cout):
+    """Enough tiles (2 x 512 x 1000) that every persistent CTA runs several
+    and the staging ring wraps around more than once."""
+    g = torch.Generator().manual_seed(cin * 3 + cout)
+    B, H, W = 2, 512, 1000
+    x = bf16(rand_act(B, H, W, cin, g))
+    dz = bf16(torch.randn((B, H, W, (cout + 7) // 8 * 8), generator=g))
+    dz[..., cout:] = 0
+    dW, db, ws = cd.unet.conv3x3_wgrad(x.to(DEV, torch.bfloat16), dz.to(DEV, torch.bfloat16), cin, cout)
+    torch.cuda.synchronize()
+    assert ws[:4].view(torch.int32).item() == 0
+    K = torch.zeros((3, 3, cin, cout), requires_grad=True)
+    bb = torch.zeros((cout,), requires_grad=True)
+    out = ut.conv3x3(x[..., :cin].permute(0, 3, 1, 2).double(), K.double(), bb.double(), relu=False)
+    out.backward(dz[..., :cout].permute(0, 3, 1, 2).double())
+    close_to_max(dW.cpu(), K.grad.float(), 2e-3, f"wgrad {cin}->{cout}")
+    close_to_max(db.cpu(), bb.grad.float(), 2e-3, f"bgrad {cin}->{cout}")
+
+
 def frame_inputs(B, H, W, seed):
     g = torch.Generator().manual_seed(seed)
     ols1 = torch.rand((B, H, W, 3), generator=g) * 3
