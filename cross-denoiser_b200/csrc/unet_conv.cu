@@ -528,33 +528,34 @@ cudaError_t launch_wgrad_t(const WgradParams &P, int B, cudaStream_t st)
     return cudaGetLastError();
 }
 
-// Persistent weight gradient with the input rows staged once.  For input row
-// i and horizontal tap kx, per input source,
-//   D_{kx}[(ky, cout) x cin] += dZ_i^T[(ky, cout) x 16 px] X_i[16 px x cin]
-// where dZ_i stacks the output-gradient rows i + 1, i, i - 1 (ky = 0, 1, 2)
-// and X_i is input row i shifted by kx - 1 pixels.  Those three gradient rows
-// are consecutive staged rows, so the M groups (ky, chunk) of A sit one 2 KB
-// plane apart and one MMA covers all three kernel rows; the horizontal tap
-// is a 16-byte (one pixel) shift of the B view.  M = 128 rows cover 3 * ZC
-// chunk groups and B has cin rounded up to 16 columns: rows and columns past
+// Persistent weight gradient: one MMA per input row and 16 pixels,
+//   D[(kx, cin) x (ky, cout)] += X_i^T[(kx, cin) x 16 px] dZ_i[16 px x (ky, cout)]
+// A holds input row i three times, shifted by kx - 1 pixels (planes [kx][chunk]
+// per source), so its M groups (kx, chunk) are consecutive 2 KB planes; B
+// holds the output-gradient rows i - 1, i, i + 1 (ky = 2, 1, 0), consecutive
+// staged rows, so its N groups (ky, chunk) are consecutive planes too.  M =
+// 128 rows cover 3 x nch chunk groups (a layer with more than 16 runs one MMA
+// per input source) and N is 24 x zc rounded up to 16: rows and columns past
 // them read other staged data and are discarded.  Both operands MN-major
 // (channels contiguous, pixels 16 bytes apart).
 //
 // A tile is R input rows x 128 pixels: one TMA box of output gradient (R + 2
-// rows from y0 - 1, 128 pixels) and one per input source (R rows, 131 pixels
-// from x0 - 1), zeros outside the image, land in a ring of S stages.  One
-// thread issues the MMAs of a stage and commits them to the stage's "empty"
-// barrier, then refills the previous stage; all threads sum the bias
-// gradient (the output gradient over the tile's R centre rows) from the
-// staged planes meanwhile.  CTAs are persistent and keep 3 x nsrc
-// accumulators in TMEM over all their tiles; one partial sum per CTA.
+// rows from y0 - 1) and, per input row, source and kx, one box of 128 pixels
+// from x0 - 1 + kx (the three copies come from L2), zeros outside the image,
+// land in a ring of S stages.  One thread issues the MMAs of a stage and
+// commits them to the stage's "empty" barrier, then refills the previous
+// stage; all threads sum the bias gradient (the output gradient over the
+// tile's R centre rows) from the staged planes meanwhile.  CTAs are
+// persistent and keep their accumulators in TMEM over all their tiles; one
+// partial sum per CTA.
 constexpr int kWgrad3Smem = 225 * 1024;
+constexpr int kWgrad3Tail = 16 * kZPlane + 2048;   // discarded A rows read up to 16 planes past a row
 
 __host__ __device__ inline size_t align1k(size_t n) { return (n + 1023) & ~(size_t)1023; }
 
 struct Wgrad3Plan {
     int R, S;
-    size_t zbytes, x0bytes, x1bytes, stage, smem;
+    size_t zbytes, xbytes, stage, smem;
 };
 
 inline Wgrad3Plan wgrad3_plan(int xc0, int xc1, int zc)
@@ -563,15 +564,12 @@ inline Wgrad3Plan wgrad3_plan(int xc0, int xc1, int zc)
     for (int R = 8; R >= 1; R >>= 1) {
         p.R = R;
         p.zbytes = (size_t)(R + 2) * zc * kZPlane;
-        p.x0bytes = (size_t)R * xc0 * kPlane;
-        p.x1bytes = (size_t)R * xc1 * kPlane;
-        p.stage = align1k(p.zbytes) + align1k(p.x0bytes) + align1k(p.x1bytes);
-        // tail: discarded A rows read up to 16 planes past a row's start
-        const size_t tail = 16 * (size_t)kZPlane + 2048;
-        const int S = (int)((kWgrad3Smem - tail) / p.stage);
+        p.xbytes = (size_t)R * 3 * (xc0 + xc1) * kZPlane;
+        p.stage = align1k(p.zbytes) + align1k(p.xbytes);
+        const int S = (int)((kWgrad3Smem - kWgrad3Tail) / p.stage);
         p.S = S > 6 ? 6 : S;
-        p.smem = p.S * p.stage + tail;
-        if (p.S >= 3) break;
+        p.smem = p.S * p.stage + kWgrad3Tail;
+        if (p.S >= 4) break;
     }
     return p;
 }
@@ -589,13 +587,13 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
                   const __grid_constant__ CUtensorMap mx1, int R, int S, int stage_bytes, int ntx, int nty, int ntiles)
 {
     extern __shared__ __align__(128) uint8_t smem[];
+    constexpr int N = (24 * ZC + 15) & ~15;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int xc0 = P.xc0, xc1 = P.xc1;
-    const int n0 = (8 * xc0 + 15) & ~15, n1 = (8 * xc1 + 15) & ~15, nacc = n0 + n1;
-    const uint32_t cols = (uint32_t)pow2_cols(3 * nacc);
-    const uint32_t zbytes = (uint32_t)((R + 2) * ZC * kZPlane), x0bytes = (uint32_t)(R * xc0 * kPlane),
-                   x1bytes = (uint32_t)(R * xc1 * kPlane);
-    const uint32_t x0off = (zbytes + 1023u) & ~1023u, x1off = x0off + ((x0bytes + 1023u) & ~1023u);
+    const int xc0 = P.xc0, xc1 = P.xc1, xc = xc0 + xc1;
+    const bool split = 3 * xc > 16;   // one MMA (accumulator) per source
+    const uint32_t cols = (uint32_t)pow2_cols(split ? 2 * N : N);
+    const uint32_t zbytes = (uint32_t)((R + 2) * ZC * kZPlane), xbytes = (uint32_t)(R * 3 * xc * kZPlane);
+    const uint32_t xoff = (zbytes + 1023u) & ~1023u;
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)S * stage_bytes + 16 * kZPlane);
     uint64_t *empty = full + S;
     uint32_t *tslot = reinterpret_cast<uint32_t *>(empty + S);
@@ -605,10 +603,16 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
         const int tx = tile % ntx, ty = (tile / ntx) % nty, b = tile / (ntx * nty);
         const int x0 = tx * kPx, y0 = ty * R;
         uint8_t *st = smem + (size_t)s * stage_bytes;
-        tc::mbar_expect_tx(&full[s], zbytes + x0bytes + x1bytes);
+        tc::mbar_expect_tx(&full[s], zbytes + xbytes);
         tc::tma_load_5d(st, &mz, 0, x0, 0, y0 - 1, b, &full[s]);
-        tc::tma_load_5d(st + x0off, &mx0, 0, x0 - 1, 0, y0, b, &full[s]);
-        if (xc1) tc::tma_load_5d(st + x1off, &mx1, 0, x0 - 1, 0, y0, b, &full[s]);
+        for (int r = 0; r < R; ++r)
+            for (int kx = 0; kx < 3; ++kx) {
+                uint8_t *row = st + xoff + (size_t)(r * 3 * xc) * kZPlane;
+                tc::tma_load_5d(row + (size_t)(kx * xc0) * kZPlane, &mx0, 0, x0 - 1 + kx, 0, y0 + r, b, &full[s]);
+                if (xc1)
+                    tc::tma_load_5d(row + (size_t)(3 * xc0 + kx * xc1) * kZPlane, &mx1, 0, x0 - 1 + kx, 0, y0 + r, b,
+                                    &full[s]);
+            }
     };
 
     if (warp == 0) tc::tmem_alloc(tslot, cols);
@@ -623,8 +627,7 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tbase = *tslot;
-    const uint32_t id0 = tc::idesc_bf16(kPx, n0) | (1u << 15) | (1u << 16);   // A and B MN-major
-    const uint32_t id1 = tc::idesc_bf16(kPx, n1 > 0 ? n1 : 16) | (1u << 15) | (1u << 16);
+    const uint32_t idesc = tc::idesc_bf16(kPx, N) | (1u << 15) | (1u << 16);   // A and B MN-major
 
     const int first = blockIdx.x, stride = gridDim.x;
     int issued = 0;   // thread 0: loads issued, by iteration index
@@ -648,16 +651,13 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
             const uint32_t sb = tc::smem_u32(st);
             for (int r = 0; r < R; ++r)
                 for (int g = 0; g < kPx / 16; ++g) {
-                    const uint64_t ad = tc::sdesc(sb + (uint32_t)(r * ZC) * kZPlane + 256u * g, 128, kZPlane);
+                    const uint64_t bd = tc::sdesc(sb + (uint32_t)(r * ZC) * kZPlane + 256u * g, 128, kZPlane);
+                    const uint32_t a0 = sb + xoff + (uint32_t)(r * 3 * xc) * kZPlane + 256u * g;
                     const uint32_t acc = (it | r | g) ? 1u : 0u;
-                    for (int kx = 0; kx < 3; ++kx) {
-                        const uint32_t b0 = sb + x0off + (uint32_t)(r * xc0) * kPlane + 16u * kx + 256u * g;
-                        tc::mma_bf16(tbase + kx * nacc, ad, tc::sdesc(b0, 128, kPlane), id0, acc);
-                        if (xc1) {
-                            const uint32_t b1 = sb + x1off + (uint32_t)(r * xc1) * kPlane + 16u * kx + 256u * g;
-                            tc::mma_bf16(tbase + kx * nacc + n0, ad, tc::sdesc(b1, 128, kPlane), id1, acc);
-                        }
-                    }
+                    tc::mma_bf16(tbase, tc::sdesc(a0, 128, kZPlane), bd, idesc, acc);
+                    if (split)
+                        tc::mma_bf16(tbase + N, tc::sdesc(a0 + (uint32_t)(3 * xc0) * kZPlane, 128, kZPlane), bd, idesc,
+                                     acc);
                 }
             tc::commit(&empty[s]);
         }
@@ -714,24 +714,38 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
             out[9 * P.cin * P.cout + tid] = v;
         }
         if (warp < 4) {
-            const int m = warp * 32 + lane, kyp = m / (8 * ZC), co = m - kyp * 8 * ZC;
-            const bool valid = kyp < 3 && co < P.cout;
-            const int ky = 2 - kyp;
-            for (int kx = 0; kx < 3; ++kx)
-                for (int src = 0; src < (xc1 ? 2 : 1); ++src) {
-                    const int ns = src ? n1 : n0, creal = 8 * (src ? xc1 : xc0), cbase = src ? 8 * xc0 : 0;
-                    for (int j = 0; j < ns; j += 16) {
-                        float v[16];
-                        tc::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + kx * nacc + (src ? n0 : 0) + j, v);
-                        if (valid) {
+            // TMEM lane m = row (group m / 8: source, kx, chunk; channel m % 8)
+            const int m = warp * 32 + lane, grp = m >> 3, e = m & 7;
+            for (int a = 0; a < (split ? 2 : 1); ++a) {
+                int kx = 3, ci = P.cin;   // invalid unless decoded below
+                if (split) {
+                    const int xs = a ? xc1 : xc0;
+                    if (grp < 3 * xs) {
+                        kx = grp / xs;
+                        ci = (a ? 8 * xc0 : 0) + 8 * (grp - kx * xs) + e;
+                    }
+                } else if (grp < 3 * xc0) {
+                    kx = grp / xc0;
+                    ci = 8 * (grp - kx * xc0) + e;
+                } else if (grp < 3 * xc) {
+                    const int g1 = grp - 3 * xc0;
+                    kx = g1 / xc1;
+                    ci = 8 * xc0 + 8 * (g1 - kx * xc1) + e;
+                }
+                const bool valid = kx < 3 && ci < P.cin;
 #pragma unroll
-                            for (int q = 0; q < 16; ++q) {
-                                const int ci = cbase + j + q;
-                                if (j + q < creal && ci < P.cin) out[((ky * 3 + kx) * P.cin + ci) * P.cout + co] = v[q];
-                            }
+                for (int j = 0; j < N; j += 16) {
+                    float v[16];
+                    tc::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + a * N + j, v);
+                    if (valid) {
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) {
+                            const int n = j + q, kyp = n / (8 * ZC), co = n - kyp * 8 * ZC;
+                            if (kyp < 3 && co < P.cout) out[(((2 - kyp) * 3 + kx) * P.cin + ci) * P.cout + co] = v[q];
                         }
                     }
                 }
+            }
         }
     }
     tc::fence_before_sync();
@@ -746,9 +760,9 @@ cudaError_t launch_wgrad3_t(const WgradParams &P, int B, int grid, cudaStream_t 
     if (p.S < 2) return cudaErrorInvalidValue;
     CUtensorMap mz, mx0, mx1;
     if (!tc::make_rows_map(&mz, P.dz, ZC, P.W, P.H, B, kPx, p.R + 2)) return cudaErrorInvalidValue;
-    if (!tc::make_rows_map(&mx0, P.x0, P.xc0, P.W, P.H, B, kStagePx, p.R)) return cudaErrorInvalidValue;
+    if (!tc::make_rows_map(&mx0, P.x0, P.xc0, P.W, P.H, B, kPx, 1)) return cudaErrorInvalidValue;
     if (P.xc1) {
-        if (!tc::make_rows_map(&mx1, P.x1, P.xc1, P.W, P.H, B, kStagePx, p.R)) return cudaErrorInvalidValue;
+        if (!tc::make_rows_map(&mx1, P.x1, P.xc1, P.W, P.H, B, kPx, 1)) return cudaErrorInvalidValue;
     } else {
         mx1 = mx0;
     }
@@ -833,12 +847,14 @@ static int sm_count()
     return n;
 }
 
-// The TMA-staged persistent kernel takes every layer whose output gradient
-// fits M (3 x 8 x zc <= 128) and whose accumulators fit TMEM.
+// The TMA-staged persistent kernel takes every layer whose (ky, cout) fit N
+// (zc <= 4) and whose (kx, cin) groups fit M per source.
 static bool wgrad3_fits(const WgradParams &P)
 {
-    const int n0 = (8 * P.xc0 + 15) & ~15, n1 = (8 * P.xc1 + 15) & ~15;
-    return P.zc >= 1 && P.zc <= 4 && 3 * (n0 + n1) <= 512 && wgrad3_plan(P.xc0, P.xc1, P.zc).S >= 2;
+    // M: 3 x chunks of one MMA within 16 groups (per source when split)
+    const int xc = P.xc0 + P.xc1;
+    const bool fits_m = 3 * xc <= 16 || (3 * P.xc0 <= 16 && 3 * P.xc1 <= 16);
+    return P.zc >= 1 && P.zc <= 4 && fits_m && wgrad3_plan(P.xc0, P.xc1, P.zc).S >= 2;
 }
 
 int wgrad_partial_rows(const WgradParams &P, int B)

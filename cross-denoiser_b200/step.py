@@ -131,6 +131,7 @@ class FrameStep:
         self._train_stream: Optional[torch.cuda.Stream] = None
         self._trained: Optional[torch.cuda.Event] = None
         self._held = None   # gradients the training stream may still be reading
+        self._side: Optional[torch.cuda.Stream] = None   # reprojection beside the regression
 
     def reset(self):
         self.history = None
@@ -173,17 +174,35 @@ class FrameStep:
         if self.history is None:
             self.history = History.zeros(B, H, W, color.device)
         h = self.history
-        y1, y2 = ops.prepare_input(color, f["color2"])
         albedo, normal = f["albedo"], f["normal"]
+
+        def reproject():
+            ones1 = torch.ones((B, H, W, 1), dtype=torch.float32, device=color.device)
+            return ops.Reproject(f["mvec"], [h.out_log, h.ols1, h.ols2], f["linearZ"], h.linearZ, normal,
+                                 h.normal, f["pnFwidth"], ones1, ones1)
+
+        compute = torch.cuda.current_stream(color.device)
+        if cfg.fused:
+            # reprojection (bandwidth-bound) needs only the history and this
+            # frame's G-buffer: run it on a side stream beside the (FP32-bound)
+            # regression.  The side stream first waits for all earlier work
+            # here, so memory it reuses is no longer read.
+            if self._side is None:
+                self._side = torch.cuda.Stream(color.device)
+            self._side.wait_stream(compute)
+            with torch.cuda.stream(self._side):
+                success, rep = reproject()
+        y1, y2 = ops.prepare_input(color, f["color2"])
         fallbacks = None
         if cfg.fp64_cond_limit > 0:
             fallbacks = torch.zeros((1,), dtype=torch.int32, device=color.device)
         ols1, ols2, _, _ = ops.cross_regression(y1, y2, albedo, normal, win_size=cfg.regression_width,
                                                 sparsity=cfg.sparsity, fp64_cond_limit=cfg.fp64_cond_limit,
                                                 fallback_count=fallbacks)
-        ones1 = torch.ones((B, H, W, 1), dtype=torch.float32, device=color.device)
-        success, rep = ops.Reproject(f["mvec"], [h.out_log, h.ols1, h.ols2], f["linearZ"], h.linearZ, normal,
-                                     h.normal, f["pnFwidth"], ones1, ones1)
+        if cfg.fused:
+            compute.wait_stream(self._side)
+        else:
+            success, rep = reproject()
         if cfg.fused:
             prev_out, prev_ols1, prev_ols2, success_prev, success_f = ops.erode_temporal_screening(
                 ols1, ols2, rep[0], rep[1], rep[2], success, cfg.win_curr, cfg.win_prev)
