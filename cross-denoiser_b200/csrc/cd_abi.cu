@@ -410,6 +410,9 @@ static bool unet_dims_ok(int B, int H, int W)
     return dims_ok(B, H, W) && H % 4 == 0 && W % 4 == 0 && H <= 4 * 65535;
 }
 
+// the tensor-core kernels stage activations and weights with bulk copies
+static bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
 size_t cd_unet_param_count(void) { return (size_t)cd::unet::param_count(); }
 
 size_t cd_unet_workspace_size(int B, int H, int W)
@@ -429,6 +432,7 @@ cd_status cd_unet_forward(const float *ols1, const float *ols2, const float *pre
     const size_t need = cd::unet::workspace_bytes(B, H, W);
     if (!workspace || workspace_bytes < need)
         return fail(CD_ENOMEM, "unet_forward: workspace of %zu bytes needed, %zu given", need, workspace_bytes);
+    if (!aligned16(workspace)) return fail(CD_EINVAL, "unet_forward: workspace not 16-byte aligned");
     return cuda_status(cd::unet::forward(ols1, ols2, prev_out, albedo, normal, params, band, alpha, workspace, B, H,
                                          W, stream),
                        "unet_forward");
@@ -444,6 +448,7 @@ cd_status cd_unet_backward(const float *grad_band, const float *grad_alpha, cons
     const size_t need = cd::unet::workspace_bytes(B, H, W);
     if (!workspace || workspace_bytes < need)
         return fail(CD_ENOMEM, "unet_backward: workspace of %zu bytes needed, %zu given", need, workspace_bytes);
+    if (!aligned16(workspace)) return fail(CD_EINVAL, "unet_backward: workspace not 16-byte aligned");
     return cuda_status(cd::unet::backward(grad_band, grad_alpha, params, grad_params, workspace, B, H, W, stream),
                        "unet_backward");
 }
@@ -475,6 +480,8 @@ cd_status cd_unet_conv3x3(const float *weight, const float *bias, const void *x,
     g_err[0] = 0;
     if (!weight || !x || !y || (!dgrad && !bias)) return fail(CD_EINVAL, "unet_conv3x3: null pointer");
     if (!conv_channels_ok(cin, cout)) return fail(CD_EINVAL, "unet_conv3x3: unsupported channels %d -> %d", cin, cout);
+    if (!aligned16(x) || !aligned16(y) || !aligned16(workspace))
+        return fail(CD_EINVAL, "unet_conv3x3: x, y and the workspace must be 16-byte aligned");
     if (!dims_ok(B, H, W) || H > 4 * 65535) return fail(CD_EINVAL, "unet_conv3x3: bad shape B=%d H=%d W=%d", B, H, W);
     const size_t need = cd::unet::conv_layer_workspace(cin, cout);
     if (!workspace || workspace_bytes < need)
@@ -497,6 +504,7 @@ cd_status cd_unet_conv3x3_wgrad(const void *x, const void *dz, float *grad, int 
     if (!x || !dz || !grad) return fail(CD_EINVAL, "unet_conv3x3_wgrad: null pointer");
     if (!conv_channels_ok(cin, cout))
         return fail(CD_EINVAL, "unet_conv3x3_wgrad: unsupported channels %d -> %d", cin, cout);
+    if (!aligned16(x) || !aligned16(dz)) return fail(CD_EINVAL, "unet_conv3x3_wgrad: x and dz must be 16-byte aligned");
     if (!dims_ok(B, H, W) || H > 4 * 65535)
         return fail(CD_EINVAL, "unet_conv3x3_wgrad: bad shape B=%d H=%d W=%d", B, H, W);
     const size_t need = cd::unet::wgrad_layer_workspace(cin, cout, B, H, W);

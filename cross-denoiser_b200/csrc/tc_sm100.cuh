@@ -6,9 +6,10 @@
 // and 16 bf16 columns is two "chunk planes" of 16 bytes per row, row i of
 // plane c at  start + c * LBO + i * 16.  Eight consecutive rows form one
 // 8x16-byte core matrix, so the stride between core matrices along M/N
-// (SBO) is 128 bytes.  A pixel row of an NHWC bf16 image with 8 channels per
-// chunk maps onto this directly: shifting the start by 16 bytes shifts the
-// matrix by one pixel, which is how the convolutions address their taps.
+// (SBO) is 128 bytes.  One row-chunk plane of a bf16 activation (unet.cuh),
+// 8 channels = 16 bytes per pixel, maps onto this directly: shifting the
+// start by 16 bytes shifts the matrix by one pixel, which is how the
+// convolutions address their taps.
 #pragma once
 #include <cstdint>
 #include <cuda.h>
@@ -130,12 +131,12 @@ __device__ __forceinline__ void cp_wait_all()
 }
 
 // ---------------------------------------------------------------------------
-// Bulk and tensor (TMA) copies global -> shared, completing on an mbarrier
-// whose transaction count the issuing thread raised with mbar_expect_tx.
-// Loads only, no multicast.
+// Bulk copies global -> shared, completing on an mbarrier whose transaction
+// count was raised with mbar_expect_tx.  Loads only, no multicast.
 // ---------------------------------------------------------------------------
-bool make_rows_map(CUtensorMap *map, const void *base, int chunks, int W, int H, int B, int box_px, int box_rows);
 
+// Arrive on the mbarrier (one of its expected arrivals) and raise its
+// transaction count by `bytes`.
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
@@ -149,17 +150,6 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
                      smem_u32(dst)),
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
-}
-
-// one box of a 5-D tensor map at coordinates (c0 innermost .. c4)
-__device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3, int c4,
-                                            uint64_t *bar)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
-        "[%7];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
-        : "memory");
 }
 
 }  // namespace tc

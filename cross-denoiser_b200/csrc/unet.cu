@@ -10,8 +10,9 @@
 //   L3  conv 16->16  half (+pool) L9  tconv 16->16  half->full
 //   L4  conv 16->32  quarter     L10 conv 24->8    full  (in: L9 | L1)
 //   L5  conv 32->32  quarter     L11 head 8->6 (1x1, fp32) -> band, alpha
-// 31,414 parameters.  Activations and activation gradients are bf16 NHWC
-// in the workspace; the forward keeps every activation for the backward.
+// 31,414 parameters.  Activations and activation gradients are bf16
+// row-chunk planes (unet.cuh) in the workspace; the forward keeps every
+// activation for the backward.
 #include <cstring>
 #include <mutex>
 #include <unordered_map>
@@ -249,7 +250,7 @@ cudaError_t forward(const float *ols1, const float *ols2, const float *prev, con
     const size_t n0 = (size_t)B * H * W;
     for (int l = 0; l < kLayers; ++l)
         if (kDef[l].kind == CONV) CD_TRY(pack(c, l, false));
-    CD_TRY(launch_pack_input(ols1, ols2, prev, albedo, normal, c.buf(X0), n0, st));
+    CD_TRY(launch_pack_input(ols1, ols2, prev, albedo, normal, c.buf(X0), n0, W, st));
     CD_TRY(conv(c, 0, false, 0, X0, 2, NONE, 0, C11, 1, NONE, 0, NONE, NONE, NONE));
     CD_TRY(conv(c, 1, false, 0, C11, 1, NONE, 0, C12, 1, NONE, 0, NONE, NONE, C13));
     CD_TRY(conv(c, 2, false, 1, C13, 1, NONE, 0, C21, 2, NONE, 0, NONE, NONE, NONE));

@@ -1,7 +1,7 @@
 // Internal interface of the U-Net kernels (unet_conv.cu, unet_ops.cu,
-// unet.cu).  Activations are NHWC bf16 with 8 channels per 16-byte chunk;
-// parameters are fp32 masters in Keras layout, packed to bf16 tensor-core
-// operands after every update.
+// unet.cu).  Activations are bf16 in row-chunk planes (below); parameters
+// are fp32 masters in Keras layout, packed to bf16 tensor-core operands after
+// every update.
 #pragma once
 #include <cstddef>
 #include <cstdint>
@@ -10,6 +10,18 @@
 
 namespace cd {
 namespace unet {
+
+// Activation layout: [B][H][nch][W][8] bf16, nch = channels / 8 (channels
+// padded to a multiple of 8 with zeros).  Each (row, chunk) is a contiguous
+// plane of 16 bytes per pixel, so a row segment of one chunk is one bulk copy
+// into the shared-memory chunk planes the tensor-core operands read, and a
+// warp reading 32 consecutive pixels of a chunk reads 512 contiguous bytes.
+// With nch = 1 this is NHWC.  Returns the index of pixel (b, y, x)'s chunk c
+// in units of 8 channels.
+__host__ __device__ inline size_t act_idx(int b, int y, int c, int x, int H, int W, int nch)
+{
+    return (((size_t)b * H + y) * nch + c) * W + x;
+}
 
 constexpr int kMaxSteps = 32;
 

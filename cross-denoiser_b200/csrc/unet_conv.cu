@@ -19,6 +19,13 @@
 // operand holds the matching weights (zero where a step's half is unused).
 // One thread issues all R x steps MMAs, commits them to an mbarrier, and the
 // four warps read their 32 TMEM lanes (one pixel each) for the epilogue.
+//
+// Staging.  Activations are row-chunk planes (unet.cuh), so every staged
+// (row, chunk) plane is one contiguous row segment in global memory: one
+// bulk copy (cp.async.bulk, 16 bytes per pixel), with the pixels and rows
+// outside the image copied from a page of zeros.  Every byte of the staged
+// planes is written by exactly one copy, so the mbarrier's transaction count
+// is the planes' total size.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
@@ -36,6 +43,29 @@ constexpr int kPlane = kStagePx * 16;       // bytes per chunk plane
 constexpr int kWaitIter = 1 << 22;          // bounded mbarrier polls
 
 __host__ __device__ inline int b_bytes(int nsteps, int nout) { return nsteps * 2 * nout * 16; }
+
+// Source of the zeros staged for pixels and rows outside the image (never
+// written; at least one plane long).
+constexpr int kZeroBytes = 4096;
+static_assert(kZeroBytes >= kPlane, "the zero page covers a staged plane");
+__device__ __align__(128) uint8_t g_zero_page[kZeroBytes] = {0};
+
+// Stage pixels [xa, xa + n) of one row-chunk plane into dst (16 bytes per
+// pixel) with bulk copies on `bar`: the pixels inside [0, W) from `row` (the
+// plane's pixel 0; null for a row outside the image), the rest from the zero
+// page.  Writes exactly n * 16 bytes.
+__device__ __forceinline__ void stage_plane(uint8_t *dst, const __nv_bfloat16 *row, int xa, int n, int W,
+                                            uint64_t *bar)
+{
+    int lo = xa, hi = xa;   // [lo, hi): the pixels copied from the image
+    if (row) {
+        lo = min(max(xa, 0), xa + n);
+        hi = max(min(xa + n, W), lo);
+    }
+    if (lo > xa) tc::bulk_load(dst, g_zero_page, (uint32_t)(lo - xa) * 16u, bar);
+    if (hi > lo) tc::bulk_load(dst + (size_t)(lo - xa) * 16, row + (size_t)lo * 8, (uint32_t)(hi - lo) * 16u, bar);
+    if (xa + n > hi) tc::bulk_load(dst + (size_t)(hi - xa) * 16, g_zero_page, (uint32_t)(xa + n - hi) * 16u, bar);
+}
 
 // Dynamic shared memory to request so that no more CTAs share an SM than
 // its 512 TMEM columns hold (228 KB of shared memory per SM): a CTA that
@@ -56,8 +86,7 @@ __host__ __device__ inline size_t conv_smem(int nsteps, int nout, int c0, int c1
 }
 
 template <int NOUT, int R>
-__global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P, const __grid_constant__ CUtensorMap m0,
-                                                      const __grid_constant__ CUtensorMap m1)
+__global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     constexpr int kCols = (R * NOUT <= 32) ? 32 : (R * NOUT <= 64) ? 64 : (R * NOUT <= 128) ? 128
@@ -74,20 +103,31 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P, const 
     uint64_t *bar = reinterpret_cast<uint64_t *>(sA1 + blk1);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
 
-    // one TMA box per input source ([row][chunk][131 px][8 ch], zeros outside
-    // the image) and one bulk copy of the packed weights, on one mbarrier
+    // per input source, planes [row][chunk][131 px][8 ch] (zeros outside the
+    // image), and the packed weights: bulk copies on one mbarrier
     if (warp == 0) tc::tmem_alloc(tslot, kCols);
     if (tid == 0) {
         tc::mbar_init(bar, 1);
         tc::fence_async_smem();
     }
     __syncthreads();   // barrier initialised before the copies are issued and waited on
-    if (tid == 0) {
-        const uint32_t bytes = (uint32_t)bb + (uint32_t)((R + 2) * (P.c0 + P.c1) * kPlane);
-        tc::mbar_expect_tx(bar, bytes);
-        tc::bulk_load(sB, P.wpack, (uint32_t)bb, bar);
-        tc::tma_load_5d(sA0, &m0, 0, x0 - 1, 0, y0 - 1, b, bar);
-        if (P.c1) tc::tma_load_5d(sA1, &m1, 0, x0 - 1, 0, y0 - 1, b, bar);
+    if (warp == 0) {
+        const int lane = tid & 31, nch = P.c0 + P.c1;
+        if (lane == 0) {
+            const uint32_t bytes = (uint32_t)bb + (uint32_t)((R + 2) * nch * kPlane);
+            tc::mbar_expect_tx(bar, bytes);
+            tc::bulk_load(sB, P.wpack, (uint32_t)bb, bar);
+        }
+        __syncwarp();   // the transaction count is raised before any copy lands
+        for (int i = lane; i < (R + 2) * nch; i += 32) {
+            const int r = i / nch, c = i - r * nch, gy = y0 - 1 + r;
+            const bool s1 = c >= P.c0;
+            const int cs = s1 ? c - P.c0 : c, ns = s1 ? P.c1 : P.c0;
+            uint8_t *dst = (s1 ? sA1 : sA0) + (size_t)(r * ns + cs) * kPlane;
+            const __nv_bfloat16 *row =
+                gy >= 0 && gy < P.H ? (s1 ? P.src1 : P.src0) + act_idx(b, gy, cs, 0, P.H, P.W, ns) * 8 : nullptr;
+            stage_plane(dst, row, x0 - 1, kStagePx, P.W, bar);
+        }
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -101,8 +141,6 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P, const 
         if (warp == 0) tc::tmem_dealloc(tbase, kCols);
         return;
     }
-    const size_t HW = (size_t)P.H * P.W;
-
     if (tid == 0) {
         const uint32_t idesc = tc::idesc_bf16(kPx, NOUT);
         const uint32_t a0 = tc::smem_u32(sA0), a1 = tc::smem_u32(sA1), b0 = tc::smem_u32(sB);
@@ -132,7 +170,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P, const 
             for (int j = 0; j < NOUT; j += 16) tc::tmem_ld16(lane_base + r * NOUT + j, v + j);
             const int y = y0 + r;
             const bool inside = x < P.W && y < P.H;
-            const size_t pix = b * HW + (size_t)(inside ? y : 0) * P.W + (inside ? x : 0);
+            const int yi = inside ? y : 0, xi = inside ? x : 0;
             if (P.bias) {
 #pragma unroll
                 for (int j = 0; j < NOUT; ++j) v[j] += __ldg(P.bias + j);
@@ -147,8 +185,9 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P, const 
 #pragma unroll
                 for (int c = 0; c < NOUT / 8; ++c) {
                     if (c >= P.d0 + P.d1) break;
-                    const __nv_bfloat16 *m = c < P.d0 ? (P.mask0 ? P.mask0 + pix * (8 * P.d0) + 8 * c : nullptr)
-                                                      : (P.mask1 ? P.mask1 + pix * (8 * P.d1) + 8 * (c - P.d0) : nullptr);
+                    const __nv_bfloat16 *m =
+                        c < P.d0 ? (P.mask0 ? P.mask0 + act_idx(b, yi, c, xi, P.H, P.W, P.d0) * 8 : nullptr)
+                                 : (P.mask1 ? P.mask1 + act_idx(b, yi, c - P.d0, xi, P.H, P.W, P.d1) * 8 : nullptr);
                     if (!m) continue;
                     const uint4 raw = *reinterpret_cast<const uint4 *>(m);
                     const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(&raw);
@@ -165,8 +204,8 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P, const 
                     __nv_bfloat162 *ob = reinterpret_cast<__nv_bfloat162 *>(&o);
 #pragma unroll
                     for (int e = 0; e < 4; ++e) ob[e] = __floats2bfloat162_rn(v[8 * c + 2 * e], v[8 * c + 2 * e + 1]);
-                    __nv_bfloat16 *d = c < P.d0 ? P.dst0 + pix * (8 * P.d0) + 8 * c
-                                                : P.dst1 + pix * (8 * P.d1) + 8 * (c - P.d0);
+                    __nv_bfloat16 *d = c < P.d0 ? P.dst0 + act_idx(b, yi, c, xi, P.H, P.W, P.d0) * 8
+                                                : P.dst1 + act_idx(b, yi, c - P.d0, xi, P.H, P.W, P.d1) * 8;
                     *reinterpret_cast<uint4 *>(d) = o;
                 }
             }
@@ -183,7 +222,6 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P, const 
                     }
                     const int py = y / 2, px = x / 2, PH = P.H / 2, PW = P.W / 2;
                     if (!(tid & 1) && py < PH && px < PW) {
-                        const size_t q = b * (size_t)PH * PW + (size_t)py * PW + px;
 #pragma unroll
                         for (int c = 0; c < NOUT / 8; ++c) {
                             if (c >= P.d0) break;
@@ -192,7 +230,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P, const 
 #pragma unroll
                             for (int e = 0; e < 4; ++e)
                                 ob[e] = __floats2bfloat162_rn(prev[8 * c + 2 * e], prev[8 * c + 2 * e + 1]);
-                            *reinterpret_cast<uint4 *>(P.pool + q * (8 * P.d0) + 8 * c) = o;
+                            *reinterpret_cast<uint4 *>(P.pool + act_idx(b, py, c, px, PH, PW, P.d0) * 8) = o;
                         }
                     }
                 } else {
@@ -212,19 +250,12 @@ cudaError_t launch_t(const ConvParams &P, int B, cudaStream_t st)
 {
     constexpr int kCols = (R * NOUT <= 32) ? 32 : (R * NOUT <= 64) ? 64 : (R * NOUT <= 128) ? 128
                                                 : (R * NOUT <= 256) ? 256 : 512;
-    CUtensorMap m0, m1;
-    if (!tc::make_rows_map(&m0, P.src0, P.c0, P.W, P.H, B, kStagePx, R + 2)) return cudaErrorInvalidValue;
-    if (P.c1) {
-        if (!tc::make_rows_map(&m1, P.src1, P.c1, P.W, P.H, B, kStagePx, R + 2)) return cudaErrorInvalidValue;
-    } else {
-        m1 = m0;
-    }
     const size_t smem = smem_for_tmem(conv_smem(P.nsteps, NOUT, P.c0, P.c1, R), kCols);
     cudaError_t e = cudaFuncSetAttribute(conv3x3_kernel<NOUT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid((P.W + kPx - 1) / kPx, (P.H + R - 1) / R, B);
-    conv3x3_kernel<NOUT, R><<<grid, 128, smem, st>>>(P, m0, m1);
+    conv3x3_kernel<NOUT, R><<<grid, 128, smem, st>>>(P);
     return cudaGetLastError();
 }
 
@@ -280,16 +311,14 @@ __global__ void __launch_bounds__(128) wgrad_kernel(const WgradParams P)
     uint8_t *sZ = sX + (size_t)((R + 2) * rs + 16) * kPlane;
     uint64_t *bar = reinterpret_cast<uint64_t *>(sZ + (size_t)(R * P.zc + 4) * kZPlane);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
-    const size_t HW = (size_t)P.H * P.W;
-
     for (int i = tid; i < (R + 2) * nch * kStagePx; i += 128) {
         const int px = i % kStagePx, t = i / kStagePx;
         const int c = t % nch, r = t / nch;
         const int gy = y0 - 1 + r, gx = x0 - 1 + px;
         const bool in = gy >= 0 && gy < P.H && gx >= 0 && gx < P.W;
-        const size_t pix = b * HW + (size_t)(in ? gy : 0) * P.W + (in ? gx : 0);
-        const __nv_bfloat16 *src = c < P.xc0 ? P.x0 + pix * (8 * P.xc0) + 8 * c
-                                             : P.x1 + pix * (8 * P.xc1) + 8 * (c - P.xc0);
+        const int yi = in ? gy : 0, xi = in ? gx : 0;
+        const __nv_bfloat16 *src = c < P.xc0 ? P.x0 + act_idx(b, yi, c, xi, P.H, P.W, P.xc0) * 8
+                                             : P.x1 + act_idx(b, yi, c - P.xc0, xi, P.H, P.W, P.xc1) * 8;
         tc::cp16(sX + (size_t)(r * rs + c) * kPlane + 16 * px, src, in ? 16u : 0u);
     }
     const uint4 ones = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);   // bf16 1.0 x 8
@@ -302,8 +331,8 @@ __global__ void __launch_bounds__(128) wgrad_kernel(const WgradParams P)
         const int c = t % P.zc, r = t / P.zc;
         const int gy = y0 + r, gx = x0 + px;
         const bool in = gy < P.H && gx < P.W;
-        const size_t pix = b * HW + (size_t)(in ? gy : 0) * P.W + (in ? gx : 0);
-        tc::cp16(sZ + (size_t)(r * P.zc + c) * kZPlane + 16 * px, P.dz + pix * (8 * P.zc) + 8 * c, in ? 16u : 0u);
+        const __nv_bfloat16 *src = P.dz + act_idx(b, in ? gy : 0, c, in ? gx : 0, P.H, P.W, P.zc) * 8;
+        tc::cp16(sZ + (size_t)(r * P.zc + c) * kZPlane + 16 * px, src, in ? 16u : 0u);
     }
     if (warp == 0) tc::tmem_alloc(tslot, kCols);
     if (tid == 0) tc::mbar_init(bar, 1);
@@ -356,163 +385,8 @@ __global__ void __launch_bounds__(128) wgrad_kernel(const WgradParams P)
     if (warp == 0) tc::tmem_dealloc(tbase, kCols);
 }
 
-// Persistent weight gradient with the three horizontal taps folded into M.
-// Each staged input row holds three copies shifted by kx = 0, 1, 2 pixels
-// (planes [kx][chunk], 128 pixels each) and a plane of ones, so for a
-// kernel row ky one MMA computes
-//   D_ky[(kx, cin) x cout] += X_ky^T[(kx, cin) x 16 px] dZ[16 px x cout]
-// and row 8 * 3 * nch of D_1 is the bias gradient.  M = 128 rows cover
-// 3 * nch + 1 chunk groups (nch <= 5); rows past them read other staged data
-// and are discarded.  CTAs are persistent (one per SM) and keep their three
-// accumulators in TMEM over all their tiles; tile i + 1 is copied in
-// (cp.async, second stage) while the tensor cores work on tile i.  One
-// partial sum per CTA.
-constexpr int kWgradPlanes = 108;   // 2 KB planes of dynamic shared memory
-
-__host__ __device__ inline int wgrad2_rows(int nch, int zc)
-{
-    const int rowp = 3 * nch + 1;
-    return (kWgradPlanes / 2 - 8 - 2 * rowp) / (rowp + zc);
-}
-
-constexpr int kWgradThreads = 256;
-
-template <int NZ>
-__global__ void __launch_bounds__(kWgradThreads, 1) wgrad2_kernel(const WgradParams P, int R, int ntx, int nty,
-                                                                  int ntiles)
-{
-    extern __shared__ __align__(128) uint8_t smem[];
-    constexpr int kCols = 3 * NZ <= 64 ? 64 : 128;
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const int nch = P.xc0 + P.xc1, zc = P.zc, rowp = 3 * nch + 1;
-    const int stage_planes = (R + 2) * rowp + R * zc;
-    uint8_t *stage[2] = {smem, smem + (size_t)stage_planes * kZPlane};
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + (size_t)(2 * stage_planes + 16) * kZPlane);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
-    const size_t HW = (size_t)P.H * P.W;
-
-    const uint4 ones = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);   // bf16 1.0 x 8
-    for (int s = 0; s < 2; ++s)
-        for (int i = tid; i < (R + 2) * kPx; i += kWgradThreads)
-            *reinterpret_cast<uint4 *>(stage[s] + (size_t)((i / kPx) * rowp + 3 * nch) * kZPlane + 16 * (i % kPx)) =
-                ones;
-
-    // thread -> pixel px of the tile row; the two halves take alternate (row, tap) pairs
-    const int px = tid & (kPx - 1), half = tid >> 7;
-    auto load_tile = [&](int tile, uint8_t *st) {
-        const int tx = tile % ntx, ty = (tile / ntx) % nty, b = tile / (ntx * nty);
-        const int x0 = tx * kPx, y0 = ty * R;
-        for (int q = half; q < (R + 2) * 3; q += kWgradThreads / kPx) {
-            const int rr = q / 3, kx = q - 3 * rr;
-            const int gy = y0 - 1 + rr, gx = x0 - 1 + kx + px;
-            const bool in = gy >= 0 && gy < P.H && gx >= 0 && gx < P.W;
-            const size_t pix = b * HW + (size_t)(in ? gy : 0) * P.W + (in ? gx : 0);
-            uint8_t *d = st + (size_t)(rr * rowp + kx * nch) * kZPlane + 16 * px;
-            const __nv_bfloat16 *s0 = P.x0 + pix * (8 * P.xc0);
-            for (int c = 0; c < P.xc0; ++c) tc::cp16(d + (size_t)c * kZPlane, s0 + 8 * c, in ? 16u : 0u);
-            if (P.xc1) {
-                const __nv_bfloat16 *s1 = P.x1 + pix * (8 * P.xc1);
-                for (int c = 0; c < P.xc1; ++c)
-                    tc::cp16(d + (size_t)(P.xc0 + c) * kZPlane, s1 + 8 * c, in ? 16u : 0u);
-            }
-        }
-        for (int r = half; r < R; r += kWgradThreads / kPx) {
-            const int gy = y0 + r, gx = x0 + px;
-            const bool in = gy < P.H && gx < P.W;
-            const size_t pix = b * HW + (size_t)(in ? gy : 0) * P.W + (in ? gx : 0);
-            uint8_t *d = st + (size_t)((R + 2) * rowp + r * zc) * kZPlane + 16 * px;
-            for (int c = 0; c < zc; ++c) tc::cp16(d + (size_t)c * kZPlane, P.dz + pix * (8 * zc) + 8 * c, in ? 16u : 0u);
-        }
-    };
-
-    if (warp == 0) tc::tmem_alloc(tslot, kCols);
-    if (tid == 0) {
-        tc::mbar_init(&bar[0], 1);
-        tc::mbar_init(&bar[1], 1);
-    }
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-    const uint32_t tbase = *tslot;
-    const uint32_t idesc = tc::idesc_bf16(kPx, NZ) | (1u << 15) | (1u << 16);   // A and B MN-major
-
-    const int first = blockIdx.x, stride = gridDim.x;
-    if (first < ntiles) load_tile(first, stage[0]);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    uint32_t phase[2] = {0u, 0u};
-    bool ok = true;
-    int it = 0;
-    for (int tile = first; tile < ntiles && ok; tile += stride, ++it) {
-        const int s = it & 1;
-        if (it >= 1) {
-            // the other stage is free once the MMAs of the previous tile are done
-            ok = tc::mbar_wait(&bar[s ^ 1], phase[s ^ 1], kWaitIter);
-            phase[s ^ 1] ^= 1u;
-        }
-        if (ok && tile + stride < ntiles) load_tile(tile + stride, stage[s ^ 1]);
-        asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 1;" ::: "memory");
-        tc::fence_async_smem();
-        tc::fence_before_sync();
-        ok = __syncthreads_and(ok) != 0;   // one decision for the whole CTA
-        tc::fence_after_sync();
-        if (tid == 0 && ok) {
-            const uint32_t sa = tc::smem_u32(stage[s]);
-            const uint32_t sz = sa + (uint32_t)((R + 2) * rowp) * kZPlane;
-            for (int r = 0; r < R; ++r)
-                for (int g = 0; g < kPx / 16; ++g) {
-                    const uint64_t bd = tc::sdesc(sz + (uint32_t)(r * zc) * kZPlane + 256u * g, 128, kZPlane);
-                    for (int ky = 0; ky < 3; ++ky) {
-                        const uint32_t a = sa + (uint32_t)((r + ky) * rowp) * kZPlane + 256u * g;
-                        tc::mma_bf16(tbase + ky * NZ, tc::sdesc(a, 128, kZPlane), bd, idesc,
-                                     (it | r | g) ? 1u : 0u);
-                    }
-                }
-            tc::commit(&bar[s]);
-        }
-    }
-    // the last tile's MMAs (if the loop ended early, its stage's commit may be missing: bounded wait)
-    if (it >= 1 && ok) ok = tc::mbar_wait(&bar[(it - 1) & 1], phase[(it - 1) & 1], kWaitIter);
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    ok = __syncthreads_and(ok) != 0;
-    tc::fence_after_sync();
-    float *out = P.partial + (size_t)blockIdx.x * (9 * P.cin * P.cout + P.cout);
-    if (!ok) {
-        if (tid == 0) atomicExch(P.err, 1);
-    } else if (it >= 1 && warp < 4) {
-        const int m = warp * 32 + (tid & 31);
-        const int kx = m / (8 * nch), c = m - kx * 8 * nch;
-        for (int ky = 0; ky < 3; ++ky)
-#pragma unroll
-            for (int j = 0; j < NZ; j += 16) {
-                float v[16];
-                tc::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + ky * NZ + j, v);
-                if (kx < 3 && c < P.cin) {
-#pragma unroll
-                    for (int q = 0; q < 16; ++q)
-                        if (j + q < P.cout) out[((ky * 3 + kx) * P.cin + c) * P.cout + j + q] = v[q];
-                } else if (kx == 3 && c == 0 && ky == 1) {
-#pragma unroll
-                    for (int q = 0; q < 16; ++q)
-                        if (j + q < P.cout) out[9 * P.cin * P.cout + j + q] = v[q];
-                }
-            }
-    }
-    tc::fence_before_sync();
-    __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tbase, kCols);
-}
-
-template <int NZ>
-cudaError_t launch_wgrad2_t(const WgradParams &P, int B, int R, int grid, cudaStream_t st)
-{
-    const int nch = P.xc0 + P.xc1, rowp = 3 * nch + 1;
-    const size_t smem = (size_t)(2 * ((R + 2) * rowp + R * P.zc) + 16) * kZPlane + 64;
-    cudaError_t e = cudaFuncSetAttribute(wgrad2_kernel<NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    const int ntx = (P.W + kPx - 1) / kPx, nty = (P.H + R - 1) / R;
-    wgrad2_kernel<NZ><<<grid, kWgradThreads, smem, st>>>(P, R, ntx, nty, B * ntx * nty);
-    return cudaGetLastError();
-}
+constexpr int kWgradThreads = 192;     // persistent weight gradient: producer, MMA, 4 bias warps
+constexpr int kWgradBiasWarps = 4;
 
 constexpr int kWgradRows = 4;
 
@@ -539,15 +413,18 @@ cudaError_t launch_wgrad_t(const WgradParams &P, int B, cudaStream_t st)
 // them read other staged data and are discarded.  Both operands MN-major
 // (channels contiguous, pixels 16 bytes apart).
 //
-// A tile is R input rows x 128 pixels: one TMA box of output gradient (R + 2
-// rows from y0 - 1) and, per input row, source and kx, one box of 128 pixels
-// from x0 - 1 + kx (the three copies come from L2), zeros outside the image,
-// land in a ring of S stages.  One thread issues the MMAs of a stage and
-// commits them to the stage's "empty" barrier, then refills the previous
-// stage; all threads sum the bias gradient (the output gradient over the
-// tile's R centre rows) from the staged planes meanwhile.  CTAs are
-// persistent and keep their accumulators in TMEM over all their tiles; one
-// partial sum per CTA.
+// A tile is R input rows x 128 pixels: the output gradient's R + 2 rows from
+// y0 - 1 and, per input row, source, kx and chunk, the 128 pixels from
+// x0 - 1 + kx (the three copies come from L2), one bulk copy per plane with
+// zeros outside the image (stage_plane), land in a ring of S stages.  The
+// warps specialise: warp 0 stages tile i into slot i % S once the slot's
+// "empty" barrier says its previous MMAs and bias reads are done (all 32
+// lanes issue copies); lane 0 of warp 1 issues the tile's MMAs when the slot
+// is full and commits them to "empty"; warps 2..5 sum the bias gradient (the
+// output gradient over the tile's R centre rows) from the staged planes and
+// arrive on "empty".  CTAs are persistent and keep their accumulators in
+// TMEM over all their tiles; one partial sum per CTA, read out of TMEM by
+// warps 2..5 at the end.  Every wait is bounded.
 constexpr int kWgrad3Smem = 225 * 1024;
 constexpr int kWgrad3Tail = 16 * kZPlane + 2048;   // discarded A rows read up to 16 planes past a row
 
@@ -583,8 +460,7 @@ __host__ __device__ inline int pow2_cols(int n)
 
 template <int ZC>
 __global__ void __launch_bounds__(kWgradThreads, 1)
-    wgrad3_kernel(const WgradParams P, const __grid_constant__ CUtensorMap mz, const __grid_constant__ CUtensorMap mx0,
-                  const __grid_constant__ CUtensorMap mx1, int R, int S, int stage_bytes, int ntx, int nty, int ntiles)
+    wgrad3_kernel(const WgradParams P, int R, int S, int stage_bytes, int ntx, int nty, int ntiles)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     constexpr int N = (24 * ZC + 15) & ~15;
@@ -597,29 +473,13 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)S * stage_bytes + 16 * kZPlane);
     uint64_t *empty = full + S;
     uint32_t *tslot = reinterpret_cast<uint32_t *>(empty + S);
-    float *red = reinterpret_cast<float *>(smem + (size_t)S * stage_bytes + 16 * kZPlane + 1024);   // [8][8 * ZC]
+    float *red = reinterpret_cast<float *>(smem + (size_t)S * stage_bytes + 16 * kZPlane + 1024);   // [4][8 * ZC]
 
-    auto issue = [&](int tile, int s) {
-        const int tx = tile % ntx, ty = (tile / ntx) % nty, b = tile / (ntx * nty);
-        const int x0 = tx * kPx, y0 = ty * R;
-        uint8_t *st = smem + (size_t)s * stage_bytes;
-        tc::mbar_expect_tx(&full[s], zbytes + xbytes);
-        tc::tma_load_5d(st, &mz, 0, x0, 0, y0 - 1, b, &full[s]);
-        for (int r = 0; r < R; ++r)
-            for (int kx = 0; kx < 3; ++kx) {
-                uint8_t *row = st + xoff + (size_t)(r * 3 * xc) * kZPlane;
-                tc::tma_load_5d(row + (size_t)(kx * xc0) * kZPlane, &mx0, 0, x0 - 1 + kx, 0, y0 + r, b, &full[s]);
-                if (xc1)
-                    tc::tma_load_5d(row + (size_t)(3 * xc0 + kx * xc1) * kZPlane, &mx1, 0, x0 - 1 + kx, 0, y0 + r, b,
-                                    &full[s]);
-            }
-    };
-
-    if (warp == 0) tc::tmem_alloc(tslot, cols);
+    if (warp == 1) tc::tmem_alloc(tslot, cols);
     if (tid == 0) {
         for (int s = 0; s < S; ++s) {
             tc::mbar_init(&full[s], 1);
-            tc::mbar_init(&empty[s], 1);
+            tc::mbar_init(&empty[s], 1 + kWgradBiasWarps);   // the MMA commit + the bias warps
         }
         tc::fence_async_smem();
     }
@@ -627,122 +487,168 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tbase = *tslot;
-    const uint32_t idesc = tc::idesc_bf16(kPx, N) | (1u << 15) | (1u << 16);   // A and B MN-major
-
     const int first = blockIdx.x, stride = gridDim.x;
-    int issued = 0;   // thread 0: loads issued, by iteration index
-    if (tid == 0)
-        for (; issued < S && first + issued * stride < ntiles; ++issued) issue(first + issued * stride, issued);
+    bool ok = true;
+    int ntile = 0;   // tiles this CTA walks
+    for (int t = first; t < ntiles; t += stride) ++ntile;
 
     float bsum[8 * ZC];
 #pragma unroll
     for (int j = 0; j < 8 * ZC; ++j) bsum[j] = 0.f;
-    const int px = tid & (kPx - 1), half = tid >> 7;
-    bool ok = true;
-    int it = 0;
-    for (int tile = first; tile < ntiles; tile += stride, ++it) {
-        const int s = it % S;
-        const bool got = tc::mbar_wait(&full[s], (uint32_t)(it / S) & 1u, kWaitIter);
-        ok = __syncthreads_and(ok && got) != 0;   // one decision for the whole CTA
-        if (!ok) break;
-        tc::fence_after_sync();
-        const uint8_t *st = smem + (size_t)s * stage_bytes;
-        if (tid == 0) {
-            const uint32_t sb = tc::smem_u32(st);
-            for (int r = 0; r < R; ++r)
-                for (int g = 0; g < kPx / 16; ++g) {
-                    const uint64_t bd = tc::sdesc(sb + (uint32_t)(r * ZC) * kZPlane + 256u * g, 128, kZPlane);
-                    const uint32_t a0 = sb + xoff + (uint32_t)(r * 3 * xc) * kZPlane + 256u * g;
-                    const uint32_t acc = (it | r | g) ? 1u : 0u;
-                    tc::mma_bf16(tbase, tc::sdesc(a0, 128, kZPlane), bd, idesc, acc);
-                    if (split)
-                        tc::mma_bf16(tbase + N, tc::sdesc(a0 + (uint32_t)(3 * xc0) * kZPlane, 128, kZPlane), bd, idesc,
-                                     acc);
-                }
-            tc::commit(&empty[s]);
-        }
-        // bias gradient: the tile's centre gradient rows (staged rows 1..R)
-        for (int r = 1 + half; r <= R; r += 2)
-#pragma unroll
-            for (int c = 0; c < ZC; ++c) {
-                const uint4 raw = *reinterpret_cast<const uint4 *>(st + (size_t)(r * ZC + c) * kZPlane + 16 * px);
-                const __nv_bfloat162 *h2 = reinterpret_cast<const __nv_bfloat162 *>(&raw);
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const float2 f = __bfloat1622float2(h2[e]);
-                    bsum[8 * c + 2 * e] += f.x;
-                    bsum[8 * c + 2 * e + 1] += f.y;
-                }
-            }
-        // refill the previous iteration's stage once its MMAs are done
-        if (tid == 0 && it >= 1) {
-            const int pit = it - 1, ps = pit % S, nt = first + (pit + S) * stride;
-            if (nt < ntiles) {
-                if (tc::mbar_wait(&empty[ps], (uint32_t)(pit / S) & 1u, kWaitIter)) {
-                    issue(nt, ps);
-                    ++issued;
-                } else {
+
+    if (warp == 0) {
+        // ---- producer: all lanes issue the planes of a stage ----
+        const int nz = (R + 2) * ZC, nplanes = nz + R * 3 * xc;
+        int i = 0;
+        for (; i < ntile; ++i) {
+            const int s = i % S, tile = first + i * stride;
+            if (i >= S) {
+                bool got = true;
+                if (lane == 0) got = tc::mbar_wait(&empty[s], (uint32_t)(i / S - 1) & 1u, kWaitIter);
+                if (!__shfl_sync(0xffffffffu, got ? 1 : 0, 0)) {
                     ok = false;
+                    break;
+                }
+            }
+            const int tx = tile % ntx, ty = (tile / ntx) % nty, b = tile / (ntx * nty);
+            const int x0 = tx * kPx, y0 = ty * R;
+            uint8_t *st = smem + (size_t)s * stage_bytes;
+            if (lane == 0) tc::mbar_expect_tx(&full[s], zbytes + xbytes);
+            __syncwarp();   // the transaction count is raised before any copy lands
+            for (int q = lane; q < nplanes; q += 32) {
+                if (q < nz) {
+                    // output gradient: rows y0 - 1 .. y0 + R, pixels x0 ..
+                    const int r = q / ZC, c = q - r * ZC, gy = y0 - 1 + r;
+                    const __nv_bfloat16 *row =
+                        gy >= 0 && gy < P.H ? P.dz + act_idx(b, gy, c, 0, P.H, P.W, ZC) * 8 : nullptr;
+                    stage_plane(st + (size_t)q * kZPlane, row, x0, kPx, P.W, &full[s]);
+                } else {
+                    // input row r, planes [kx][chunk] of source 0 then of source 1
+                    const int u = q - nz, r = u / (3 * xc), v = u - r * 3 * xc, gy = y0 + r;
+                    const bool s1 = v >= 3 * xc0;
+                    const int xs = s1 ? xc1 : xc0, w = s1 ? v - 3 * xc0 : v, kx = w / xs, c = w - kx * xs;
+                    const __nv_bfloat16 *row =
+                        gy < P.H ? (s1 ? P.x1 : P.x0) + act_idx(b, gy, c, 0, P.H, P.W, xs) * 8 : nullptr;
+                    stage_plane(st + xoff + (size_t)u * kZPlane, row, x0 - 1 + kx, kPx, P.W, &full[s]);
                 }
             }
         }
+        // every copy issued has landed before the CTA may exit
+        if (lane == 0)
+            for (int s = 0; s < S && s < i; ++s)
+                tc::mbar_wait(&full[s], (uint32_t)((i - s + S - 1) / S - 1) & 1u, kWaitIter);
+    } else if (warp == 1) {
+        // ---- MMA issue (one thread) ----
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_bf16(kPx, N) | (1u << 15) | (1u << 16);   // A and B MN-major
+            int i = 0;
+            for (; i < ntile; ++i) {
+                const int s = i % S;
+                if (!tc::mbar_wait(&full[s], (uint32_t)(i / S) & 1u, kWaitIter)) {
+                    ok = false;
+                    break;
+                }
+                tc::fence_after_sync();
+                const uint32_t sb = tc::smem_u32(smem + (size_t)s * stage_bytes);
+                // descriptors of row 0, pixel group 0; rows and groups at
+                // constant strides (start field in 16-byte units)
+                const uint64_t bd0 = tc::sdesc(sb, 128, kZPlane), ad0 = tc::sdesc(sb + xoff, 128, kZPlane);
+                const uint64_t ad1 = ad0 + ((uint64_t)(3 * xc0 * kZPlane) >> 4);
+                for (int r = 0; r < R; ++r) {
+                    const uint64_t br = bd0 + ((uint64_t)(r * ZC * kZPlane) >> 4);
+                    const uint64_t ar = (uint64_t)(r * 3 * xc * kZPlane) >> 4;
+#pragma unroll
+                    for (int g = 0; g < kPx / 16; ++g) {
+                        const uint32_t acc = (i | r | g) ? 1u : 0u;
+                        const uint64_t gg = (uint64_t)(256 * g) >> 4;
+                        tc::mma_bf16(tbase, ad0 + ar + gg, br + gg, idesc, acc);
+                        if (split) tc::mma_bf16(tbase + N, ad1 + ar + gg, br + gg, idesc, acc);
+                    }
+                }
+                tc::commit(&empty[s]);
+            }
+            // the last MMAs are done before the accumulators are read
+            if (ok && i >= 1) ok = tc::mbar_wait(&empty[(i - 1) % S], (uint32_t)((i - 1) / S) & 1u, kWaitIter);
+        }
+        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+    } else {
+        // ---- bias warps: the tile's centre gradient rows (staged rows 1..R) ----
+        const int px = tid - 64;
+        for (int i = 0; i < ntile; ++i) {
+            const int s = i % S;
+            bool got = true;
+            if (lane == 0) got = tc::mbar_wait(&full[s], (uint32_t)(i / S) & 1u, kWaitIter);
+            if (!__shfl_sync(0xffffffffu, got ? 1 : 0, 0)) {
+                ok = false;
+                break;
+            }
+            const uint8_t *st = smem + (size_t)s * stage_bytes;
+            for (int r = 1; r <= R; ++r)
+#pragma unroll
+                for (int c = 0; c < ZC; ++c) {
+                    const uint4 raw = *reinterpret_cast<const uint4 *>(st + (size_t)(r * ZC + c) * kZPlane + 16 * px);
+                    const __nv_bfloat162 *h2 = reinterpret_cast<const __nv_bfloat162 *>(&raw);
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const float2 f = __bfloat1622float2(h2[e]);
+                        bsum[8 * c + 2 * e] += f.x;
+                        bsum[8 * c + 2 * e + 1] += f.y;
+                    }
+                }
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(&empty[s]))
+                                        : "memory");
+        }
     }
-    // the last MMAs, and (after an early exit) the loads still in flight
-    bool fin = true;
-    if (tid == 0) {
-        if (it >= 1) fin = tc::mbar_wait(&empty[(it - 1) % S], (uint32_t)((it - 1) / S) & 1u, kWaitIter);
-        for (int j = it; j < issued; ++j) tc::mbar_wait(&full[j % S], (uint32_t)(j / S) & 1u, kWaitIter);
-    }
-    ok = __syncthreads_and(ok && fin) != 0;
+    ok = __syncthreads_and(ok) != 0;
     tc::fence_after_sync();
     float *out = P.partial + (size_t)blockIdx.x * (9 * P.cin * P.cout + P.cout);
     if (!ok) {
         if (tid == 0) atomicExch(P.err, 1);
-    } else if (it >= 1) {
-        // bias: lanes, then warps in a fixed order
+    } else if (ntile >= 1 && warp >= 2) {
+        const int bw = warp - 2;
+        // bias: lanes, then the four warps in a fixed order
 #pragma unroll
         for (int j = 0; j < 8 * ZC; ++j) {
             float v = bsum[j];
 #pragma unroll
             for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) red[warp * 8 * ZC + j] = v;
+            if (lane == 0) red[bw * 8 * ZC + j] = v;
         }
-        __syncthreads();
-        if (tid < P.cout) {
+        asm volatile("bar.sync 1, %0;" ::"n"(kWgradBiasWarps * 32) : "memory");   // the bias warps only
+        if (bw == 0 && lane < P.cout) {
             float v = 0.f;
-            for (int w = 0; w < kWgradThreads / 32; ++w) v += red[w * 8 * ZC + tid];
-            out[9 * P.cin * P.cout + tid] = v;
+            for (int w = 0; w < kWgradBiasWarps; ++w) v += red[w * 8 * ZC + lane];
+            out[9 * P.cin * P.cout + lane] = v;
         }
-        if (warp < 4) {
-            // TMEM lane m = row (group m / 8: source, kx, chunk; channel m % 8)
-            const int m = warp * 32 + lane, grp = m >> 3, e = m & 7;
-            for (int a = 0; a < (split ? 2 : 1); ++a) {
-                int kx = 3, ci = P.cin;   // invalid unless decoded below
-                if (split) {
-                    const int xs = a ? xc1 : xc0;
-                    if (grp < 3 * xs) {
-                        kx = grp / xs;
-                        ci = (a ? 8 * xc0 : 0) + 8 * (grp - kx * xs) + e;
-                    }
-                } else if (grp < 3 * xc0) {
-                    kx = grp / xc0;
-                    ci = 8 * (grp - kx * xc0) + e;
-                } else if (grp < 3 * xc) {
-                    const int g1 = grp - 3 * xc0;
-                    kx = g1 / xc1;
-                    ci = 8 * xc0 + 8 * (g1 - kx * xc1) + e;
+        // TMEM lane m = row (group m / 8: source, kx, chunk; channel m % 8)
+        const int q = warp & 3, m = q * 32 + lane, grp = m >> 3, e = m & 7;
+        for (int a = 0; a < (split ? 2 : 1); ++a) {
+            int kx = 3, ci = P.cin;   // invalid unless decoded below
+            if (split) {
+                const int xs = a ? xc1 : xc0;
+                if (grp < 3 * xs) {
+                    kx = grp / xs;
+                    ci = (a ? 8 * xc0 : 0) + 8 * (grp - kx * xs) + e;
                 }
-                const bool valid = kx < 3 && ci < P.cin;
+            } else if (grp < 3 * xc0) {
+                kx = grp / xc0;
+                ci = 8 * (grp - kx * xc0) + e;
+            } else if (grp < 3 * xc) {
+                const int g1 = grp - 3 * xc0;
+                kx = g1 / xc1;
+                ci = 8 * xc0 + 8 * (g1 - kx * xc1) + e;
+            }
+            const bool valid = kx < 3 && ci < P.cin;
 #pragma unroll
-                for (int j = 0; j < N; j += 16) {
-                    float v[16];
-                    tc::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + a * N + j, v);
-                    if (valid) {
+            for (int j = 0; j < N; j += 16) {
+                float v[16];
+                tc::tmem_ld16(tbase + ((uint32_t)(q * 32) << 16) + a * N + j, v);
+                if (valid) {
 #pragma unroll
-                        for (int q = 0; q < 16; ++q) {
-                            const int n = j + q, kyp = n / (8 * ZC), co = n - kyp * 8 * ZC;
-                            if (kyp < 3 && co < P.cout) out[(((2 - kyp) * 3 + kx) * P.cin + ci) * P.cout + co] = v[q];
-                        }
+                    for (int qq = 0; qq < 16; ++qq) {
+                        const int n = j + qq, kyp = n / (8 * ZC), co = n - kyp * 8 * ZC;
+                        if (kyp < 3 && co < P.cout) out[(((2 - kyp) * 3 + kx) * P.cin + ci) * P.cout + co] = v[qq];
                     }
                 }
             }
@@ -750,7 +656,7 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tbase, cols);
+    if (warp == 1) tc::tmem_dealloc(tbase, cols);
 }
 
 template <int ZC>
@@ -758,19 +664,10 @@ cudaError_t launch_wgrad3_t(const WgradParams &P, int B, int grid, cudaStream_t 
 {
     const Wgrad3Plan p = wgrad3_plan(P.xc0, P.xc1, ZC);
     if (p.S < 2) return cudaErrorInvalidValue;
-    CUtensorMap mz, mx0, mx1;
-    if (!tc::make_rows_map(&mz, P.dz, ZC, P.W, P.H, B, kPx, p.R + 2)) return cudaErrorInvalidValue;
-    if (!tc::make_rows_map(&mx0, P.x0, P.xc0, P.W, P.H, B, kPx, 1)) return cudaErrorInvalidValue;
-    if (P.xc1) {
-        if (!tc::make_rows_map(&mx1, P.x1, P.xc1, P.W, P.H, B, kPx, 1)) return cudaErrorInvalidValue;
-    } else {
-        mx1 = mx0;
-    }
     cudaError_t e = cudaFuncSetAttribute(wgrad3_kernel<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
     if (e != cudaSuccess) return e;
     const int ntx = (P.W + kPx - 1) / kPx, nty = (P.H + p.R - 1) / p.R;
-    wgrad3_kernel<ZC><<<grid, kWgradThreads, p.smem, st>>>(P, mz, mx0, mx1, p.R, p.S, (int)p.stage, ntx, nty,
-                                                            B * ntx * nty);
+    wgrad3_kernel<ZC><<<grid, kWgradThreads, p.smem, st>>>(P, p.R, p.S, (int)p.stage, ntx, nty, B * ntx * nty);
     return cudaGetLastError();
 }
 
@@ -836,9 +733,6 @@ cudaError_t launch_pack(const float *w, __nv_bfloat16 *dst, const PackTable &T, 
 
 size_t wgrad_tiles(int B, int H, int W) { return (size_t)B * ((W + kPx - 1) / kPx) * ((H + kWgradRows - 1) / kWgradRows); }
 
-// Partial-sum rows the weight gradient of this layer writes: one per CTA of
-// the persistent kernel (nch <= 5), one per tile otherwise.
-static bool wgrad_persistent(const WgradParams &P) { return P.xc0 + P.xc1 <= 5 && wgrad2_rows(P.xc0 + P.xc1, P.zc) >= 1; }
 
 static int sm_count()
 {
@@ -847,7 +741,7 @@ static int sm_count()
     return n;
 }
 
-// The TMA-staged persistent kernel takes every layer whose (ky, cout) fit N
+// The persistent kernel takes every layer whose (ky, cout) fit N
 // (zc <= 4) and whose (kx, cin) groups fit M per source.
 static bool wgrad3_fits(const WgradParams &P)
 {
@@ -857,15 +751,12 @@ static bool wgrad3_fits(const WgradParams &P)
     return P.zc >= 1 && P.zc <= 4 && fits_m && wgrad3_plan(P.xc0, P.xc1, P.zc).S >= 2;
 }
 
+// Partial-sum rows the weight gradient of this layer writes: one per CTA of
+// the persistent kernel, one per tile otherwise.
 int wgrad_partial_rows(const WgradParams &P, int B)
 {
-    if (wgrad3_fits(P)) {
-        const int R = wgrad3_plan(P.xc0, P.xc1, P.zc).R;
-        const int tiles = B * ((P.W + kPx - 1) / kPx) * ((P.H + R - 1) / R);
-        return tiles < sm_count() ? tiles : sm_count();
-    }
-    if (!wgrad_persistent(P)) return (int)wgrad_tiles(B, P.H, P.W);
-    const int R = wgrad2_rows(P.xc0 + P.xc1, P.zc);
+    if (!wgrad3_fits(P)) return (int)wgrad_tiles(B, P.H, P.W);
+    const int R = wgrad3_plan(P.xc0, P.xc1, P.zc).R;
     const int tiles = B * ((P.W + kPx - 1) / kPx) * ((P.H + R - 1) / R);
     return tiles < sm_count() ? tiles : sm_count();
 }
@@ -888,56 +779,9 @@ cudaError_t launch_wgrad(const WgradParams &P, int B, cudaStream_t st)
         default: return launch_wgrad3_t<4>(P, B, grid, st);
         }
     }
-    if (wgrad_persistent(P)) {
-        const int R = wgrad2_rows(P.xc0 + P.xc1, P.zc), grid = wgrad_partial_rows(P, B);
-        return P.cout <= 16 ? launch_wgrad2_t<16>(P, B, R, grid, st) : launch_wgrad2_t<32>(P, B, R, grid, st);
-    }
     return P.cout <= 16 ? launch_wgrad_t<16>(P, B, st) : launch_wgrad_t<32>(P, B, st);
 }
 
 }  // namespace unet
 }  // namespace cd
 
-namespace cd {
-namespace tc {
-
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-static EncodeTiledFn encode_fn()
-{
-    static EncodeTiledFn fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-    }
-    return fn;
-}
-
-// NHWC bf16 tensor with `chunks` x 8 channels viewed as 5-D {8 channels, W
-// pixels, chunks, H rows, B} (the chunk dimension's stride, 16 bytes, is
-// inside a pixel), boxes of {8, box_px, chunks, box_rows, 1}: a box lands in
-// shared memory as [row][chunk][pixel][8 channels], one 16-byte-per-pixel
-// chunk plane per (row, chunk).
-bool make_rows_map(CUtensorMap *map, const void *base, int chunks, int W, int H, int B, int box_px, int box_rows)
-{
-    EncodeTiledFn fn = encode_fn();
-    if (!fn || chunks < 1 || box_px > 256 || box_rows > 256 || chunks > 256) return false;
-    const cuuint64_t C = (cuuint64_t)chunks * 8;
-    const cuuint64_t dims[5] = {8, (cuuint64_t)W, (cuuint64_t)chunks, (cuuint64_t)H, (cuuint64_t)B};
-    const cuuint64_t strides[4] = {C * 2, 16, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
-    const cuuint32_t box[5] = {8, (cuuint32_t)box_px, (cuuint32_t)chunks, (cuuint32_t)box_rows, 1};
-    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
-    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void *>(base), dims, strides, box, estr,
-              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
-
-}  // namespace tc
-}  // namespace cd

@@ -17,6 +17,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
+#include "unet.cuh"
 #include "unet_ops.cuh"
 
 namespace cd {
@@ -43,14 +44,16 @@ CD_DEV void st8(__nv_bfloat16 *p, const float *v)
     *reinterpret_cast<uint4 *>(p) = o;
 }
 
-// [ols1, ols2, prev_out, albedo, normal] (fp32, 3 channels each) -> bf16, 16 channels (15 + zero)
+// [ols1, ols2, prev_out, albedo, normal] (fp32, 3 channels each) -> bf16, 16
+// channels (15 + zero) in two row-chunk planes; n = B * H * W pixels, W wide
 __global__ void __launch_bounds__(256) pack_input_kernel(const float *__restrict__ a, const float *__restrict__ b,
                                                          const float *__restrict__ c, const float *__restrict__ d,
                                                          const float *__restrict__ e, __nv_bfloat16 *__restrict__ x,
-                                                         size_t n)
+                                                         size_t n, int W)
 {
     const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
+    const int row = (int)(p / W), px = (int)(p - (size_t)row * W);
     float v[16];
     const float *src[5] = {a, b, c, d, e};
 #pragma unroll
@@ -60,8 +63,8 @@ __global__ void __launch_bounds__(256) pack_input_kernel(const float *__restrict
         v[3 * k + 2] = __ldg(src[k] + 3 * p + 2);
     }
     v[15] = 0.f;
-    st8(x + 16 * p, v);
-    st8(x + 16 * p + 8, v + 8);
+    st8(x + act_idx(0, row, 0, px, 0, W, 2) * 8, v);
+    st8(x + act_idx(0, row, 1, px, 0, W, 2) * 8, v + 8);
 }
 
 // Conv2DTranspose(kernel 1, stride 2) forward, one thread per output pixel.
@@ -81,17 +84,16 @@ __global__ void __launch_bounds__(256) tconv_fwd_kernel(const __nv_bfloat16 *__r
 #pragma unroll
     for (int c = 0; c < CO; ++c) o[c] = sK[CO * CI + c];
     if (!(xo & 1) && !(yo & 1)) {
-        const size_t p = ((size_t)b * Hi + yo / 2) * Wi + xo / 2;
         float x[CI];
 #pragma unroll
-        for (int c = 0; c < CI; c += 8) ld8(in + p * CI + c, x + c);
+        for (int c = 0; c < CI; c += 8) ld8(in + act_idx(b, yo / 2, c / 8, xo / 2, Hi, Wi, CI / 8) * 8, x + c);
 #pragma unroll
         for (int co = 0; co < CO; ++co)
 #pragma unroll
             for (int ci = 0; ci < CI; ++ci) o[co] = fmaf(sK[co * CI + ci], x[ci], o[co]);
     }
 #pragma unroll
-    for (int c = 0; c < CO; c += 8) st8(out + q * CO + c, o + c);
+    for (int c = 0; c < CO; c += 8) st8(out + act_idx(b, yo, c / 8, xo, Ho, Wo, CO / 8) * 8, o + c);
 }
 
 // Conv2DTranspose backward: a block of kN input pixels computes
@@ -119,16 +121,16 @@ __global__ void __launch_bounds__(kN) tconv_bwd_kernel(const __nv_bfloat16 *__re
     float bsum[CO];
 #pragma unroll
     for (int c = 0; c < CO; ++c) bsum[c] = 0.f;
+    const int xi = (int)(p % Wi), yi = (int)((p / Wi) % Hi), b = (int)(p / ((size_t)Wi * Hi));
     if (p < n) {
-        const int xi = (int)(p % Wi), yi = (int)((p / Wi) % Hi), b = (int)(p / ((size_t)Wi * Hi));
 #pragma unroll
-        for (int c = 0; c < CI; c += 8) ld8(in + p * CI + c, x + c);
-        const int Wo = 2 * Wi;
+        for (int c = 0; c < CI; c += 8) ld8(in + act_idx(b, yi, c / 8, xi, Hi, Wi, CI / 8) * 8, x + c);
+        const int Wo = 2 * Wi, Ho = 2 * Hi;
         for (int a = 0; a < 4; ++a) {
-            const size_t q = ((size_t)b * 2 * Hi + 2 * yi + (a >> 1)) * Wo + 2 * xi + (a & 1);
+            const int yo = 2 * yi + (a >> 1), xo = 2 * xi + (a & 1);
             float g[CO];
 #pragma unroll
-            for (int c = 0; c < CO; c += 8) ld8(dout + q * CO + c, g + c);
+            for (int c = 0; c < CO; c += 8) ld8(dout + act_idx(b, yo, c / 8, xo, Ho, Wo, CO / 8) * 8, g + c);
 #pragma unroll
             for (int c = 0; c < CO; ++c) {
                 bsum[c] += g[c];
@@ -154,7 +156,7 @@ __global__ void __launch_bounds__(kN) tconv_bwd_kernel(const __nv_bfloat16 *__re
             g[ci] = x[ci] > 0.f ? s : 0.f;
         }
 #pragma unroll
-        for (int c = 0; c < CI; c += 8) st8(dz_in + p * CI + c, g + c);
+        for (int c = 0; c < CI; c += 8) st8(dz_in + act_idx(b, yi, c / 8, xi, Hi, Wi, CI / 8) * 8, g + c);
     }
     float *out = partial + (size_t)blockIdx.x * (CO * CI + CO);
     for (int j = t; j < CO * CI + CO; j += kN) {
@@ -264,20 +266,20 @@ __global__ void __launch_bounds__(256) pool_bwd_kernel(const __nv_bfloat16 *__re
     if (q >= (size_t)B * H * W) return;
     const int x = (int)(q % W), y = (int)((q / W) % H), b = (int)(q / ((size_t)W * H));
     const int PH = H / 2, PW = W / 2;
+    constexpr int NC = C / 8;
     float a[C], g[C];
 #pragma unroll
     for (int c = 0; c < C; c += 8) {
-        ld8(act + q * C + c, a + c);
-        ld8(dskip + q * C + c, g + c);
+        ld8(act + act_idx(b, y, c / 8, x, H, W, NC) * 8, a + c);
+        ld8(dskip + act_idx(b, y, c / 8, x, H, W, NC) * 8, g + c);
     }
     const int py = y / 2, px = x / 2;
     if (py < PH && px < PW) {
-        const size_t pq = ((size_t)b * PH + py) * PW + px;
         float m[C], dp[C];
 #pragma unroll
         for (int c = 0; c < C; c += 8) {
-            ld8(pooled + pq * C + c, m + c);
-            ld8(dpool + pq * C + c, dp + c);
+            ld8(pooled + act_idx(b, py, c / 8, px, PH, PW, NC) * 8, m + c);
+            ld8(dpool + act_idx(b, py, c / 8, px, PH, PW, NC) * 8, dp + c);
         }
         // position of this pixel in its window and of the first maximum before it
         const int me = (y & 1) * 2 + (x & 1);
@@ -286,8 +288,8 @@ __global__ void __launch_bounds__(256) pool_bwd_kernel(const __nv_bfloat16 *__re
             if (a[c] != m[c]) continue;
             bool first = true;
             for (int k = 0; k < me; ++k) {
-                const size_t r = ((size_t)b * H + 2 * py + (k >> 1)) * W + 2 * px + (k & 1);
-                if (__bfloat162float(act[r * C + c]) == m[c]) first = false;
+                const size_t r = act_idx(b, 2 * py + (k >> 1), c / 8, 2 * px + (k & 1), H, W, NC);
+                if (__bfloat162float(act[r * 8 + (c & 7)]) == m[c]) first = false;
             }
             if (first) g[c] += dp[c];
         }
@@ -296,7 +298,7 @@ __global__ void __launch_bounds__(256) pool_bwd_kernel(const __nv_bfloat16 *__re
     for (int c = 0; c < C; ++c)
         if (!(a[c] > 0.f)) g[c] = 0.f;
 #pragma unroll
-    for (int c = 0; c < C; c += 8) st8(dz + q * C + c, g + c);
+    for (int c = 0; c < C; c += 8) st8(dz + act_idx(b, y, c / 8, x, H, W, NC) * 8, g + c);
 }
 
 // Two-stage fixed-order reduction of per-tile partial sums: stage 1 sums
@@ -350,9 +352,9 @@ __global__ void step_kernel(int *step) { *step += 1; }
 }  // namespace
 
 cudaError_t launch_pack_input(const float *a, const float *b, const float *c, const float *d, const float *e,
-                              __nv_bfloat16 *x, size_t n, cudaStream_t st)
+                              __nv_bfloat16 *x, size_t n, int W, cudaStream_t st)
 {
-    pack_input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, b, c, d, e, x, n);
+    pack_input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, b, c, d, e, x, n, W);
     return cudaGetLastError();
 }
 

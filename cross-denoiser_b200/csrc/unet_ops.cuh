@@ -1,4 +1,5 @@
-// Launchers of the U-Net's non-convolution kernels (unet_ops.cu).
+// Launchers of the U-Net's non-convolution kernels (unet_ops.cu).  Activation
+// tensors are bf16 row-chunk planes (unet.cuh).
 #pragma once
 #include <cstddef>
 #include <cuda_bf16.h>
@@ -8,7 +9,7 @@ namespace cd {
 namespace unet {
 
 cudaError_t launch_pack_input(const float *a, const float *b, const float *c, const float *d, const float *e,
-                              __nv_bfloat16 *x, size_t n, cudaStream_t st);
+                              __nv_bfloat16 *x, size_t n, int W, cudaStream_t st);
 cudaError_t launch_tconv_fwd(int ci, int co, const __nv_bfloat16 *in, const float *K, const float *bias,
                              __nv_bfloat16 *out, int Hi, int Wi, int B, cudaStream_t st);
 size_t tconv_blocks(int ci, int Hi, int Wi, int B);

@@ -144,27 +144,43 @@ class UNet:
         self.apply_gradients()
 
 
+def to_planes(x):
+    """[B,H,W,C] (C a multiple of 8) -> the kernels' row-chunk planes [B,H,C/8,W,8]."""
+    B, H, W, C = x.shape
+    return x.reshape(B, H, W, C // 8, 8).permute(0, 1, 3, 2, 4).contiguous()
+
+
+def from_planes(p):
+    """Row-chunk planes [B,H,C/8,W,8] -> [B,H,W,C]."""
+    B, H, n, W, _ = p.shape
+    return p.permute(0, 1, 3, 2, 4).reshape(B, H, W, 8 * n)
+
+
 def conv3x3(weight, bias, x, cin: int, cout: int, dgrad: bool = False):
     """One 3x3 conv layer on the tensor-core kernel (cd_unet_conv3x3).
-    x: [B,H,W,C] bf16 with C = cin (or cout for dgrad) rounded up to 8."""
+    x: [B,H,W,C] bf16 with C = cin (or cout for dgrad) rounded up to 8; the
+    kernel reads and writes row-chunk planes, converted here."""
     B, H, W, _ = x.shape
     out_ch = cin if dgrad else cout
-    y = torch.empty((B, H, W, (out_ch + 7) // 8 * 8), dtype=torch.bfloat16, device=x.device)
+    xp = to_planes(x)   # held until the launch is queued
+    yp = torch.empty((B, H, (out_ch + 7) // 8, W, 8), dtype=torch.bfloat16, device=x.device)
     L = _lib.lib()
     nb = int(L.cd_unet_conv3x3_workspace_size(cin, cout))
     ws = torch.zeros((max(nb, 1),), dtype=torch.uint8, device=x.device)
-    _lib.check(L.cd_unet_conv3x3(_ptr(weight), None if bias is None else _ptr(bias), _ptr(x.contiguous()), _ptr(y),
+    _lib.check(L.cd_unet_conv3x3(_ptr(weight), None if bias is None else _ptr(bias), _ptr(xp), _ptr(yp),
                                  cin, cout, int(dgrad), B, H, W, _ptr(ws), nb, _stream()), "unet_conv3x3")
-    return y, ws
+    return from_planes(yp), ws
 
 
 def conv3x3_wgrad(x, dz, cin: int, cout: int):
-    """[dW (3,3,cin,cout), db (cout,)] of a 3x3 conv layer (cd_unet_conv3x3_wgrad)."""
+    """[dW (3,3,cin,cout), db (cout,)] of a 3x3 conv layer (cd_unet_conv3x3_wgrad);
+    x, dz as for conv3x3."""
     B, H, W, _ = x.shape
     L = _lib.lib()
     nb = int(L.cd_unet_conv3x3_wgrad_workspace_size(cin, cout, B, H, W))
     ws = torch.zeros((max(nb, 1),), dtype=torch.uint8, device=x.device)
     g = torch.empty((9 * cin * cout + cout,), dtype=torch.float32, device=x.device)
-    _lib.check(L.cd_unet_conv3x3_wgrad(_ptr(x.contiguous()), _ptr(dz.contiguous()), _ptr(g), cin, cout, B, H, W,
-                                       _ptr(ws), nb, _stream()), "unet_conv3x3_wgrad")
+    xp, dzp = to_planes(x), to_planes(dz)   # held until the launch is queued
+    _lib.check(L.cd_unet_conv3x3_wgrad(_ptr(xp), _ptr(dzp), _ptr(g), cin, cout, B, H, W, _ptr(ws), nb, _stream()),
+               "unet_conv3x3_wgrad")
     return g[:9 * cin * cout].view(3, 3, cin, cout), g[9 * cin * cout:], ws

@@ -374,8 +374,9 @@ CD_API cd_status cd_adam_update(float *params, const float *grads, float *m, flo
                                 cudaStream_t stream);
 
 /* One 3x3 'same' conv layer of the network through the same tensor-core    */
-/* kernels (for layer-level checks).  x, y: NHWC bf16 with channel counts    */
-/* rounded up to multiples of 8.  dgrad = 0: y = relu(conv(x) + bias),       */
+/* kernels (for layer-level checks).  x, y, dz: bf16 row-chunk planes         */
+/* [B][H][C/8][W][8] (C rounded up to a multiple of 8; with C = 8 this is     */
+/* NHWC), 16-byte aligned.  dgrad = 0: y = relu(conv(x) + bias),             */
 /* x has cin channels, y cout; dgrad = 1: y = dL/dx given x = dL/dz (the     */
 /* pre-activation gradient, cout channels), no bias, no ReLU.  cin in        */
 /* {8, 15, 16, 24, 32, 48}, cout in {8, 16, 32}.                              */
