@@ -53,9 +53,21 @@ __global__ void __launch_bounds__(256) variance_kernel(const float *__restrict__
             az += v.z;
             ++n;
         }
-    const float fn = (float)n;
     const float3 c = ld3(img, (size_t)cy * W + cx);
-    const float v = norm2(ax / fn - c.x, ay / fn - c.y, az / fn - c.z);
+    float mx, my, mz;
+    if (n == 8) {
+        // interior pixels: a quotient by 8 is the product by 1/8, exactly
+        // (__fmul_rn: rounded on its own, never fused into the subtraction)
+        mx = __fmul_rn(ax, 0.125f);
+        my = __fmul_rn(ay, 0.125f);
+        mz = __fmul_rn(az, 0.125f);
+    } else {
+        const float fn = (float)n;
+        mx = ax / fn;
+        my = ay / fn;
+        mz = az / fn;
+    }
+    const float v = norm2(mx - c.x, my - c.y, mz - c.z);
     var[(size_t)cy * W + cx] = v;
     sd[(size_t)cy * W + cx] = sqrtf(v);
 }
@@ -302,7 +314,7 @@ template <int N> CD_DEV void cp_async_wait() { asm volatile("cp.async.wait_group
 
 CD_DEV int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
 
-__global__ void __launch_bounds__(kThreads) regression_kernel(
+__global__ void __launch_bounds__(kThreads, 8) regression_kernel(
     const float *__restrict__ imga, const float *__restrict__ imgb,
     const float *__restrict__ albedo, const float *__restrict__ normal,
     const float *__restrict__ vara, const float *__restrict__ varb,
