@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(kN) tconv_bwd_kernel(const __nv_bfloat16 *__re
                                                         __nv_bfloat16 *__restrict__ dz_in, float *__restrict__ partial,
                                                         int Hi, int Wi, int B)
 {
-    __shared__ float sK[CO * CI];
+    __shared__ __align__(16) float sK[CO * CI];
     __shared__ float sx[kN][CI + 1], sd[kN][CO + 1], sb[kN][CO + 1];
     for (int i = threadIdx.x; i < CO * CI; i += blockDim.x) sK[i] = K[i];
     const size_t n = (size_t)B * Hi * Wi;
@@ -147,28 +147,61 @@ __global__ void __launch_bounds__(kN) tconv_bwd_kernel(const __nv_bfloat16 *__re
     }
     __syncthreads();
     if (p < n) {
+        // co outer, ci inner: each g[ci] still sums over co in order, and a
+        // row of K is read as float4s
         float g[CI];
 #pragma unroll
-        for (int ci = 0; ci < CI; ++ci) {
-            float s = 0.f;
+        for (int ci = 0; ci < CI; ++ci) g[ci] = 0.f;
 #pragma unroll
-            for (int co = 0; co < CO; ++co) s = fmaf(sK[co * CI + ci], d[co], s);
-            g[ci] = x[ci] > 0.f ? s : 0.f;
+        for (int co = 0; co < CO; ++co) {
+            const float4 *kr = reinterpret_cast<const float4 *>(sK + co * CI);
+#pragma unroll
+            for (int c4 = 0; c4 < CI / 4; ++c4) {
+                const float4 k4 = kr[c4];
+                g[4 * c4] = fmaf(k4.x, d[co], g[4 * c4]);
+                g[4 * c4 + 1] = fmaf(k4.y, d[co], g[4 * c4 + 1]);
+                g[4 * c4 + 2] = fmaf(k4.z, d[co], g[4 * c4 + 2]);
+                g[4 * c4 + 3] = fmaf(k4.w, d[co], g[4 * c4 + 3]);
+            }
         }
+#pragma unroll
+        for (int ci = 0; ci < CI; ++ci) g[ci] = x[ci] > 0.f ? g[ci] : 0.f;
 #pragma unroll
         for (int c = 0; c < CI; c += 8) st8(dz_in + act_idx(b, yi, c / 8, xi, Hi, Wi, CI / 8) * 8, g + c);
     }
     float *out = partial + (size_t)blockIdx.x * (CO * CI + CO);
-    for (int j = t; j < CO * CI + CO; j += kN) {
-        float s = 0.f;
-        if (j < CO * CI) {
-            const int co = j / CI, ci = j - co * CI;
-            for (int k = 0; k < kN; ++k) s = fmaf(sd[k][co], sx[k][ci], s);
-        } else {
-            const int co = j - CO * CI;
-            for (int k = 0; k < kN; ++k) s += sb[k][co];
+    // dK in TM x TN register tiles (each output sums over the block's pixels
+    // in order), then db
+    constexpr int TN = (CO * CI) / kN >= 4 ? 4 : (CO * CI) / kN, TM = (CO * CI) / (kN * TN);
+    static_assert(TM >= 1 && TM * TN * kN == CO * CI && CI % TN == 0 && CO % TM == 0, "register tiles cover dK");
+    {
+        const int tci = t % (CI / TN), tco = t / (CI / TN);
+        const int ci0 = TN * tci, co0 = TM * tco;
+        float s[TM][TN];
+#pragma unroll
+        for (int a = 0; a < TM; ++a)
+#pragma unroll
+            for (int c = 0; c < TN; ++c) s[a][c] = 0.f;
+        for (int k = 0; k < kN; ++k) {
+            float dv[TM], xv[TN];
+#pragma unroll
+            for (int a = 0; a < TM; ++a) dv[a] = sd[k][co0 + a];
+#pragma unroll
+            for (int c = 0; c < TN; ++c) xv[c] = sx[k][ci0 + c];
+#pragma unroll
+            for (int a = 0; a < TM; ++a)
+#pragma unroll
+                for (int c = 0; c < TN; ++c) s[a][c] = fmaf(dv[a], xv[c], s[a][c]);
         }
-        out[j] = s;
+#pragma unroll
+        for (int a = 0; a < TM; ++a)
+#pragma unroll
+            for (int c = 0; c < TN; ++c) out[(co0 + a) * CI + ci0 + c] = s[a][c];
+    }
+    if (t < CO) {
+        float s = 0.f;
+        for (int k = 0; k < kN; ++k) s += sb[k][t];
+        out[CO * CI + t] = s;
     }
 }
 
@@ -198,21 +231,31 @@ __global__ void __launch_bounds__(256) head_fwd_kernel(const __nv_bfloat16 *__re
 }
 
 // Head backward: dZ of c5_1 (times its ReLU derivative) and the block's
-// partial sums of dKh[ci][co] and dbh[co].
-__global__ void __launch_bounds__(128) head_bwd_kernel(const __nv_bfloat16 *__restrict__ x, const float *__restrict__ K,
-                                                       const float *__restrict__ bias, const float *__restrict__ gband,
-                                                       const float *__restrict__ galpha, __nv_bfloat16 *__restrict__ dz,
-                                                       float *__restrict__ partial, size_t n)
+// partial sums of dKh[ci][co] and dbh[co].  Each thread walks pixels
+// p = thread, thread + grid size, ... accumulating its 54 parameter-gradient
+// terms in registers; the block then reduces them (lanes, then warps, in a
+// fixed order) to one partial row.
+constexpr int kHeadThreads = 256;
+constexpr int kHeadMaxBlocks = 592;
+
+__global__ void __launch_bounds__(kHeadThreads) head_bwd_kernel(const __nv_bfloat16 *__restrict__ x,
+                                                                const float *__restrict__ K,
+                                                                const float *__restrict__ bias,
+                                                                const float *__restrict__ gband,
+                                                                const float *__restrict__ galpha,
+                                                                __nv_bfloat16 *__restrict__ dz,
+                                                                float *__restrict__ partial, size_t n)
 {
-    constexpr int kN = 128;
     __shared__ float sK[54];
-    __shared__ float sx[kN][9], sg[kN][7];
+    __shared__ float red[kHeadThreads / 32][54];
     if (threadIdx.x < 54) sK[threadIdx.x] = threadIdx.x < 48 ? K[threadIdx.x] : bias[threadIdx.x - 48];
     __syncthreads();
-    const int t = threadIdx.x;
-    const size_t p = (size_t)blockIdx.x * kN + t;
-    float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, g[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (p < n) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float acc[54];
+#pragma unroll
+    for (int j = 0; j < 54; ++j) acc[j] = 0.f;
+    for (size_t p = (size_t)blockIdx.x * kHeadThreads + threadIdx.x; p < n; p += (size_t)gridDim.x * kHeadThreads) {
+        float v[8], g[6];
         ld8(x + 8 * p, v);
 #pragma unroll
         for (int co = 0; co < 6; ++co) {
@@ -236,25 +279,32 @@ __global__ void __launch_bounds__(128) head_bwd_kernel(const __nv_bfloat16 *__re
             d[ci] = v[ci] > 0.f ? s : 0.f;
         }
         st8(dz + 8 * p, d);
+#pragma unroll
+        for (int ci = 0; ci < 8; ++ci)
+#pragma unroll
+            for (int co = 0; co < 6; ++co) acc[ci * 6 + co] = fmaf(v[ci], g[co], acc[ci * 6 + co]);
+#pragma unroll
+        for (int co = 0; co < 6; ++co) acc[48 + co] += g[co];
     }
 #pragma unroll
-    for (int c = 0; c < 8; ++c) sx[t][c] = v[c];
+    for (int j = 0; j < 54; ++j) {
+        float s = acc[j];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) sg[t][c] = g[c];
+        for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) red[warp][j] = s;
+    }
     __syncthreads();
-    if (t < 54) {
+    if (threadIdx.x < 54) {
         float s = 0.f;
-        if (t < 48) {
-            const int ci = t / 6, co = t - 6 * ci;
-            for (int k = 0; k < kN; ++k) s = fmaf(sx[k][ci], sg[k][co], s);
-        } else {
-            for (int k = 0; k < kN; ++k) s += sg[k][t - 48];
-        }
-        partial[(size_t)blockIdx.x * 54 + t] = s;
+        for (int w = 0; w < kHeadThreads / 32; ++w) s += red[w][threadIdx.x];
+        partial[(size_t)blockIdx.x * 54 + threadIdx.x] = s;
     }
 }
 
-// dZ = (maxpool backward of dpool + dskip) * [act > 0], C channels (multiple of 8)
+// dZ = (maxpool backward of dpool + dskip) * [act > 0], C channels (multiple
+// of 8).  One thread per pooled pixel (H and W even): it reads the four
+// pixels of its 2x2 window once per 8-channel chunk; the pooled gradient
+// goes to the first maximum of the window (row-major), as in the forward.
 template <int C>
 __global__ void __launch_bounds__(256) pool_bwd_kernel(const __nv_bfloat16 *__restrict__ act,
                                                        const __nv_bfloat16 *__restrict__ pooled,
@@ -262,43 +312,41 @@ __global__ void __launch_bounds__(256) pool_bwd_kernel(const __nv_bfloat16 *__re
                                                        const __nv_bfloat16 *__restrict__ dskip,
                                                        __nv_bfloat16 *__restrict__ dz, int H, int W, int B)
 {
-    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= (size_t)B * H * W) return;
-    const int x = (int)(q % W), y = (int)((q / W) % H), b = (int)(q / ((size_t)W * H));
-    const int PH = H / 2, PW = W / 2;
     constexpr int NC = C / 8;
-    float a[C], g[C];
+    const int PH = H / 2, PW = W / 2;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (size_t)B * PH * PW) return;
+    const int px = (int)(q % PW), py = (int)((q / PW) % PH), b = (int)(q / ((size_t)PW * PH));
 #pragma unroll
-    for (int c = 0; c < C; c += 8) {
-        ld8(act + act_idx(b, y, c / 8, x, H, W, NC) * 8, a + c);
-        ld8(dskip + act_idx(b, y, c / 8, x, H, W, NC) * 8, g + c);
-    }
-    const int py = y / 2, px = x / 2;
-    if (py < PH && px < PW) {
-        float m[C], dp[C];
+    for (int c = 0; c < NC; ++c) {
+        float m[8], dp[8], a[4][8], g[4][8];
+        ld8(pooled + act_idx(b, py, c, px, PH, PW, NC) * 8, m);
+        ld8(dpool + act_idx(b, py, c, px, PH, PW, NC) * 8, dp);
 #pragma unroll
-        for (int c = 0; c < C; c += 8) {
-            ld8(pooled + act_idx(b, py, c / 8, px, PH, PW, NC) * 8, m + c);
-            ld8(dpool + act_idx(b, py, c / 8, px, PH, PW, NC) * 8, dp + c);
+        for (int k = 0; k < 4; ++k) {
+            const size_t r = act_idx(b, 2 * py + (k >> 1), c, 2 * px + (k & 1), H, W, NC) * 8;
+            ld8(act + r, a[k]);
+            ld8(dskip + r, g[k]);
         }
-        // position of this pixel in its window and of the first maximum before it
-        const int me = (y & 1) * 2 + (x & 1);
 #pragma unroll
-        for (int c = 0; c < C; ++c) {
-            if (a[c] != m[c]) continue;
-            bool first = true;
-            for (int k = 0; k < me; ++k) {
-                const size_t r = act_idx(b, 2 * py + (k >> 1), c / 8, 2 * px + (k & 1), H, W, NC);
-                if (__bfloat162float(act[r * 8 + (c & 7)]) == m[c]) first = false;
+        for (int e = 0; e < 8; ++e) {
+            bool taken = false;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (!taken && a[k][e] == m[e]) {
+                    g[k][e] += dp[e];
+                    taken = true;
+                }
             }
-            if (first) g[c] += dp[c];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+                if (!(a[k][e] > 0.f)) g[k][e] = 0.f;
+            st8(dz + act_idx(b, 2 * py + (k >> 1), c, 2 * px + (k & 1), H, W, NC) * 8, g[k]);
         }
     }
-#pragma unroll
-    for (int c = 0; c < C; ++c)
-        if (!(a[c] > 0.f)) g[c] = 0.f;
-#pragma unroll
-    for (int c = 0; c < C; c += 8) st8(dz + act_idx(b, y, c / 8, x, H, W, NC) * 8, g + c);
 }
 
 // Two-stage fixed-order reduction of per-tile partial sums: stage 1 sums
@@ -396,12 +444,16 @@ cudaError_t launch_head_fwd(const __nv_bfloat16 *x, const float *K, const float 
     return cudaGetLastError();
 }
 
-size_t head_blocks(size_t n) { return (n + 127) / 128; }
+size_t head_blocks(size_t n)
+{
+    const size_t g = (n + kHeadThreads - 1) / kHeadThreads;
+    return g < (size_t)kHeadMaxBlocks ? g : (size_t)kHeadMaxBlocks;
+}
 
 cudaError_t launch_head_bwd(const __nv_bfloat16 *x, const float *K, const float *bias, const float *gband,
                             const float *galpha, __nv_bfloat16 *dz, float *partial, size_t n, cudaStream_t st)
 {
-    head_bwd_kernel<<<(unsigned)head_blocks(n), 128, 0, st>>>(x, K, bias, gband, galpha, dz, partial, n);
+    head_bwd_kernel<<<(unsigned)head_blocks(n), kHeadThreads, 0, st>>>(x, K, bias, gband, galpha, dz, partial, n);
     return cudaGetLastError();
 }
 
@@ -409,7 +461,8 @@ cudaError_t launch_pool_bwd(int C, const __nv_bfloat16 *act, const __nv_bfloat16
                             const __nv_bfloat16 *dpool, const __nv_bfloat16 *dskip, __nv_bfloat16 *dz, int H, int W,
                             int B, cudaStream_t st)
 {
-    const size_t n = (size_t)B * H * W;
+    if ((H | W) & 1) return cudaErrorInvalidValue;   // the network's levels are even-sized
+    const size_t n = (size_t)B * (H / 2) * (W / 2);
     const unsigned g = (unsigned)((n + 255) / 256);
     if (C == 8) pool_bwd_kernel<8><<<g, 256, 0, st>>>(act, pooled, dpool, dskip, dz, H, W, B);
     else if (C == 16) pool_bwd_kernel<16><<<g, 256, 0, st>>>(act, pooled, dpool, dskip, dz, H, W, B);
