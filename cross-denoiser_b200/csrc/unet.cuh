@@ -53,8 +53,6 @@ struct ConvParams {
 };
 
 int build_steps(int c0, int c1, KStep *steps, StepHalf (*half)[2]);
-int conv_rows(int nout, int nch);
-size_t conv_smem_bytes(int nsteps, int nout, int nch);
 cudaError_t launch_conv3x3(const ConvParams &P, int B, int nout, cudaStream_t st);
 
 // Pack fp32 Keras weights W[3][3][cin][cout] into the B operand of a conv

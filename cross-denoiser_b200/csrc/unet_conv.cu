@@ -426,29 +426,38 @@ cudaError_t launch_wgrad_t(const WgradParams &P, int B, cudaStream_t st)
 // TMEM over all their tiles; one partial sum per CTA, read out of TMEM by
 // warps 2..5 at the end.  Every wait is bounded.
 constexpr int kWgrad3Smem = 225 * 1024;
-constexpr int kWgrad3Tail = 16 * kZPlane + 2048;   // discarded A rows read up to 16 planes past a row
+
+// shared memory past the last stage: discarded A rows (M groups past the
+// layer's 3 x chunks) read up to 16 planes past a row, then the barriers
+__host__ __device__ inline size_t wgrad3_tail(int tw) { return (size_t)16 * tw * 16 + 2048; }
 
 __host__ __device__ inline size_t align1k(size_t n) { return (n + 1023) & ~(size_t)1023; }
 
 struct Wgrad3Plan {
-    int R, S;
+    int TW, R, S;   // tile width (pixels), input rows per tile, ring slots
     size_t zbytes, xbytes, stage, smem;
 };
 
+// Tiles 256 pixels wide where three ring slots fit (half the bulk copies
+// per pixel: each row-plane copy is 4 KB), else 128.
 inline Wgrad3Plan wgrad3_plan(int xc0, int xc1, int zc)
 {
     Wgrad3Plan p{};
-    for (int R = 8; R >= 1; R >>= 1) {
-        p.R = R;
-        p.zbytes = (size_t)(R + 2) * zc * kZPlane;
-        p.xbytes = (size_t)R * 3 * (xc0 + xc1) * kZPlane;
-        p.stage = align1k(p.zbytes) + align1k(p.xbytes);
-        const int S = (int)((kWgrad3Smem - kWgrad3Tail) / p.stage);
-        p.S = S > 6 ? 6 : S;
-        p.smem = p.S * p.stage + kWgrad3Tail;
-        if (p.S >= 4) break;
+    for (int tw = 256; tw >= 128; tw >>= 1) {
+        const size_t tail = wgrad3_tail(tw);
+        for (int R = 8; R >= 1; R >>= 1) {
+            p.TW = tw;
+            p.R = R;
+            p.zbytes = (size_t)(R + 2) * zc * tw * 16;
+            p.xbytes = (size_t)R * 3 * (xc0 + xc1) * tw * 16;
+            p.stage = align1k(p.zbytes) + align1k(p.xbytes);
+            const int S = (int)((kWgrad3Smem - tail) / p.stage);
+            p.S = S > 6 ? 6 : S;
+            p.smem = p.S * p.stage + tail;
+            if (p.S >= (tw == 256 ? 3 : 4)) return p;
+        }
     }
-    return p;
+    return p;   // 128-pixel tiles, one row: S may be below 4
 }
 
 __host__ __device__ inline int pow2_cols(int n)
@@ -458,22 +467,23 @@ __host__ __device__ inline int pow2_cols(int n)
     return c;
 }
 
-template <int ZC>
+template <int ZC, int TW>
 __global__ void __launch_bounds__(kWgradThreads, 1)
     wgrad3_kernel(const WgradParams P, int R, int S, int stage_bytes, int ntx, int nty, int ntiles)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     constexpr int N = (24 * ZC + 15) & ~15;
+    constexpr int kTP = TW * 16;   // bytes per staged plane
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int xc0 = P.xc0, xc1 = P.xc1, xc = xc0 + xc1;
     const bool split = 3 * xc > 16;   // one MMA (accumulator) per source
     const uint32_t cols = (uint32_t)pow2_cols(split ? 2 * N : N);
-    const uint32_t zbytes = (uint32_t)((R + 2) * ZC * kZPlane), xbytes = (uint32_t)(R * 3 * xc * kZPlane);
+    const uint32_t zbytes = (uint32_t)((R + 2) * ZC * kTP), xbytes = (uint32_t)(R * 3 * xc * kTP);
     const uint32_t xoff = (zbytes + 1023u) & ~1023u;
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)S * stage_bytes + 16 * kZPlane);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)S * stage_bytes + 16 * kTP);
     uint64_t *empty = full + S;
     uint32_t *tslot = reinterpret_cast<uint32_t *>(empty + S);
-    float *red = reinterpret_cast<float *>(smem + (size_t)S * stage_bytes + 16 * kZPlane + 1024);   // [4][8 * ZC]
+    float *red = reinterpret_cast<float *>(smem + (size_t)S * stage_bytes + 16 * kTP + 1024);   // [4][8 * ZC]
 
     if (warp == 1) tc::tmem_alloc(tslot, cols);
     if (tid == 0) {
@@ -511,7 +521,7 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
                 }
             }
             const int tx = tile % ntx, ty = (tile / ntx) % nty, b = tile / (ntx * nty);
-            const int x0 = tx * kPx, y0 = ty * R;
+            const int x0 = tx * TW, y0 = ty * R;
             uint8_t *st = smem + (size_t)s * stage_bytes;
             if (lane == 0) tc::mbar_expect_tx(&full[s], zbytes + xbytes);
             __syncwarp();   // the transaction count is raised before any copy lands
@@ -521,7 +531,7 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
                     const int r = q / ZC, c = q - r * ZC, gy = y0 - 1 + r;
                     const __nv_bfloat16 *row =
                         gy >= 0 && gy < P.H ? P.dz + act_idx(b, gy, c, 0, P.H, P.W, ZC) * 8 : nullptr;
-                    stage_plane(st + (size_t)q * kZPlane, row, x0, kPx, P.W, &full[s]);
+                    stage_plane(st + (size_t)q * kTP, row, x0, TW, P.W, &full[s]);
                 } else {
                     // input row r, planes [kx][chunk] of source 0 then of source 1
                     const int u = q - nz, r = u / (3 * xc), v = u - r * 3 * xc, gy = y0 + r;
@@ -529,7 +539,7 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
                     const int xs = s1 ? xc1 : xc0, w = s1 ? v - 3 * xc0 : v, kx = w / xs, c = w - kx * xs;
                     const __nv_bfloat16 *row =
                         gy < P.H ? (s1 ? P.x1 : P.x0) + act_idx(b, gy, c, 0, P.H, P.W, xs) * 8 : nullptr;
-                    stage_plane(st + xoff + (size_t)u * kZPlane, row, x0 - 1 + kx, kPx, P.W, &full[s]);
+                    stage_plane(st + xoff + (size_t)u * kTP, row, x0 - 1 + kx, TW, P.W, &full[s]);
                 }
             }
         }
@@ -552,13 +562,13 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
                 const uint32_t sb = tc::smem_u32(smem + (size_t)s * stage_bytes);
                 // descriptors of row 0, pixel group 0; rows and groups at
                 // constant strides (start field in 16-byte units)
-                const uint64_t bd0 = tc::sdesc(sb, 128, kZPlane), ad0 = tc::sdesc(sb + xoff, 128, kZPlane);
-                const uint64_t ad1 = ad0 + ((uint64_t)(3 * xc0 * kZPlane) >> 4);
+                const uint64_t bd0 = tc::sdesc(sb, 128, kTP), ad0 = tc::sdesc(sb + xoff, 128, kTP);
+                const uint64_t ad1 = ad0 + ((uint64_t)(3 * xc0 * kTP) >> 4);
                 for (int r = 0; r < R; ++r) {
-                    const uint64_t br = bd0 + ((uint64_t)(r * ZC * kZPlane) >> 4);
-                    const uint64_t ar = (uint64_t)(r * 3 * xc * kZPlane) >> 4;
+                    const uint64_t br = bd0 + ((uint64_t)(r * ZC * kTP) >> 4);
+                    const uint64_t ar = (uint64_t)(r * 3 * xc * kTP) >> 4;
 #pragma unroll
-                    for (int g = 0; g < kPx / 16; ++g) {
+                    for (int g = 0; g < TW / 16; ++g) {
                         const uint32_t acc = (i | r | g) ? 1u : 0u;
                         const uint64_t gg = (uint64_t)(256 * g) >> 4;
                         tc::mma_bf16(tbase, ad0 + ar + gg, br + gg, idesc, acc);
@@ -573,7 +583,7 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
         ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
     } else {
         // ---- bias warps: the tile's centre gradient rows (staged rows 1..R) ----
-        const int px = tid - 64;
+        const int px0 = tid - 64;   // pixels px0, px0 + 128, ...
         for (int i = 0; i < ntile; ++i) {
             const int s = i % S;
             bool got = true;
@@ -585,8 +595,10 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
             const uint8_t *st = smem + (size_t)s * stage_bytes;
             for (int r = 1; r <= R; ++r)
 #pragma unroll
-                for (int c = 0; c < ZC; ++c) {
-                    const uint4 raw = *reinterpret_cast<const uint4 *>(st + (size_t)(r * ZC + c) * kZPlane + 16 * px);
+                for (int c = 0; c < ZC; ++c)
+#pragma unroll
+                for (int px = px0; px < TW; px += 128) {
+                    const uint4 raw = *reinterpret_cast<const uint4 *>(st + (size_t)(r * ZC + c) * kTP + 16 * px);
                     const __nv_bfloat162 *h2 = reinterpret_cast<const __nv_bfloat162 *>(&raw);
 #pragma unroll
                     for (int e = 0; e < 4; ++e) {
@@ -659,23 +671,31 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
     if (warp == 1) tc::tmem_dealloc(tbase, cols);
 }
 
+template <int ZC, int TW>
+cudaError_t launch_wgrad3_tw(const WgradParams &P, const Wgrad3Plan &p, int B, int grid, cudaStream_t st)
+{
+    cudaError_t e = cudaFuncSetAttribute(wgrad3_kernel<ZC, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)p.smem);
+    if (e != cudaSuccess) return e;
+    const int ntx = (P.W + TW - 1) / TW, nty = (P.H + p.R - 1) / p.R;
+    wgrad3_kernel<ZC, TW><<<grid, kWgradThreads, p.smem, st>>>(P, p.R, p.S, (int)p.stage, ntx, nty, B * ntx * nty);
+    return cudaGetLastError();
+}
+
 template <int ZC>
 cudaError_t launch_wgrad3_t(const WgradParams &P, int B, int grid, cudaStream_t st)
 {
     const Wgrad3Plan p = wgrad3_plan(P.xc0, P.xc1, ZC);
     if (p.S < 2) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(wgrad3_kernel<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
-    if (e != cudaSuccess) return e;
-    const int ntx = (P.W + kPx - 1) / kPx, nty = (P.H + p.R - 1) / p.R;
-    wgrad3_kernel<ZC><<<grid, kWgradThreads, p.smem, st>>>(P, p.R, p.S, (int)p.stage, ntx, nty, B * ntx * nty);
-    return cudaGetLastError();
+    return p.TW == 256 ? launch_wgrad3_tw<ZC, 256>(P, p, B, grid, st) : launch_wgrad3_tw<ZC, 128>(P, p, B, grid, st);
 }
 
 }  // namespace
 
-int conv_rows(int nout, int nch) { return nout >= 32 ? 4 : (nch > 4 ? 4 : 8); }
+// Output rows per CTA: 4 (more CTAs per SM than 8-row tiles; measured faster
+// in the whole network although the row halo grows from 25 to 50 %).
+constexpr int kConvRows = 4;
 
-size_t conv_smem_bytes(int nsteps, int nout, int nch) { return conv_smem(nsteps, nout, nch, 0, conv_rows(nout, nch)); }
 
 // K-step table for input chunks split over two sources (c0 chunks of source
 // 0, then c1 of source 1; 8 channels each), per source: channel pairs of
@@ -711,10 +731,9 @@ int build_steps(int c0, int c1, KStep *steps, StepHalf (*half)[2])
 
 cudaError_t launch_conv3x3(const ConvParams &P, int B, int nout, cudaStream_t st)
 {
-    const int nch = P.c0 + P.c1;
-    if (nout == 16) return conv_rows(16, nch) == 8 ? launch_t<16, 8>(P, B, st) : launch_t<16, 4>(P, B, st);
-    if (nout == 32) return launch_t<32, 4>(P, B, st);
-    if (nout == 48) return launch_t<48, 4>(P, B, st);
+    if (nout == 16) return launch_t<16, kConvRows>(P, B, st);
+    if (nout == 32) return launch_t<32, kConvRows>(P, B, st);
+    if (nout == 48) return launch_t<48, kConvRows>(P, B, st);
     return cudaErrorInvalidValue;
 }
 
@@ -756,8 +775,8 @@ static bool wgrad3_fits(const WgradParams &P)
 int wgrad_partial_rows(const WgradParams &P, int B)
 {
     if (!wgrad3_fits(P)) return (int)wgrad_tiles(B, P.H, P.W);
-    const int R = wgrad3_plan(P.xc0, P.xc1, P.zc).R;
-    const int tiles = B * ((P.W + kPx - 1) / kPx) * ((P.H + R - 1) / R);
+    const Wgrad3Plan p = wgrad3_plan(P.xc0, P.xc1, P.zc);
+    const int tiles = B * ((P.W + p.TW - 1) / p.TW) * ((P.H + p.R - 1) / p.R);
     return tiles < sm_count() ? tiles : sm_count();
 }
 

@@ -349,30 +349,28 @@ __global__ void __launch_bounds__(256) pool_bwd_kernel(const __nv_bfloat16 *__re
     }
 }
 
-// Two-stage fixed-order reduction of per-tile partial sums: stage 1 sums
-// groups of kGroup consecutive tiles (grid y = group), stage 2 sums the groups.
-constexpr int kGroup = 64;
+// Fixed-order reduction of per-tile partial sums, one launch: a block owns
+// 32 output columns (lane = column) and its 32 warps take the rows
+// t = warp, warp + 32, ... in order; the warps' sums are then added in warp
+// order.  The same partials always give the same result.
+constexpr int kReduceWarps = 32;
 
-__global__ void __launch_bounds__(256) reduce_group_kernel(const float *__restrict__ partial,
-                                                           float *__restrict__ out, int n, int tiles)
+__global__ void __launch_bounds__(32 * kReduceWarps) reduce_kernel(const float *__restrict__ partial,
+                                                                   float *__restrict__ out, int n, int tiles)
 {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    const int t0 = blockIdx.y * kGroup, t1 = min(tiles, t0 + kGroup);
+    __shared__ float red[kReduceWarps][33];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int j = blockIdx.x * 32 + lane;
     float s = 0.f;
-    for (int t = t0; t < t1; ++t) s += partial[(size_t)t * n + j];
-    out[(size_t)blockIdx.y * n + j] = s;
-}
-
-// out[j] = sum over t < tiles of partial[t * n + j], in order of t
-__global__ void __launch_bounds__(256) reduce_kernel(const float *__restrict__ partial, float *__restrict__ out,
-                                                     int n, int tiles)
-{
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    float s = 0.f;
-    for (int t = 0; t < tiles; ++t) s += partial[(size_t)t * n + j];
-    out[j] = s;
+    if (j < n)
+        for (int t = warp; t < tiles; t += kReduceWarps) s += __ldg(partial + (size_t)t * n + j);
+    red[warp][lane] = s;
+    __syncthreads();
+    if (warp == 0 && j < n) {
+        float v = 0.f;
+        for (int w = 0; w < kReduceWarps; ++w) v += red[w][lane];
+        out[j] = v;
+    }
 }
 
 // The update count lives in device memory (so a captured graph replays
@@ -470,18 +468,11 @@ cudaError_t launch_pool_bwd(int C, const __nv_bfloat16 *act, const __nv_bfloat16
     return cudaGetLastError();
 }
 
-size_t reduce_floats(int n, int tiles) { return (size_t)n * tiles + (size_t)n * ((tiles + kGroup - 1) / kGroup); }
+size_t reduce_floats(int n, int tiles) { return (size_t)n * tiles; }
 
 cudaError_t launch_reduce(float *partial, float *out, int n, int tiles, cudaStream_t st)
 {
-    if (tiles <= kGroup) {
-        reduce_kernel<<<(n + 255) / 256, 256, 0, st>>>(partial, out, n, tiles);
-        return cudaGetLastError();
-    }
-    const int groups = (tiles + kGroup - 1) / kGroup;
-    float *mid = partial + (size_t)n * tiles;
-    reduce_group_kernel<<<dim3((n + 255) / 256, groups), 256, 0, st>>>(partial, mid, n, tiles);
-    reduce_kernel<<<(n + 255) / 256, 256, 0, st>>>(mid, out, n, groups);
+    reduce_kernel<<<(n + 31) / 32, 32 * kReduceWarps, 0, st>>>(partial, out, n, tiles);
     return cudaGetLastError();
 }
 

@@ -24,8 +24,7 @@ cudaError_t launch_pool_bwd(int C, const __nv_bfloat16 *act, const __nv_bfloat16
                             const __nv_bfloat16 *dpool, const __nv_bfloat16 *dskip, __nv_bfloat16 *dz, int H, int W,
                             int B, cudaStream_t st);
 // Sum per-tile partials partial[t * n + j] over t into out[j] (fixed order).
-// The partial buffer must hold reduce_floats(n, tiles) floats: the tiles'
-// sums followed by room for the per-group sums.
+// The partial buffer holds reduce_floats(n, tiles) floats.
 size_t reduce_floats(int n, int tiles);
 cudaError_t launch_reduce(float *partial, float *out, int n, int tiles, cudaStream_t st);
 cudaError_t launch_adam(float *w, const float *g, float *m, float *v, int n, int *step, float lr, float b1, float b2,
