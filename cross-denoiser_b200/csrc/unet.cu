@@ -139,18 +139,26 @@ struct Ctx {
         if (e_ != cudaSuccess) return e_;  \
     } while (0)
 
-cudaError_t pack(const Ctx &c, int l, bool dgrad)
+// Pack the B operands of every 3x3 layer (forward tables, or the dgrad
+// tables of layers 1..10) in one launch.
+cudaError_t pack_all(const Ctx &c, bool dgrad)
 {
-    const LayerDef &d = kDef[l];
-    PackTable T{};
-    KStep st[kMaxSteps];
-    T.nsteps = dgrad ? build_steps(chunks(d.cout), 0, st, T.half) : build_steps(kSrc0[l], kSrc1[l], st, T.half);
-    T.nout = nout_of(dgrad ? d.cin : d.cout);
-    T.cin = d.cin;
-    T.cout = d.cout;
-    T.dgrad = dgrad ? 1 : 0;
-    __nv_bfloat16 *dst = reinterpret_cast<__nv_bfloat16 *>(c.ws + (dgrad ? c.L.pack_dg[l] : c.L.pack_fwd[l]));
-    return launch_pack(c.w(l), dst, T, c.st);
+    PackJobs J{};
+    for (int l = dgrad ? 1 : 0; l < kLayers; ++l) {
+        const LayerDef &d = kDef[l];
+        if (d.kind != CONV) continue;
+        PackJob &j = J.job[J.n++];
+        KStep st[kMaxSteps];
+        j.T.nsteps =
+            dgrad ? build_steps(chunks(d.cout), 0, st, j.T.half) : build_steps(kSrc0[l], kSrc1[l], st, j.T.half);
+        j.T.nout = nout_of(dgrad ? d.cin : d.cout);
+        j.T.cin = d.cin;
+        j.T.cout = d.cout;
+        j.T.dgrad = dgrad ? 1 : 0;
+        j.w = c.w(l);
+        j.dst = reinterpret_cast<__nv_bfloat16 *>(c.ws + (dgrad ? c.L.pack_dg[l] : c.L.pack_fwd[l]));
+    }
+    return launch_pack_jobs(J, c.st);
 }
 
 // conv of `l` (forward, or dgrad when dgrad) at pyramid level lvl
@@ -228,7 +236,9 @@ Side *side_stream(cudaStream_t main)
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(main, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return nullptr;
     Side sd;
-    if (cudaStreamCreateWithFlags(&sd.s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+    int prio = 0;   // the companion runs at the caller's stream priority
+    if (cudaStreamGetPriority(main, &prio) != cudaSuccess) prio = 0;
+    if (cudaStreamCreateWithPriority(&sd.s, cudaStreamNonBlocking, prio) != cudaSuccess) return nullptr;
     if (cudaEventCreateWithFlags(&sd.fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&sd.join, cudaEventDisableTiming) != cudaSuccess)
         return nullptr;
@@ -248,8 +258,7 @@ cudaError_t forward(const float *ols1, const float *ols2, const float *prev, con
 {
     Ctx c{static_cast<uint8_t *>(ws), layout(B, H, W), B, H, W, st, params};
     const size_t n0 = (size_t)B * H * W;
-    for (int l = 0; l < kLayers; ++l)
-        if (kDef[l].kind == CONV) CD_TRY(pack(c, l, false));
+    CD_TRY(pack_all(c, false));
     CD_TRY(launch_pack_input(ols1, ols2, prev, albedo, normal, c.buf(X0), n0, W, st));
     CD_TRY(conv(c, 0, false, 0, X0, 2, NONE, 0, C11, 1, NONE, 0, NONE, NONE, NONE));
     CD_TRY(conv(c, 1, false, 0, C11, 1, NONE, 0, C12, 1, NONE, 0, NONE, NONE, C13));
@@ -279,8 +288,7 @@ cudaError_t backward(const float *gband, const float *galpha, const float *param
         return wgrad(c, grads, l, lvl, x0, xc0, x1, xc1, dz, side->s, c.partial2());
     };
     auto body = [&]() -> cudaError_t {
-        for (int l = 1; l < kLayers; ++l)
-            if (kDef[l].kind == CONV) CD_TRY(pack(c, l, true));
+        CD_TRY(pack_all(c, true));
         // head
         CD_TRY(launch_head_bwd(c.buf(C51), c.w(11), c.b(11), gband, galpha, c.buf(DZ10), c.partial(), n0, st));
         CD_TRY(launch_reduce(c.partial(), grads + param_offset(11), 54, (int)head_blocks(n0), st));

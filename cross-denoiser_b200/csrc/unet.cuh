@@ -64,6 +64,19 @@ struct PackTable {
 };
 cudaError_t launch_pack(const float *w, __nv_bfloat16 *dst, const PackTable &T, cudaStream_t st);
 
+// Several layers' packing in one launch (one grid row per job).
+constexpr int kMaxPackJobs = 12;
+struct PackJob {
+    const float *w;
+    __nv_bfloat16 *dst;
+    PackTable T;
+};
+struct PackJobs {
+    PackJob job[kMaxPackJobs];
+    int n;
+};
+cudaError_t launch_pack_jobs(const PackJobs &J, cudaStream_t st);
+
 // Weight gradient of a 3x3 conv on the tensor cores: per CTA partial sums of
 // dW[ky][kx][cin][cout] and db[cout] over its pixel tile.
 struct WgradParams {

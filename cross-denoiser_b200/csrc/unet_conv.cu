@@ -262,9 +262,9 @@ cudaError_t launch_t(const ConvParams &P, int B, cudaStream_t st)
 // Packed B operand: per step s, half h, conv output row n, element e
 // (dst[((s * 2 + h) * nout + n) * 8 + e]) the weight of tap (ky, kx) from
 // conv input channel 8 * chunk + e to conv output channel n.
-__global__ void pack_kernel(const float *__restrict__ w, __nv_bfloat16 *__restrict__ dst, const PackTable T)
+__device__ __forceinline__ void pack_one(const float *__restrict__ w, __nv_bfloat16 *__restrict__ dst,
+                                         const PackTable &T, int i)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= T.nsteps * 2 * T.nout * 8) return;
     const int e = i & 7, n = (i >> 3) % T.nout, h = (i / (8 * T.nout)) & 1, s = i / (16 * T.nout);
     const StepHalf hf = T.half[s][h];
@@ -279,6 +279,18 @@ __global__ void pack_kernel(const float *__restrict__ w, __nv_bfloat16 *__restri
         }
     }
     dst[i] = __float2bfloat16_rn(v);
+}
+
+__global__ void pack_kernel(const float *__restrict__ w, __nv_bfloat16 *__restrict__ dst, const PackTable T)
+{
+    pack_one(w, dst, T, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// grid row j packs job j
+__global__ void pack_jobs_kernel(const __grid_constant__ PackJobs J)
+{
+    const PackJob &j = J.job[blockIdx.y];
+    pack_one(j.w, j.dst, j.T, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Weight gradient.  D_tap[cin x cout] = sum_p X[p + tap][cin] dZ[p][cout]:
@@ -742,6 +754,18 @@ cudaError_t launch_conv3x3(const ConvParams &P, int B, int nout, cudaStream_t st
 
 namespace cd {
 namespace unet {
+
+cudaError_t launch_pack_jobs(const PackJobs &J, cudaStream_t st)
+{
+    if (J.n < 1 || J.n > kMaxPackJobs) return cudaErrorInvalidValue;
+    int most = 0;
+    for (int j = 0; j < J.n; ++j) {
+        const int n = J.job[j].T.nsteps * 2 * J.job[j].T.nout * 8;
+        most = n > most ? n : most;
+    }
+    pack_jobs_kernel<<<dim3((most + 255) / 256, J.n), 256, 0, st>>>(J);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_pack(const float *w, __nv_bfloat16 *dst, const PackTable &T, cudaStream_t st)
 {

@@ -67,33 +67,48 @@ __global__ void __launch_bounds__(256) pack_input_kernel(const float *__restrict
     st8(x + act_idx(0, row, 1, px, 0, W, 2) * 8, v + 8);
 }
 
-// Conv2DTranspose(kernel 1, stride 2) forward, one thread per output pixel.
+// Conv2DTranspose(kernel 1, stride 2) forward, one thread per input pixel
+// (i, j): output (2i, 2j) = K x + b (each channel summed over ci in order,
+// K rows read as float4), outputs (2i, 2j + 1), (2i + 1, 2j), (2i + 1, 2j + 1)
+// = b.
 template <int CI, int CO>
 __global__ void __launch_bounds__(256) tconv_fwd_kernel(const __nv_bfloat16 *__restrict__ in,
                                                         const float *__restrict__ K, const float *__restrict__ bias,
                                                         __nv_bfloat16 *__restrict__ out, int Hi, int Wi, int B)
 {
-    __shared__ float sK[CO * CI + CO];
+    __shared__ __align__(16) float sK[CO * CI + CO];
     for (int i = threadIdx.x; i < CO * CI + CO; i += blockDim.x) sK[i] = i < CO * CI ? K[i] : bias[i - CO * CI];
     __syncthreads();
     const int Ho = 2 * Hi, Wo = 2 * Wi;
-    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= (size_t)B * Ho * Wo) return;
-    const int xo = (int)(q % Wo), yo = (int)((q / Wo) % Ho), b = (int)(q / ((size_t)Wo * Ho));
-    float o[CO];
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (size_t)B * Hi * Wi) return;
+    const int xi = (int)(p % Wi), yi = (int)((p / Wi) % Hi), b = (int)(p / ((size_t)Wi * Hi));
+    float x[CI];
 #pragma unroll
-    for (int c = 0; c < CO; ++c) o[c] = sK[CO * CI + c];
-    if (!(xo & 1) && !(yo & 1)) {
-        float x[CI];
+    for (int c = 0; c < CI; c += 8) ld8(in + act_idx(b, yi, c / 8, xi, Hi, Wi, CI / 8) * 8, x + c);
+    float o[CO], ob[CO];
 #pragma unroll
-        for (int c = 0; c < CI; c += 8) ld8(in + act_idx(b, yo / 2, c / 8, xo / 2, Hi, Wi, CI / 8) * 8, x + c);
+    for (int co = 0; co < CO; ++co) {
+        ob[co] = sK[CO * CI + co];
+        float s = ob[co];
+        const float4 *kr = reinterpret_cast<const float4 *>(sK + co * CI);
 #pragma unroll
-        for (int co = 0; co < CO; ++co)
-#pragma unroll
-            for (int ci = 0; ci < CI; ++ci) o[co] = fmaf(sK[co * CI + ci], x[ci], o[co]);
+        for (int c4 = 0; c4 < CI / 4; ++c4) {
+            const float4 k4 = kr[c4];
+            s = fmaf(k4.x, x[4 * c4], s);
+            s = fmaf(k4.y, x[4 * c4 + 1], s);
+            s = fmaf(k4.z, x[4 * c4 + 2], s);
+            s = fmaf(k4.w, x[4 * c4 + 3], s);
+        }
+        o[co] = s;
     }
 #pragma unroll
-    for (int c = 0; c < CO; c += 8) st8(out + act_idx(b, yo, c / 8, xo, Ho, Wo, CO / 8) * 8, o + c);
+    for (int c = 0; c < CO; c += 8) {
+        st8(out + act_idx(b, 2 * yi, c / 8, 2 * xi, Ho, Wo, CO / 8) * 8, o + c);
+        st8(out + act_idx(b, 2 * yi, c / 8, 2 * xi + 1, Ho, Wo, CO / 8) * 8, ob + c);
+        st8(out + act_idx(b, 2 * yi + 1, c / 8, 2 * xi, Ho, Wo, CO / 8) * 8, ob + c);
+        st8(out + act_idx(b, 2 * yi + 1, c / 8, 2 * xi + 1, Ho, Wo, CO / 8) * 8, ob + c);
+    }
 }
 
 // Conv2DTranspose backward: a block of kN input pixels computes
@@ -407,7 +422,7 @@ cudaError_t launch_pack_input(const float *a, const float *b, const float *c, co
 cudaError_t launch_tconv_fwd(int ci, int co, const __nv_bfloat16 *in, const float *K, const float *bias,
                              __nv_bfloat16 *out, int Hi, int Wi, int B, cudaStream_t st)
 {
-    const size_t n = (size_t)B * 4 * Hi * Wi;
+    const size_t n = (size_t)B * Hi * Wi;
     const unsigned g = (unsigned)((n + 255) / 256);
     if (ci == 32 && co == 32) tconv_fwd_kernel<32, 32><<<g, 256, 0, st>>>(in, K, bias, out, Hi, Wi, B);
     else if (ci == 16 && co == 16) tconv_fwd_kernel<16, 16><<<g, 256, 0, st>>>(in, K, bias, out, Hi, Wi, B);

@@ -153,7 +153,9 @@ class FrameStep:
             self.on_gradients(g_band, g_alpha)
             return
         if self._train_stream is None:
-            self._train_stream = torch.cuda.Stream(device)
+            # high priority: the update's small, latency-bound kernels are
+            # placed first and the next frame's FP32-bound ops fill the SMs
+            self._train_stream = torch.cuda.Stream(device, priority=-1)
             self._trained = torch.cuda.Event()
         ts = self._train_stream
         ts.wait_stream(torch.cuda.current_stream(device))
