@@ -414,62 +414,68 @@ cudaError_t launch_wgrad_t(const WgradParams &P, int B, cudaStream_t st)
     return cudaGetLastError();
 }
 
-// Persistent weight gradient: one MMA per input row and 16 pixels,
-//   D[(kx, cin) x (ky, cout)] += X_i^T[(kx, cin) x 16 px] dZ_i[16 px x (ky, cout)]
-// A holds input row i three times, shifted by kx - 1 pixels (planes [kx][chunk]
-// per source), so its M groups (kx, chunk) are consecutive 2 KB planes; B
-// holds the output-gradient rows i - 1, i, i + 1 (ky = 2, 1, 0), consecutive
-// staged rows, so its N groups (ky, chunk) are consecutive planes too.  M =
-// 128 rows cover 3 x nch chunk groups (a layer with more than 16 runs one MMA
-// per input source) and N is 24 x zc rounded up to 16: rows and columns past
-// them read other staged data and are discarded.  Both operands MN-major
-// (channels contiguous, pixels 16 bytes apart).
+// Persistent weight gradient: three MMAs per input row and 16 pixels, one
+// per horizontal tap kx,
+//   D_kx[cin x (ky, cout)] += X_i^T[cin x 16 px from x0 + 16g + kx - 1] dZ_i[16 px x (ky, cout)]
+// A is input row i as staged once (130 pixels from x0 - 1, planes per
+// chunk), the tap a 16-byte (one pixel) shift of its K start, so its M
+// groups are the chunk planes (source 0, then source 1); B holds the
+// output-gradient rows i - 1, i, i + 1 (ky = 2, 1, 0), consecutive staged
+// rows, so its N groups (ky, chunk) are consecutive planes.  M = 128 rows
+// cover the 8 x chunks input channels and N is 24 x zc rounded up to 16:
+// rows and columns past them read other staged data and are discarded.
+// Both operands MN-major (channels contiguous, pixels 16 bytes apart).
+// A tcgen05 MMA of this shape costs about the same for any N up to 64, so
+// the taps cost three MMAs; staging each input row once instead of three
+// shifted copies halves the L2 -> shared-memory traffic, which bounded it.
 //
 // A tile is R input rows x 128 pixels: the output gradient's R + 2 rows from
-// y0 - 1 and, per input row, source, kx and chunk, the 128 pixels from
-// x0 - 1 + kx (the three copies come from L2), one bulk copy per plane with
-// zeros outside the image (stage_plane), land in a ring of S stages.  The
-// warps specialise: warp 0 stages tile i into slot i % S once the slot's
-// "empty" barrier says its previous MMAs and bias reads are done (all 32
-// lanes issue copies); lane 0 of warp 1 issues the tile's MMAs when the slot
-// is full and commits them to "empty"; warps 2..5 sum the bias gradient (the
-// output gradient over the tile's R centre rows) from the staged planes and
-// arrive on "empty".  CTAs are persistent and keep their accumulators in
-// TMEM over all their tiles; one partial sum per CTA, read out of TMEM by
-// warps 2..5 at the end.  Every wait is bounded.
+// y0 - 1 (128 pixels from x0) and the input rows (130 pixels from x0 - 1),
+// one bulk copy per plane with zeros outside the image (stage_plane), land
+// in a ring of S stages.  The warps specialise: warp 0 stages tile i into
+// slot i % S once the slot's "empty" barrier says its previous MMAs and bias
+// reads are done (all 32 lanes issue copies); lane 0 of warp 1 issues the
+// tile's MMAs when the slot is full and commits them to "empty"; warps 2..5
+// sum the bias gradient (the output gradient over the tile's R centre rows)
+// from the staged planes and arrive on "empty".  CTAs are persistent and
+// keep their accumulators in TMEM over all their tiles; one partial sum per
+// CTA, read out of TMEM by warps 2..5 at the end.  Every wait is bounded.
 constexpr int kWgrad3Smem = 225 * 1024;
+constexpr int kXPx = kPx + 2;                 // staged input pixels per row
+constexpr int kXPlane = kXPx * 16;
 
 // shared memory past the last stage: discarded A rows (M groups past the
-// layer's 3 x chunks) read up to 16 planes past a row, then the barriers
-__host__ __device__ inline size_t wgrad3_tail(int tw) { return (size_t)16 * tw * 16 + 2048; }
+// layer's chunks) read up to 16 planes past a row, then the barriers
+constexpr size_t kWgrad3Tail = (size_t)16 * kXPlane + 2048;
 
 __host__ __device__ inline size_t align1k(size_t n) { return (n + 1023) & ~(size_t)1023; }
 
 struct Wgrad3Plan {
-    int TW, R, S;   // tile width (pixels), input rows per tile, ring slots
+    int R, S;   // input rows per tile, ring slots
     size_t zbytes, xbytes, stage, smem;
 };
 
-// Tiles 256 pixels wide where three ring slots fit (half the bulk copies
-// per pixel: each row-plane copy is 4 KB), else 128.
+__host__ __device__ inline Wgrad3Plan wgrad3_stage(int xc, int zc, int R)
+{
+    Wgrad3Plan p{};
+    p.R = R;
+    p.zbytes = (size_t)(R + 2) * zc * kZPlane;
+    p.xbytes = (size_t)R * xc * kXPlane;
+    p.stage = align1k(p.zbytes) + align1k(p.xbytes);
+    return p;
+}
+
 inline Wgrad3Plan wgrad3_plan(int xc0, int xc1, int zc)
 {
     Wgrad3Plan p{};
-    for (int tw = 256; tw >= 128; tw >>= 1) {
-        const size_t tail = wgrad3_tail(tw);
-        for (int R = 8; R >= 1; R >>= 1) {
-            p.TW = tw;
-            p.R = R;
-            p.zbytes = (size_t)(R + 2) * zc * tw * 16;
-            p.xbytes = (size_t)R * 3 * (xc0 + xc1) * tw * 16;
-            p.stage = align1k(p.zbytes) + align1k(p.xbytes);
-            const int S = (int)((kWgrad3Smem - tail) / p.stage);
-            p.S = S > 6 ? 6 : S;
-            p.smem = p.S * p.stage + tail;
-            if (p.S >= (tw == 256 ? 3 : 4)) return p;
-        }
+    for (int R = 8; R >= 1; R >>= 1) {
+        p = wgrad3_stage(xc0 + xc1, zc, R);
+        const int S = (int)((kWgrad3Smem - kWgrad3Tail) / p.stage);
+        p.S = S > 6 ? 6 : S;
+        p.smem = p.S * p.stage + kWgrad3Tail;
+        if (p.S >= 4) break;
     }
-    return p;   // 128-pixel tiles, one row: S may be below 4
+    return p;
 }
 
 __host__ __device__ inline int pow2_cols(int n)
@@ -479,23 +485,22 @@ __host__ __device__ inline int pow2_cols(int n)
     return c;
 }
 
-template <int ZC, int TW>
+template <int ZC>
 __global__ void __launch_bounds__(kWgradThreads, 1)
     wgrad3_kernel(const WgradParams P, int R, int S, int stage_bytes, int ntx, int nty, int ntiles)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     constexpr int N = (24 * ZC + 15) & ~15;
-    constexpr int kTP = TW * 16;   // bytes per staged plane
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int xc0 = P.xc0, xc1 = P.xc1, xc = xc0 + xc1;
-    const bool split = 3 * xc > 16;   // one MMA (accumulator) per source
-    const uint32_t cols = (uint32_t)pow2_cols(split ? 2 * N : N);
-    const uint32_t zbytes = (uint32_t)((R + 2) * ZC * kTP), xbytes = (uint32_t)(R * 3 * xc * kTP);
-    const uint32_t xoff = (zbytes + 1023u) & ~1023u;
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)S * stage_bytes + 16 * kTP);
+    const uint32_t cols = (uint32_t)pow2_cols(3 * N);
+    const Wgrad3Plan pl = wgrad3_stage(xc, ZC, R);
+    const uint32_t zbytes = (uint32_t)pl.zbytes, xbytes = (uint32_t)pl.xbytes;
+    const uint32_t xoff = (uint32_t)align1k(pl.zbytes);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)S * stage_bytes + 16 * kXPlane);
     uint64_t *empty = full + S;
     uint32_t *tslot = reinterpret_cast<uint32_t *>(empty + S);
-    float *red = reinterpret_cast<float *>(smem + (size_t)S * stage_bytes + 16 * kTP + 1024);   // [4][8 * ZC]
+    float *red = reinterpret_cast<float *>(smem + (size_t)S * stage_bytes + 16 * kXPlane + 1024);   // [4][8 * ZC]
 
     if (warp == 1) tc::tmem_alloc(tslot, cols);
     if (tid == 0) {
@@ -520,7 +525,7 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
 
     if (warp == 0) {
         // ---- producer: all lanes issue the planes of a stage ----
-        const int nz = (R + 2) * ZC, nplanes = nz + R * 3 * xc;
+        const int nz = (R + 2) * ZC, nplanes = nz + R * xc;
         int i = 0;
         for (; i < ntile; ++i) {
             const int s = i % S, tile = first + i * stride;
@@ -533,7 +538,7 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
                 }
             }
             const int tx = tile % ntx, ty = (tile / ntx) % nty, b = tile / (ntx * nty);
-            const int x0 = tx * TW, y0 = ty * R;
+            const int x0 = tx * kPx, y0 = ty * R;
             uint8_t *st = smem + (size_t)s * stage_bytes;
             if (lane == 0) tc::mbar_expect_tx(&full[s], zbytes + xbytes);
             __syncwarp();   // the transaction count is raised before any copy lands
@@ -543,15 +548,15 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
                     const int r = q / ZC, c = q - r * ZC, gy = y0 - 1 + r;
                     const __nv_bfloat16 *row =
                         gy >= 0 && gy < P.H ? P.dz + act_idx(b, gy, c, 0, P.H, P.W, ZC) * 8 : nullptr;
-                    stage_plane(st + (size_t)q * kTP, row, x0, TW, P.W, &full[s]);
+                    stage_plane(st + (size_t)q * kZPlane, row, x0, kPx, P.W, &full[s]);
                 } else {
-                    // input row r, planes [kx][chunk] of source 0 then of source 1
-                    const int u = q - nz, r = u / (3 * xc), v = u - r * 3 * xc, gy = y0 + r;
-                    const bool s1 = v >= 3 * xc0;
-                    const int xs = s1 ? xc1 : xc0, w = s1 ? v - 3 * xc0 : v, kx = w / xs, c = w - kx * xs;
+                    // input row r, chunk c (source 0, then source 1): pixels x0 - 1 .. x0 + 128
+                    const int u = q - nz, r = u / xc, c = u - r * xc, gy = y0 + r;
+                    const bool s1 = c >= xc0;
+                    const int xs = s1 ? xc1 : xc0, cs = s1 ? c - xc0 : c;
                     const __nv_bfloat16 *row =
-                        gy < P.H ? (s1 ? P.x1 : P.x0) + act_idx(b, gy, c, 0, P.H, P.W, xs) * 8 : nullptr;
-                    stage_plane(st + xoff + (size_t)u * kTP, row, x0 - 1 + kx, TW, P.W, &full[s]);
+                        gy < P.H ? (s1 ? P.x1 : P.x0) + act_idx(b, gy, cs, 0, P.H, P.W, xs) * 8 : nullptr;
+                    stage_plane(st + xoff + (size_t)u * kXPlane, row, x0 - 1, kXPx, P.W, &full[s]);
                 }
             }
         }
@@ -572,19 +577,18 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
                 }
                 tc::fence_after_sync();
                 const uint32_t sb = tc::smem_u32(smem + (size_t)s * stage_bytes);
-                // descriptors of row 0, pixel group 0; rows and groups at
-                // constant strides (start field in 16-byte units)
-                const uint64_t bd0 = tc::sdesc(sb, 128, kTP), ad0 = tc::sdesc(sb + xoff, 128, kTP);
-                const uint64_t ad1 = ad0 + ((uint64_t)(3 * xc0 * kTP) >> 4);
+                // descriptors of row 0, pixel group 0; rows, groups and taps
+                // at constant strides (start field in 16-byte units)
+                const uint64_t bd0 = tc::sdesc(sb, 128, kZPlane), ad0 = tc::sdesc(sb + xoff, 128, kXPlane);
                 for (int r = 0; r < R; ++r) {
-                    const uint64_t br = bd0 + ((uint64_t)(r * ZC * kTP) >> 4);
-                    const uint64_t ar = (uint64_t)(r * 3 * xc * kTP) >> 4;
+                    const uint64_t br = bd0 + ((uint64_t)(r * ZC * kZPlane) >> 4);
+                    const uint64_t ar = ad0 + ((uint64_t)(r * xc * kXPlane) >> 4);
 #pragma unroll
-                    for (int g = 0; g < TW / 16; ++g) {
+                    for (int g = 0; g < kPx / 16; ++g) {
                         const uint32_t acc = (i | r | g) ? 1u : 0u;
-                        const uint64_t gg = (uint64_t)(256 * g) >> 4;
-                        tc::mma_bf16(tbase, ad0 + ar + gg, br + gg, idesc, acc);
-                        if (split) tc::mma_bf16(tbase + N, ad1 + ar + gg, br + gg, idesc, acc);
+                        const uint64_t bg = br + ((uint64_t)(256 * g) >> 4), ag = ar + ((uint64_t)(256 * g) >> 4);
+#pragma unroll
+                        for (int kx = 0; kx < 3; ++kx) tc::mma_bf16(tbase + kx * N, ag + kx, bg, idesc, acc);
                     }
                 }
                 tc::commit(&empty[s]);
@@ -595,7 +599,7 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
         ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
     } else {
         // ---- bias warps: the tile's centre gradient rows (staged rows 1..R) ----
-        const int px0 = tid - 64;   // pixels px0, px0 + 128, ...
+        const int px = tid - 64;
         for (int i = 0; i < ntile; ++i) {
             const int s = i % S;
             bool got = true;
@@ -607,10 +611,8 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
             const uint8_t *st = smem + (size_t)s * stage_bytes;
             for (int r = 1; r <= R; ++r)
 #pragma unroll
-                for (int c = 0; c < ZC; ++c)
-#pragma unroll
-                for (int px = px0; px < TW; px += 128) {
-                    const uint4 raw = *reinterpret_cast<const uint4 *>(st + (size_t)(r * ZC + c) * kTP + 16 * px);
+                for (int c = 0; c < ZC; ++c) {
+                    const uint4 raw = *reinterpret_cast<const uint4 *>(st + (size_t)(r * ZC + c) * kZPlane + 16 * px);
                     const __nv_bfloat162 *h2 = reinterpret_cast<const __nv_bfloat162 *>(&raw);
 #pragma unroll
                     for (int e = 0; e < 4; ++e) {
@@ -645,53 +647,28 @@ __global__ void __launch_bounds__(kWgradThreads, 1)
             for (int w = 0; w < kWgradBiasWarps; ++w) v += red[w * 8 * ZC + lane];
             out[9 * P.cin * P.cout + lane] = v;
         }
-        // TMEM lane m = row (group m / 8: source, kx, chunk; channel m % 8)
-        const int q = warp & 3, m = q * 32 + lane, grp = m >> 3, e = m & 7;
-        for (int a = 0; a < (split ? 2 : 1); ++a) {
-            int kx = 3, ci = P.cin;   // invalid unless decoded below
-            if (split) {
-                const int xs = a ? xc1 : xc0;
-                if (grp < 3 * xs) {
-                    kx = grp / xs;
-                    ci = (a ? 8 * xc0 : 0) + 8 * (grp - kx * xs) + e;
-                }
-            } else if (grp < 3 * xc0) {
-                kx = grp / xc0;
-                ci = 8 * (grp - kx * xc0) + e;
-            } else if (grp < 3 * xc) {
-                const int g1 = grp - 3 * xc0;
-                kx = g1 / xc1;
-                ci = 8 * xc0 + 8 * (g1 - kx * xc1) + e;
-            }
-            const bool valid = kx < 3 && ci < P.cin;
+        // TMEM lane m = input channel (chunks of source 0, then of source 1,
+        // 8 channels each; the concatenation's channel index)
+        const int q = warp & 3, m = q * 32 + lane;
+        const bool valid = m < 8 * xc && m < P.cin;
+#pragma unroll
+        for (int kx = 0; kx < 3; ++kx)
 #pragma unroll
             for (int j = 0; j < N; j += 16) {
                 float v[16];
-                tc::tmem_ld16(tbase + ((uint32_t)(q * 32) << 16) + a * N + j, v);
+                tc::tmem_ld16(tbase + ((uint32_t)(q * 32) << 16) + kx * N + j, v);
                 if (valid) {
 #pragma unroll
                     for (int qq = 0; qq < 16; ++qq) {
                         const int n = j + qq, kyp = n / (8 * ZC), co = n - kyp * 8 * ZC;
-                        if (kyp < 3 && co < P.cout) out[(((2 - kyp) * 3 + kx) * P.cin + ci) * P.cout + co] = v[qq];
+                        if (kyp < 3 && co < P.cout) out[(((2 - kyp) * 3 + kx) * P.cin + m) * P.cout + co] = v[qq];
                     }
                 }
             }
-        }
     }
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 1) tc::tmem_dealloc(tbase, cols);
-}
-
-template <int ZC, int TW>
-cudaError_t launch_wgrad3_tw(const WgradParams &P, const Wgrad3Plan &p, int B, int grid, cudaStream_t st)
-{
-    cudaError_t e = cudaFuncSetAttribute(wgrad3_kernel<ZC, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)p.smem);
-    if (e != cudaSuccess) return e;
-    const int ntx = (P.W + TW - 1) / TW, nty = (P.H + p.R - 1) / p.R;
-    wgrad3_kernel<ZC, TW><<<grid, kWgradThreads, p.smem, st>>>(P, p.R, p.S, (int)p.stage, ntx, nty, B * ntx * nty);
-    return cudaGetLastError();
 }
 
 template <int ZC>
@@ -699,7 +676,11 @@ cudaError_t launch_wgrad3_t(const WgradParams &P, int B, int grid, cudaStream_t 
 {
     const Wgrad3Plan p = wgrad3_plan(P.xc0, P.xc1, ZC);
     if (p.S < 2) return cudaErrorInvalidValue;
-    return p.TW == 256 ? launch_wgrad3_tw<ZC, 256>(P, p, B, grid, st) : launch_wgrad3_tw<ZC, 128>(P, p, B, grid, st);
+    cudaError_t e = cudaFuncSetAttribute(wgrad3_kernel<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+    if (e != cudaSuccess) return e;
+    const int ntx = (P.W + kPx - 1) / kPx, nty = (P.H + p.R - 1) / p.R;
+    wgrad3_kernel<ZC><<<grid, kWgradThreads, p.smem, st>>>(P, p.R, p.S, (int)p.stage, ntx, nty, B * ntx * nty);
+    return cudaGetLastError();
 }
 
 }  // namespace
@@ -785,13 +766,11 @@ static int sm_count()
 }
 
 // The persistent kernel takes every layer whose (ky, cout) fit N
-// (zc <= 4) and whose (kx, cin) groups fit M per source.
+// (zc <= 4) and whose input channels fit M (at most 16 chunks).
 static bool wgrad3_fits(const WgradParams &P)
 {
-    // M: 3 x chunks of one MMA within 16 groups (per source when split)
     const int xc = P.xc0 + P.xc1;
-    const bool fits_m = 3 * xc <= 16 || (3 * P.xc0 <= 16 && 3 * P.xc1 <= 16);
-    return P.zc >= 1 && P.zc <= 4 && fits_m && wgrad3_plan(P.xc0, P.xc1, P.zc).S >= 2;
+    return P.zc >= 1 && P.zc <= 4 && xc >= 1 && xc <= 16 && wgrad3_plan(P.xc0, P.xc1, P.zc).S >= 2;
 }
 
 // Partial-sum rows the weight gradient of this layer writes: one per CTA of
@@ -800,7 +779,7 @@ int wgrad_partial_rows(const WgradParams &P, int B)
 {
     if (!wgrad3_fits(P)) return (int)wgrad_tiles(B, P.H, P.W);
     const Wgrad3Plan p = wgrad3_plan(P.xc0, P.xc1, P.zc);
-    const int tiles = B * ((P.W + p.TW - 1) / p.TW) * ((P.H + p.R - 1) / p.R);
+    const int tiles = B * ((P.W + kPx - 1) / kPx) * ((P.H + p.R - 1) / p.R);
     return tiles < sm_count() ? tiles : sm_count();
 }
 
