@@ -23,9 +23,88 @@ constexpr int kBeta = kP * 3;    // floats per centre and buffer
 // Variance: var = |mean of the in-bounds 3x3 neighbours minus the centre -
 // centre|^2 summed over channels (ops/regression.cu.cc:244-276).  Also
 // writes sqrt(var) to a workspace plane: the regression and reconstruction
-// read the standard deviation of every tap.  blockIdx.z = 2 * batch + buffer.
+// read the standard deviation of every tap.
+//
+// variance_kernel: one thread per pixel computes both buffers from the
+// block's footprint in shared memory (rows of 40 pixels from x0 - 4, as
+// stored: 3 floats per pixel), each row copied by one warp with one float4
+// per lane.  Needs W % 4 == 0 and 16-byte aligned images, so that every
+// float4 lies wholly inside or wholly outside an image row.
+// variance_px_kernel (any W): one thread per pixel and buffer, global loads.
+// blockIdx.z = 2 * batch + buffer there.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) variance_kernel(const float *__restrict__ imga,
+constexpr int kVX = 32, kVY = 8;
+constexpr int kVRow = 3 * (kVX + 8), kVTH = kVY + 2;   // footprint row: 40 pixels x 3 floats
+
+__global__ void __launch_bounds__(kVX * kVY) variance_kernel(const float *__restrict__ imga,
+                                                             const float *__restrict__ imgb,
+                                                             float *__restrict__ vara,
+                                                             float *__restrict__ varb,
+                                                             float *__restrict__ sda,
+                                                             float *__restrict__ sdb, int H, int W)
+{
+    __shared__ __align__(16) float tile[2][kVTH][kVRow];
+    const int x0 = blockIdx.x * kVX, y0 = blockIdx.y * kVY, xa = x0 - 4;
+    const size_t base = (size_t)blockIdx.z * H * W;
+    const int lane = threadIdx.x, warp = threadIdx.y;
+    constexpr int kRows = 2 * kVTH, kIt = (kRows + kVY - 1) / kVY;
+    float4 v[kIt];
+    // every load issued before the first store
+#pragma unroll
+    for (int k = 0; k < kIt; ++k) {
+        const int rr = warp + k * kVY, buf = rr >= kVTH, ty = rr - buf * kVTH, gy = y0 - 1 + ty;
+        const int f = 3 * xa + 4 * lane;   // float offset in the image row
+        v[k] = make_float4(0.f, 0.f, 0.f, 0.f);   // outside the image: never read
+        if (rr < kRows && 4 * lane < kVRow && gy >= 0 && gy < H && f >= 0 && f + 4 <= 3 * W)
+            v[k] = __ldg(reinterpret_cast<const float4 *>((buf ? imgb : imga) + 3 * (base + (size_t)gy * W) + f));
+    }
+#pragma unroll
+    for (int k = 0; k < kIt; ++k) {
+        const int rr = warp + k * kVY, buf = rr >= kVTH, ty = rr - buf * kVTH;
+        if (rr < kRows && 4 * lane < kVRow) *reinterpret_cast<float4 *>(&tile[buf][ty][4 * lane]) = v[k];
+    }
+    __syncthreads();
+    const int cx = x0 + lane, cy = y0 + warp;
+    if (cx >= W || cy >= H) return;
+    const size_t p = base + (size_t)cy * W + cx;
+#pragma unroll
+    for (int buf = 0; buf < 2; ++buf) {
+        float ax = 0.f, ay = 0.f, az = 0.f;
+        int n = 0;
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx) {
+                if (dy == 0 && dx == 0) continue;
+                const int ix = cx + dx, iy = cy + dy;
+                if (ix < 0 || ix >= W || iy < 0 || iy >= H) continue;
+                const float *t = &tile[buf][warp + 1 + dy][3 * (lane + 4 + dx)];
+                ax += t[0];
+                ay += t[1];
+                az += t[2];
+                ++n;
+            }
+        const float *t = &tile[buf][warp + 1][3 * (lane + 4)];
+        float mx, my, mz;
+        if (n == 8) {
+            // interior pixels: a quotient by 8 is the product by 1/8, exactly
+            // (__fmul_rn: rounded on its own, never fused into the subtraction)
+            mx = __fmul_rn(ax, 0.125f);
+            my = __fmul_rn(ay, 0.125f);
+            mz = __fmul_rn(az, 0.125f);
+        } else {
+            const float fn = (float)n;
+            mx = ax / fn;
+            my = ay / fn;
+            mz = az / fn;
+        }
+        const float var = norm2(mx - t[0], my - t[1], mz - t[2]);
+        (buf ? varb : vara)[p] = var;
+        (buf ? sdb : sda)[p] = sqrtf(var);
+    }
+}
+
+__global__ void __launch_bounds__(256) variance_px_kernel(const float *__restrict__ imga,
                                                        const float *__restrict__ imgb,
                                                        float *__restrict__ vara,
                                                        float *__restrict__ varb,
@@ -605,9 +684,15 @@ __global__ void __launch_bounds__(kRX * kRY) recon_kernel(
 cudaError_t launch_variance(const float *imga, const float *imgb, float *vara, float *varb, float *sda,
                             float *sdb, int B, int H, int W, cudaStream_t st)
 {
-    dim3 block(32, 8);
-    dim3 grid((W + 31) / 32, (H + 7) / 8, 2 * B);
-    variance_kernel<<<grid, block, 0, st>>>(imga, imgb, vara, varb, sda, sdb, H, W);
+    dim3 block(kVX, kVY);
+    const bool vec = W % 4 == 0 && ((reinterpret_cast<uintptr_t>(imga) | reinterpret_cast<uintptr_t>(imgb)) & 15) == 0;
+    if (vec) {
+        dim3 grid((W + kVX - 1) / kVX, (H + kVY - 1) / kVY, B);
+        variance_kernel<<<grid, block, 0, st>>>(imga, imgb, vara, varb, sda, sdb, H, W);
+    } else {
+        dim3 grid((W + kVX - 1) / kVX, (H + kVY - 1) / kVY, 2 * B);
+        variance_px_kernel<<<grid, block, 0, st>>>(imga, imgb, vara, varb, sda, sdb, H, W);
+    }
     return cudaGetLastError();
 }
 

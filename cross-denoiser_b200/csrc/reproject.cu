@@ -60,9 +60,12 @@ __global__ void __launch_bounds__(256) reproject_kernel(
     unsigned vmask = 0u, box = 0u;
     int lx = 0, ly = 0, ipx = 0, ipy = 0;
 
-    if (__ldg(opac + c) != 0.f) {
-        const float mx = __ldg(mvec + 3 * c), my = __ldg(mvec + 3 * c + 1);
-        const float fwN = __ldg(pnfw + 3 * c + 1);
+    // own-pixel inputs loaded together, not behind the opacity test
+    const float op = __ldg(opac + c), mx = __ldg(mvec + 3 * c), my = __ldg(mvec + 3 * c + 1);
+    const float fwN = __ldg(pnfw + 3 * c + 1);
+    const float Z = __ldg(linz + 3 * c), fwZ = __ldg(linz + 3 * c + 1);
+    const float3 n = ld3(nrm, c);
+    if (op != 0.f) {
         const float fW = (float)W, fH = (float)H, fx = (float)cx, fy = (float)cy;
         // iposPrev = int(pos + mvec * dim + 0.5)   (line 97)
         ipx = __float2int_rz(__fadd_rn(__fmaf_rn(mx, fW, fx), 0.5f));
@@ -73,19 +76,25 @@ __global__ void __launch_bounds__(256) reproject_kernel(
         lx = __float2int_rz(ppx);
         ly = __float2int_rz(ppy);
         const bool border_ok = !(ipx < 1 || ipy < 1 || ipx > W - 1 || ipy > H - 1);
-        const float Z = __ldg(linz + 3 * c), fwZ = __ldg(linz + 3 * c + 1);
-        const float3 n = ld3(nrm, c);
 
         if (border_ok) {
+            // the four taps' previous opacity, depth and normal, all loads
+            // issued before the first test
+            float po[4], zp[4];
+            float3 np[4];
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
                 const int qx = lx + (s & 1), qy = ly + (s >> 1);
+                po[s] = 0.f;
                 if (qx >= W || qx < 0 || qy >= H || qy < 0) continue;
                 const size_t q = base + (size_t)qy * W + qx;
-                if (__ldg(popac + q) == 0.f) continue;
-                if (depth_normal_ok(Z, __ldg(plinz + 3 * q), fwZ, n, ld3(pnrm, q), fwN))
-                    vmask |= 1u << s;
+                po[s] = __ldg(popac + q);
+                zp[s] = __ldg(plinz + 3 * q);
+                np[s] = ld3(pnrm, q);
             }
+#pragma unroll
+            for (int s = 0; s < 4; ++s)
+                if (po[s] != 0.f && depth_normal_ok(Z, zp[s], fwZ, n, np[s], fwN)) vmask |= 1u << s;
         }
         if (vmask) {
             // bilinear weights from the fractional part (line 130-137)

@@ -25,10 +25,13 @@ constexpr int kTX = 32, kTY = 16;
 constexpr float kBig = 10000000.f;
 constexpr int kVals = 9;   // current1.xyz, current2.xyz, (current1+current2)/2 .xyz
 
-__host__ __device__ inline size_t ts_smem(int hc)
+// tile planes (6 x tw x th floats), row-pass planes (2 x kVals x th x kTX
+// floats) and the raw mask footprint ((kTX + 2 + 2hp) x (kTY + 2 + 2hp) bytes)
+__host__ __device__ inline size_t ts_smem(int hc, int hp)
 {
     const int tw = kTX + 2 * hc, th = kTY + 2 * hc;
-    return ((size_t)6 * tw * th + (size_t)2 * kVals * th * kTX) * sizeof(float);
+    return ((size_t)6 * tw * th + (size_t)2 * kVals * th * kTX) * sizeof(float) +
+           (size_t)(kTX + 2 + 2 * hp) * (kTY + 2 + 2 * hp);
 }
 
 // min over the in-bounds 3x3 window of the byte mask, as 0.f / 1.f
@@ -84,20 +87,21 @@ __global__ void __launch_bounds__(kTX * kTY, 2) temporal_kernel(
     out2 += 3 * px * b;
     succ += px * b;
 
+    uint8_t *smask = reinterpret_cast<uint8_t *>(rmax + kVals * rplane);
     const int tid = threadIdx.y * kTX + threadIdx.x;
     const int x0 = blockIdx.x * kTX - hc, y0 = blockIdx.y * kTY - hc;
     const float qnan = __int_as_float(0x7fffffff);
-    // The pixel's history and mask do not depend on the tile: issue their
-    // loads first so their latency overlaps the staging and the row pass.
+    // The pixel's history does not depend on the tile: issue its loads first
+    // so their latency overlaps the staging and the row pass.
     const int cx = blockIdx.x * kTX + threadIdx.x, cy = blockIdx.y * kTY + threadIdx.y;
     const bool inside = cx < W && cy < H;
     const size_t p = inside ? (size_t)cy * W + cx : 0;
     const float3 h0 = ld3(prev, p), h1 = ld3(prev1, p), h2 = ld3(prev2, p);
-    const float m = inside ? (kFused ? eroded_at(raw, cx, cy, H, W) : __ldg(rs + p)) : 0.f;
+    // current-frame footprint, as planes
     for (int t = tid; t < tplane; t += kTX * kTY) {
         const int ty = t / tw, tx = t - ty * tw;
         const int gx = x0 + tx, gy = y0 + ty;
-        float3 a = make_float3(qnan, qnan, qnan), c = a;
+        float3 a = make_float3(qnan, qnan, qnan), c = a;   // outside the image: skipped by fminf / fmaxf
         if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
             a = ld3(cur1, (size_t)gy * W + gx);
             c = ld3(cur2, (size_t)gy * W + gx);
@@ -109,7 +113,25 @@ __global__ void __launch_bounds__(kTX * kTY, 2) temporal_kernel(
         tile[4 * tplane + t] = c.y;
         tile[5 * tplane + t] = c.z;
     }
+    // raw mask footprint for the erosion of every pixel within hp of the
+    // tile; outside the image 1, which the min ignores
+    const int mw = kTX + 2 + 2 * hp, mh = kTY + 2 + 2 * hp;
+    const int mx0 = blockIdx.x * kTX - 1 - hp, my0 = blockIdx.y * kTY - 1 - hp;
+    if (kFused) {
+        for (int i = tid; i < mw * mh; i += kTX * kTY) {
+            const int r = i / mw, q = i - r * mw, gx = mx0 + q, gy = my0 + r;
+            smask[i] = gx >= 0 && gx < W && gy >= 0 && gy < H ? (__ldg(raw + (size_t)gy * W + gx) ? 1 : 0) : 1;
+        }
+    }
     __syncthreads();
+    // eroded mask at image pixel (x, y), |x - cx| <= hp, |y - cy| <= hp
+    auto eroded_s = [&](int x, int y) {
+        const uint8_t *r0 = smask + (y - my0 - 1) * mw + (x - mx0 - 1);
+        const uint8_t v = r0[0] & r0[1] & r0[2] & r0[mw] & r0[mw + 1] & r0[mw + 2] & r0[2 * mw] & r0[2 * mw + 1] &
+                          r0[2 * mw + 2];
+        return v ? 1.f : 0.f;
+    };
+    const float m = inside ? (kFused ? eroded_s(cx, cy) : __ldg(rs + p)) : 0.f;
     // row pass: min/max along x over 2*hc+1 tile columns
     for (int t = tid; t < rplane; t += kTX * kTY) {
         const int r = t / kTX, x = t - r * kTX;
@@ -180,7 +202,7 @@ __global__ void __launch_bounds__(kTX * kTY, 2) temporal_kernel(
             if (ix < 0 || ix >= W || iy < 0 || iy >= H) continue;
             const size_t q = (size_t)iy * W + ix;
             const bool centre = ix == cx && iy == cy;
-            const float mq = centre ? m : (kFused ? eroded_at(raw, ix, iy, H, W) : __ldg(rs + q));
+            const float mq = centre ? m : (kFused ? eroded_s(ix, iy) : __ldg(rs + q));
             if (mq < 1.f) continue;
             const float3 v0 = centre ? h0 : ld3(prev, q), v1 = centre ? h1 : ld3(prev1, q);
             const float3 v2 = centre ? h2 : ld3(prev2, q);
@@ -224,7 +246,7 @@ cudaError_t launch_temporal(const float *c1, const float *c2, const float *prev,
                             int win_prev, cudaStream_t st)
 {
     const int hc = win_curr / 2, hp = win_prev / 2;
-    const size_t smem = ts_smem(hc);
+    const size_t smem = ts_smem(hc, hp);
     if (smem > 220 * 1024) return cudaErrorInvalidConfiguration;
     dim3 block(kTX, kTY);
     dim3 grid((W + kTX - 1) / kTX, (H + kTY - 1) / kTY, B);
