@@ -20,58 +20,20 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
+#include "f32x2.cuh"
 
 namespace cd {
 namespace fsw {
 
-typedef unsigned long long f2;   // two floats: low half = buffer A, high half = buffer B
-
-CD_DEV f2 pack(float lo, float hi)
-{
-    f2 r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
-}
-CD_DEV float lo(f2 v)
-{
-    float a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
-    (void)b;
-    return a;
-}
-CD_DEV float hi(f2 v)
-{
-    float a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
-    (void)a;
-    return b;
-}
-CD_DEV f2 fma2(f2 a, f2 b, f2 c)
-{
-    f2 d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-CD_DEV f2 mul2(f2 a, f2 b)
-{
-    f2 d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-CD_DEV f2 add2(f2 a, f2 b)
-{
-    f2 d;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-CD_DEV f2 sub2(f2 a, f2 b)
-{
-    f2 d;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-// |v|^2 of three pairs as the scalar norm2 rounds it: fma(z, z, fma(x, x, y*y))
-CD_DEV f2 sqnorm2(f2 x, f2 y, f2 z) { return fma2(z, z, fma2(x, x, mul2(y, y))); }
+using x2::f2;   // two floats: low half = buffer A, high half = buffer B
+using x2::pack;
+using x2::lo;
+using x2::hi;
+using x2::fma2;
+using x2::mul2;
+using x2::add2;
+using x2::sub2;
+using x2::sqnorm2;
 
 constexpr int kBX = 32, kBY = 8;
 

@@ -12,6 +12,7 @@
 // and ch = 0..2 the colour channel; 18 floats per centre and buffer.
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
+#include "f32x2.cuh"
 
 namespace cd {
 namespace {
@@ -517,19 +518,83 @@ __global__ void __launch_bounds__(kThreads, 8) regression_kernel(
 // the regression's normal equations, nothing downstream amplifies their
 // last-bit differences.
 // ---------------------------------------------------------------------------
-constexpr int kRX = 32, kRY = 4;
-constexpr int kRec = 13;   // float4 per staged centre
+constexpr int kRX = 32, kRY = 4, kRR = 1;   // threads in x, y; output rows per thread (1 or 2)
+static_assert(kRR == 1 || kRR == 2, "the reconstruction loop pairs at most two rows");
+constexpr int kRec = 13;                     // float4 per staged centre
 
 __host__ __device__ inline int floordiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
 __host__ __device__ inline size_t recon_smem(int hw, int sp, int rs)
 {
     const int cxmax = ((kRX - 1) * rs + 2 * hw) / sp + 2;
-    const int cymax = ((kRY - 1) * rs + 2 * hw) / sp + 2;
+    const int cymax = ((kRY * kRR - 1) * rs + 2 * hw) / sp + 2;
     return (size_t)kRec * cxmax * cymax * sizeof(float4);
 }
 
-CD_DEV float4 ld4f(const float *p) { return make_float4(__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3)); }
+
+// Block reconstruction.  Buffers A and B share every centre and pixel pair,
+// so their arithmetic runs as packed FP32x2 pairs (low lane A, high lane B;
+// same operation order and per-lane rounding as the scalar formulation of
+// ops/regression.cu.cc:465-500).  Staged record of a centre, 13 x 16 bytes
+// (pairs (A, B) unless noted):
+//   0..8   coefficients j = r * 3 + ch, two per record: (A_j, B_j, A_j+1, B_j+1)
+//   9      (feature.x, feature.y)      10  (feature.z, variance)
+//   11     (sd, albedo.x albedo.y)     12  albedo.z normal.xyz (scalars)
+// One output pixel of the reconstruction: its features as (A, B) pairs,
+// albedo / normal, and the running sums.
+struct RPix {
+    x2::f2 f_x, f_y, f_z, var, sd;
+    float3 al, nr;
+    x2::f2 o0, o1, o2, sw;
+};
+// A staged centre record (layout below), records 0..11 as pairs and 12 as
+// scalars.
+struct RRec {
+    ulonglong2 c[12];
+    float4 l12;
+};
+
+// Contribution of one centre to one pixel, both buffers
+// (ops/regression.cu.cc:465-500, same operation order as the scalar form).
+CD_DEV void recon_pair(const RRec &C, RPix &P)
+{
+    using namespace x2;
+    const ulonglong2 F9 = C.c[9], F10 = C.c[10], F11 = C.c[11];
+    const float4 L12 = C.l12;
+    const float da0 = P.al.x - lo(F11.y), da1 = P.al.y - hi(F11.y), da2 = P.al.z - L12.x;
+    const float dn0 = P.nr.x - L12.y, dn1 = P.nr.y - L12.z, dn2 = P.nr.z - L12.w;
+    const f2 d0 = sub2(P.f_x, F9.x), d1 = sub2(P.f_y, F9.y), d2 = sub2(P.f_z, F10.x);
+    const f2 den_r = add2(add2(P.sd, F11.x), pack(1e-2f, 1e-2f));
+    const f2 rden = pack(__fdividef(1.f, lo(den_r)), __fdividef(1.f, hi(den_r)));
+    const f2 den_w = add2(add2(P.var, F10.y), pack(1e-4f, 1e-4f));
+    const f2 q = mul2(sqnorm2(d0, d1, d2), pack(__fdividef(1.f, lo(den_w)), __fdividef(1.f, hi(den_w))));
+    const f2 w = add2(pack(__expf(-lo(q)), __expf(-hi(q))), pack(1e-7f, 1e-7f));
+    // coefficient j = r * 3 + ch sits in record j / 2, half j % 2:
+    // r 0: c0.x c0.y c1.x | r 1: c1.y c2.x c2.y | r 2: c3.x c3.y c4.x
+    // r 3: c4.y c5.x c5.y | r 4: c6.x c6.y c7.x | r 5: c7.y c8.x c8.y
+    const ulonglong2 *c = C.c;
+    f2 p0 = c[0].x, p1 = c[0].y, p2 = c[1].x;
+    p0 = fma2(c[1].y, mul2(d0, rden), p0);
+    p1 = fma2(c[2].x, mul2(d1, rden), p1);
+    p2 = fma2(c[2].y, mul2(d2, rden), p2);
+    p0 = fma2(c[3].x, pack(da0, da0), p0);
+    p1 = fma2(c[3].y, pack(da1, da1), p1);
+    p2 = fma2(c[4].x, pack(da2, da2), p2);
+    const f2 n0 = pack(dn0, dn0), n1 = pack(dn1, dn1), n2 = pack(dn2, dn2);
+    p0 = fma2(c[4].y, n0, p0);
+    p1 = fma2(c[5].x, n0, p1);
+    p2 = fma2(c[5].y, n0, p2);
+    p0 = fma2(c[6].x, n1, p0);
+    p1 = fma2(c[6].y, n1, p1);
+    p2 = fma2(c[7].x, n1, p2);
+    p0 = fma2(c[7].y, n2, p0);
+    p1 = fma2(c[8].x, n2, p1);
+    p2 = fma2(c[8].y, n2, p2);
+    P.o0 = fma2(w, p0, P.o0);
+    P.o1 = fma2(w, p1, P.o1);
+    P.o2 = fma2(w, p2, P.o2);
+    P.sw = add2(P.sw, w);
+}
 
 __global__ void __launch_bounds__(kRX * kRY) recon_kernel(
     const float *__restrict__ imga, const float *__restrict__ imgb,
@@ -539,6 +604,7 @@ __global__ void __launch_bounds__(kRX * kRY) recon_kernel(
     const float *__restrict__ beta, float *__restrict__ outa, float *__restrict__ outb,
     int H, int W, int hw, int sp, int rs)
 {
+    using namespace x2;
     extern __shared__ float4 rec[];
     const int Wr = W / rs, Hr = H / rs;
     const int Ws = W / sp, Hs = H / sp;
@@ -558,8 +624,8 @@ __global__ void __launch_bounds__(kRX * kRY) recon_kernel(
 
     // centres any pixel of this tile can reach (a superset of every
     // per-pixel range below)
-    const int ox0 = blockIdx.x * kRX, oy0 = blockIdx.y * kRY;
-    const int ox1 = min(ox0 + kRX - 1, Wr - 1), oy1 = min(oy0 + kRY - 1, Hr - 1);
+    const int ox0 = blockIdx.x * kRX, oy0 = blockIdx.y * (kRY * kRR);
+    const int ox1 = min(ox0 + kRX - 1, Wr - 1), oy1 = min(oy0 + kRY * kRR - 1, Hr - 1);
     const int cx_lo = max(0, floordiv(ox0 * rs - hw, sp));
     const int cx_hi = min(Ws - 1, (ox1 * rs + hw) / sp);
     const int cy_lo = max(0, floordiv(oy0 * rs - hw, sp));
@@ -571,112 +637,72 @@ __global__ void __launch_bounds__(kRX * kRY) recon_kernel(
     for (int e = tid; e < nc * 9; e += kRX * kRY) {
         const int n = e / 9, f = e - 9 * n;
         const int iy = cy_lo + n / ncx, ix = cx_lo + n % ncx;
-        const size_t cb = ((size_t)iy * Ws + ix) * kBeta;
-        float4 v;
-        if (f < 4)
-            v = ld4f(betaA + cb + 4 * f);
-        else if (f == 4)
-            v = make_float4(__ldg(betaA + cb + 16), __ldg(betaA + cb + 17), __ldg(betaB + cb), __ldg(betaB + cb + 1));
-        else
-            v = ld4f(betaB + cb + 2 + 4 * (f - 5));
-        rec[n * kRec + f] = v;
+        const size_t cb = ((size_t)iy * Ws + ix) * kBeta + 2 * f;
+        rec[n * kRec + f] = make_float4(__ldg(betaA + cb), __ldg(betaB + cb), __ldg(betaA + cb + 1), __ldg(betaB + cb + 1));
     }
     for (int n = tid; n < nc; n += kRX * kRY) {
         const int iy = cy_lo + n / ncx, ix = cx_lo + n % ncx;
         const size_t t = (size_t)(iy * sp) * W + ix * sp;
         const float3 fa = ld3(imga, t), fb = ld3(imgb, t), al = ld3(albedo, t), nr = ld3(normal, t);
-        rec[n * kRec + 9] = make_float4(fa.x, fa.y, fa.z, __ldg(vara + t));
-        rec[n * kRec + 10] = make_float4(fb.x, fb.y, fb.z, __ldg(varb + t));
-        rec[n * kRec + 11] = make_float4(al.x, al.y, al.z, __ldg(sda + t));
-        rec[n * kRec + 12] = make_float4(nr.x, nr.y, nr.z, __ldg(sdb + t));
+        rec[n * kRec + 9] = make_float4(fa.x, fb.x, fa.y, fb.y);
+        rec[n * kRec + 10] = make_float4(fa.z, fb.z, __ldg(vara + t), __ldg(varb + t));
+        rec[n * kRec + 11] = make_float4(__ldg(sda + t), __ldg(sdb + t), al.x, al.y);
+        rec[n * kRec + 12] = make_float4(al.z, nr.x, nr.y, nr.z);
     }
     __syncthreads();
 
-    const int cx = ox0 + threadIdx.x, cy = oy0 + threadIdx.y;
-    if (cx >= Wr || cy >= Hr) return;
-    const int pxo = cx * rs, pyo = cy * rs;
-    const size_t p = (size_t)pyo * W + pxo;
+    // each thread: kRR output rows from cy0 of column cx (with kRR = 2 both
+    // rows read every staged record once; measured slower on sm_100a than
+    // one row per thread, whose lower register count keeps more warps per SM)
+    const int cx = ox0 + threadIdx.x, cy0 = oy0 + threadIdx.y * kRR;
+    if (cx >= Wr || cy0 >= Hr) return;
+    const bool two = kRR > 1 && cy0 + 1 < Hr;
+    const int pxo = cx * rs;
     const int sx = max(0, idivup(pxo - hw, sp));
     const int ex = min((W - 1) / sp, (pxo + hw) / sp);
-    const int sy = max(0, idivup(pyo - hw, sp));
-    const int ey = min((H - 1) / sp, (pyo + hw) / sp);
-
-    const float3 fa = ld3(imga, p), fb = ld3(imgb, p), al = ld3(albedo, p), nr = ld3(normal, p);
-    const float va = __ldg(vara + p), vb = __ldg(varb + p);
-    const float sa = __ldg(sda + p), sb = __ldg(sdb + p);
-    float oa0 = 0.f, oa1 = 0.f, oa2 = 0.f, ob0 = 0.f, ob1 = 0.f, ob2 = 0.f;
-    float swa = 0.f, swb = 0.f;
-    for (int iy = sy; iy <= ey; ++iy) {
+    RPix P[kRR];
+    int sy[kRR], ey[kRR];
+#pragma unroll
+    for (int r = 0; r < kRR; ++r) {
+        const int pyo = (two || r == 0 ? cy0 + r : cy0) * rs;
+        sy[r] = max(0, idivup(pyo - hw, sp));
+        ey[r] = min((H - 1) / sp, (pyo + hw) / sp);
+        const size_t p = (size_t)pyo * W + pxo;
+        const float3 fa = ld3(imga, p), fb = ld3(imgb, p);
+        P[r].al = ld3(albedo, p);
+        P[r].nr = ld3(normal, p);
+        P[r].f_x = pack(fa.x, fb.x);
+        P[r].f_y = pack(fa.y, fb.y);
+        P[r].f_z = pack(fa.z, fb.z);
+        P[r].var = pack(__ldg(vara + p), __ldg(varb + p));
+        P[r].sd = pack(__ldg(sda + p), __ldg(sdb + p));
+        P[r].o0 = P[r].o1 = P[r].o2 = P[r].sw = 0ull;   // +0.0f in both lanes
+    }
+    // the union of both rows' centre rows (the first centre row is not
+    // monotonic in y near the top edge: idivup truncates toward zero)
+    const int yfirst = two ? min(sy[0], sy[kRR - 1]) : sy[0], ylast = two ? max(ey[0], ey[kRR - 1]) : ey[0];
+    for (int iy = yfirst; iy <= ylast; ++iy) {
+        // uniform across the warp
+        const bool u0 = iy >= sy[0] && iy <= ey[0], u1 = two && iy >= sy[kRR - 1] && iy <= ey[kRR - 1];
         const int nrow = (iy - cy_lo) * ncx - cx_lo;
         for (int ix = sx; ix <= ex; ++ix) {
-            const float4 *R = rec + (nrow + ix) * kRec;
-            const float4 A9 = R[9], B10 = R[10], L11 = R[11], N12 = R[12];
-            const float da0 = al.x - L11.x, da1 = al.y - L11.y, da2 = al.z - L11.z;
-            const float dn0 = nr.x - N12.x, dn1 = nr.y - N12.y, dn2 = nr.z - N12.z;
-            // buffer A: features imga, coefficients records 0..4.x
-            {
-                const float d0 = fa.x - A9.x, d1 = fa.y - A9.y, d2 = fa.z - A9.z;
-                const float rden = __fdividef(1.f, (sa + L11.w) + 1e-2f);
-                const float w = __expf(-(sqnorm(d0, d1, d2) * __fdividef(1.f, (va + A9.w) + 1e-4f))) + 1e-7f;
-                const float4 c0 = R[0], c1 = R[1], c2 = R[2], c3 = R[3], c4 = R[4];
-                // beta layout r * 3 + k: c0 = (b0x b0y b0z b1x) c1 = (b1y b1z b2x b2y)
-                // c2 = (b2z b3x b3y b3z) c3 = (b4x b4y b4z b5x) c4 = (b5y b5z | B b0x b0y)
-                float p0 = c0.x, p1 = c0.y, p2 = c0.z;
-                p0 = fmaf(c0.w, d0 * rden, p0);
-                p1 = fmaf(c1.x, d1 * rden, p1);
-                p2 = fmaf(c1.y, d2 * rden, p2);
-                p0 = fmaf(c1.z, da0, p0);
-                p1 = fmaf(c1.w, da1, p1);
-                p2 = fmaf(c2.x, da2, p2);
-                p0 = fmaf(c2.y, dn0, p0);
-                p1 = fmaf(c2.z, dn0, p1);
-                p2 = fmaf(c2.w, dn0, p2);
-                p0 = fmaf(c3.x, dn1, p0);
-                p1 = fmaf(c3.y, dn1, p1);
-                p2 = fmaf(c3.z, dn1, p2);
-                p0 = fmaf(c3.w, dn2, p0);
-                p1 = fmaf(c4.x, dn2, p1);
-                p2 = fmaf(c4.y, dn2, p2);
-                oa0 = fmaf(w, p0, oa0);
-                oa1 = fmaf(w, p1, oa1);
-                oa2 = fmaf(w, p2, oa2);
-                swa += w;
-            }
-            // buffer B: features imgb, coefficients records 4.zw..8
-            {
-                const float d0 = fb.x - B10.x, d1 = fb.y - B10.y, d2 = fb.z - B10.z;
-                const float rden = __fdividef(1.f, (sb + N12.w) + 1e-2f);
-                const float w = __expf(-(sqnorm(d0, d1, d2) * __fdividef(1.f, (vb + B10.w) + 1e-4f))) + 1e-7f;
-                const float4 c4 = R[4], c5 = R[5], c6 = R[6], c7 = R[7], c8 = R[8];
-                // c4.zw = (b0x b0y) c5 = (b0z b1x b1y b1z) c6 = (b2x b2y b2z b3x)
-                // c7 = (b3y b3z b4x b4y) c8 = (b4z b5x b5y b5z)
-                float p0 = c4.z, p1 = c4.w, p2 = c5.x;
-                p0 = fmaf(c5.y, d0 * rden, p0);
-                p1 = fmaf(c5.z, d1 * rden, p1);
-                p2 = fmaf(c5.w, d2 * rden, p2);
-                p0 = fmaf(c6.x, da0, p0);
-                p1 = fmaf(c6.y, da1, p1);
-                p2 = fmaf(c6.z, da2, p2);
-                p0 = fmaf(c6.w, dn0, p0);
-                p1 = fmaf(c7.x, dn0, p1);
-                p2 = fmaf(c7.y, dn0, p2);
-                p0 = fmaf(c7.z, dn1, p0);
-                p1 = fmaf(c7.w, dn1, p1);
-                p2 = fmaf(c8.x, dn1, p2);
-                p0 = fmaf(c8.y, dn2, p0);
-                p1 = fmaf(c8.z, dn2, p1);
-                p2 = fmaf(c8.w, dn2, p2);
-                ob0 = fmaf(w, p0, ob0);
-                ob1 = fmaf(w, p1, ob1);
-                ob2 = fmaf(w, p2, ob2);
-                swb += w;
-            }
+            const ulonglong2 *R = reinterpret_cast<const ulonglong2 *>(rec + (nrow + ix) * kRec);
+            RRec C;
+#pragma unroll
+            for (int j = 0; j < 12; ++j) C.c[j] = R[j];
+            C.l12 = rec[(nrow + ix) * kRec + 12];
+            if (u0) recon_pair(C, P[0]);
+            if (u1) recon_pair(C, P[kRR - 1]);
         }
     }
-    const float dA = fmaxf(swa, 1e-7f), dB = fmaxf(swb, 1e-7f);
-    const size_t o = (size_t)b * Hr * Wr + (size_t)cy * Wr + cx;
-    st3(outa, o, make_float3(fmaxf(0.f, oa0 / dA), fmaxf(0.f, oa1 / dA), fmaxf(0.f, oa2 / dA)));
-    st3(outb, o, make_float3(fmaxf(0.f, ob0 / dB), fmaxf(0.f, ob1 / dB), fmaxf(0.f, ob2 / dB)));
+#pragma unroll
+    for (int r = 0; r < kRR; ++r) {
+        if (r > 0 && !two) break;
+        const float dA = fmaxf(lo(P[r].sw), 1e-7f), dB = fmaxf(hi(P[r].sw), 1e-7f);
+        const size_t o = (size_t)b * Hr * Wr + (size_t)(cy0 + r) * Wr + cx;
+        st3(outa, o, make_float3(fmaxf(0.f, lo(P[r].o0) / dA), fmaxf(0.f, lo(P[r].o1) / dA), fmaxf(0.f, lo(P[r].o2) / dA)));
+        st3(outb, o, make_float3(fmaxf(0.f, hi(P[r].o0) / dB), fmaxf(0.f, hi(P[r].o1) / dB), fmaxf(0.f, hi(P[r].o2) / dB)));
+    }
 }
 
 }  // namespace
@@ -729,7 +755,7 @@ cudaError_t launch_recon(const float *imga, const float *imgb, const float *albe
     if (e != cudaSuccess) return e;
     const int Wr = W / rs, Hr = H / rs;
     dim3 block(kRX, kRY);
-    dim3 grid((Wr + kRX - 1) / kRX, (Hr + kRY - 1) / kRY, B);
+    dim3 grid((Wr + kRX - 1) / kRX, (Hr + kRY * kRR - 1) / (kRY * kRR), B);
     recon_kernel<<<grid, block, smem, st>>>(imga, imgb, albedo, normal, vara, varb, sda, sdb, beta, outa,
                                             outb, H, W, hw, sp, rs);
     return cudaGetLastError();

@@ -11,7 +11,7 @@
 // +-1e7 sentinel (ops/temporal.cu.cc:29).
 //
 // The current window is evaluated separably: a row pass over a shared-memory
-// tile (32x16 pixels plus the radius) takes the min/max along x, a column pass
+// tile (32x8 pixels plus the radius) takes the min/max along x, a column pass
 // along y.  Out-of-image taps are stored as NaN, which fminf/fmaxf skip, so
 // the result equals the reference's in-bounds loop.  The accept/reject
 // decisions are exact: they involve only additions, halvings and compares.
@@ -21,7 +21,7 @@
 namespace cd {
 namespace {
 
-constexpr int kTX = 32, kTY = 16;
+constexpr int kTX = 32, kTY = 8;
 constexpr float kBig = 10000000.f;
 constexpr int kVals = 9;   // current1.xyz, current2.xyz, (current1+current2)/2 .xyz
 
@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(256) erode_kernel(const uint8_t *__restrict__ 
 }
 
 template <bool kFused>
-__global__ void __launch_bounds__(kTX * kTY, 2) temporal_kernel(
+__global__ void __launch_bounds__(kTX * kTY, 3) temporal_kernel(
     const float *__restrict__ cur1, const float *__restrict__ cur2,
     const float *__restrict__ prev, const float *__restrict__ prev1,
     const float *__restrict__ prev2, const float *__restrict__ rs,
