@@ -508,92 +508,30 @@ __global__ void __launch_bounds__(kThreads, 8) regression_kernel(
 // ---------------------------------------------------------------------------
 // Block reconstruction (ops/regression.cu.cc:289-365).  A CTA owns 32x4
 // output pixels.  The centres their windows reach are staged in shared
-// memory as 13 float4 records each:
-//   [0..8]  beta of buffers A and B (18 + 18 floats: coefficient-major)
-//   [9]  (imga.xyz, varA)  [10] (imgb.xyz, varB)
-//   [11] (albedo.xyz, sdA) [12] (normal.xyz, sdB)
-// Each thread sums, over the centres of its own window (the reference's
-// clamped iDivUp range, in its order), w * (beta_c . delta(p, c)) with delta
-// taken as (p - c).  The quotients use a reciprocal and a multiply: unlike
-// the regression's normal equations, nothing downstream amplifies their
-// last-bit differences.
+// memory as 13 float4 records each.  Each thread sums, over the centres of
+// its own window (the reference's clamped iDivUp range, in its order),
+// w * (beta_c . delta(p, c)) with delta taken as (p - c).  The quotients use
+// a reciprocal and a multiply: unlike the regression's normal equations,
+// nothing downstream amplifies their last-bit differences.
+//
+// Buffers A and B share every centre and pixel pair, so their arithmetic
+// runs as packed FP32x2 pairs (low lane A, high lane B; same operation
+// order and per-lane rounding as the scalar formulation, ops/regression.cu.cc
+// :465-500).  Record of a centre (pairs (A, B) unless noted):
+//   0..8   coefficients j = r * 3 + ch, two per record: (A_j, B_j, A_j+1, B_j+1)
+//   9      (feature.x, feature.y)      10  (feature.z, variance)
+//   11     (sd, albedo.x albedo.y)     12  albedo.z normal.xyz (scalars)
 // ---------------------------------------------------------------------------
-constexpr int kRX = 32, kRY = 4, kRR = 1;   // threads in x, y; output rows per thread (1 or 2)
-static_assert(kRR == 1 || kRR == 2, "the reconstruction loop pairs at most two rows");
-constexpr int kRec = 13;                     // float4 per staged centre
+constexpr int kRX = 32, kRY = 4;
+constexpr int kRec = 13;   // float4 per staged centre
 
 __host__ __device__ inline int floordiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
 __host__ __device__ inline size_t recon_smem(int hw, int sp, int rs)
 {
     const int cxmax = ((kRX - 1) * rs + 2 * hw) / sp + 2;
-    const int cymax = ((kRY * kRR - 1) * rs + 2 * hw) / sp + 2;
+    const int cymax = ((kRY - 1) * rs + 2 * hw) / sp + 2;
     return (size_t)kRec * cxmax * cymax * sizeof(float4);
-}
-
-
-// Block reconstruction.  Buffers A and B share every centre and pixel pair,
-// so their arithmetic runs as packed FP32x2 pairs (low lane A, high lane B;
-// same operation order and per-lane rounding as the scalar formulation of
-// ops/regression.cu.cc:465-500).  Staged record of a centre, 13 x 16 bytes
-// (pairs (A, B) unless noted):
-//   0..8   coefficients j = r * 3 + ch, two per record: (A_j, B_j, A_j+1, B_j+1)
-//   9      (feature.x, feature.y)      10  (feature.z, variance)
-//   11     (sd, albedo.x albedo.y)     12  albedo.z normal.xyz (scalars)
-// One output pixel of the reconstruction: its features as (A, B) pairs,
-// albedo / normal, and the running sums.
-struct RPix {
-    x2::f2 f_x, f_y, f_z, var, sd;
-    float3 al, nr;
-    x2::f2 o0, o1, o2, sw;
-};
-// A staged centre record (layout below), records 0..11 as pairs and 12 as
-// scalars.
-struct RRec {
-    ulonglong2 c[12];
-    float4 l12;
-};
-
-// Contribution of one centre to one pixel, both buffers
-// (ops/regression.cu.cc:465-500, same operation order as the scalar form).
-CD_DEV void recon_pair(const RRec &C, RPix &P)
-{
-    using namespace x2;
-    const ulonglong2 F9 = C.c[9], F10 = C.c[10], F11 = C.c[11];
-    const float4 L12 = C.l12;
-    const float da0 = P.al.x - lo(F11.y), da1 = P.al.y - hi(F11.y), da2 = P.al.z - L12.x;
-    const float dn0 = P.nr.x - L12.y, dn1 = P.nr.y - L12.z, dn2 = P.nr.z - L12.w;
-    const f2 d0 = sub2(P.f_x, F9.x), d1 = sub2(P.f_y, F9.y), d2 = sub2(P.f_z, F10.x);
-    const f2 den_r = add2(add2(P.sd, F11.x), pack(1e-2f, 1e-2f));
-    const f2 rden = pack(__fdividef(1.f, lo(den_r)), __fdividef(1.f, hi(den_r)));
-    const f2 den_w = add2(add2(P.var, F10.y), pack(1e-4f, 1e-4f));
-    const f2 q = mul2(sqnorm2(d0, d1, d2), pack(__fdividef(1.f, lo(den_w)), __fdividef(1.f, hi(den_w))));
-    const f2 w = add2(pack(__expf(-lo(q)), __expf(-hi(q))), pack(1e-7f, 1e-7f));
-    // coefficient j = r * 3 + ch sits in record j / 2, half j % 2:
-    // r 0: c0.x c0.y c1.x | r 1: c1.y c2.x c2.y | r 2: c3.x c3.y c4.x
-    // r 3: c4.y c5.x c5.y | r 4: c6.x c6.y c7.x | r 5: c7.y c8.x c8.y
-    const ulonglong2 *c = C.c;
-    f2 p0 = c[0].x, p1 = c[0].y, p2 = c[1].x;
-    p0 = fma2(c[1].y, mul2(d0, rden), p0);
-    p1 = fma2(c[2].x, mul2(d1, rden), p1);
-    p2 = fma2(c[2].y, mul2(d2, rden), p2);
-    p0 = fma2(c[3].x, pack(da0, da0), p0);
-    p1 = fma2(c[3].y, pack(da1, da1), p1);
-    p2 = fma2(c[4].x, pack(da2, da2), p2);
-    const f2 n0 = pack(dn0, dn0), n1 = pack(dn1, dn1), n2 = pack(dn2, dn2);
-    p0 = fma2(c[4].y, n0, p0);
-    p1 = fma2(c[5].x, n0, p1);
-    p2 = fma2(c[5].y, n0, p2);
-    p0 = fma2(c[6].x, n1, p0);
-    p1 = fma2(c[6].y, n1, p1);
-    p2 = fma2(c[7].x, n1, p2);
-    p0 = fma2(c[7].y, n2, p0);
-    p1 = fma2(c[8].x, n2, p1);
-    p2 = fma2(c[8].y, n2, p2);
-    P.o0 = fma2(w, p0, P.o0);
-    P.o1 = fma2(w, p1, P.o1);
-    P.o2 = fma2(w, p2, P.o2);
-    P.sw = add2(P.sw, w);
 }
 
 __global__ void __launch_bounds__(kRX * kRY) recon_kernel(
@@ -624,8 +562,8 @@ __global__ void __launch_bounds__(kRX * kRY) recon_kernel(
 
     // centres any pixel of this tile can reach (a superset of every
     // per-pixel range below)
-    const int ox0 = blockIdx.x * kRX, oy0 = blockIdx.y * (kRY * kRR);
-    const int ox1 = min(ox0 + kRX - 1, Wr - 1), oy1 = min(oy0 + kRY * kRR - 1, Hr - 1);
+    const int ox0 = blockIdx.x * kRX, oy0 = blockIdx.y * kRY;
+    const int ox1 = min(ox0 + kRX - 1, Wr - 1), oy1 = min(oy0 + kRY - 1, Hr - 1);
     const int cx_lo = max(0, floordiv(ox0 * rs - hw, sp));
     const int cx_hi = min(Ws - 1, (ox1 * rs + hw) / sp);
     const int cy_lo = max(0, floordiv(oy0 * rs - hw, sp));
@@ -651,58 +589,67 @@ __global__ void __launch_bounds__(kRX * kRY) recon_kernel(
     }
     __syncthreads();
 
-    // each thread: kRR output rows from cy0 of column cx (with kRR = 2 both
-    // rows read every staged record once; measured slower on sm_100a than
-    // one row per thread, whose lower register count keeps more warps per SM)
-    const int cx = ox0 + threadIdx.x, cy0 = oy0 + threadIdx.y * kRR;
-    if (cx >= Wr || cy0 >= Hr) return;
-    const bool two = kRR > 1 && cy0 + 1 < Hr;
-    const int pxo = cx * rs;
+    const int cx = ox0 + threadIdx.x, cy = oy0 + threadIdx.y;
+    if (cx >= Wr || cy >= Hr) return;
+    const int pxo = cx * rs, pyo = cy * rs;
+    const size_t p = (size_t)pyo * W + pxo;
     const int sx = max(0, idivup(pxo - hw, sp));
     const int ex = min((W - 1) / sp, (pxo + hw) / sp);
-    RPix P[kRR];
-    int sy[kRR], ey[kRR];
-#pragma unroll
-    for (int r = 0; r < kRR; ++r) {
-        const int pyo = (two || r == 0 ? cy0 + r : cy0) * rs;
-        sy[r] = max(0, idivup(pyo - hw, sp));
-        ey[r] = min((H - 1) / sp, (pyo + hw) / sp);
-        const size_t p = (size_t)pyo * W + pxo;
-        const float3 fa = ld3(imga, p), fb = ld3(imgb, p);
-        P[r].al = ld3(albedo, p);
-        P[r].nr = ld3(normal, p);
-        P[r].f_x = pack(fa.x, fb.x);
-        P[r].f_y = pack(fa.y, fb.y);
-        P[r].f_z = pack(fa.z, fb.z);
-        P[r].var = pack(__ldg(vara + p), __ldg(varb + p));
-        P[r].sd = pack(__ldg(sda + p), __ldg(sdb + p));
-        P[r].o0 = P[r].o1 = P[r].o2 = P[r].sw = 0ull;   // +0.0f in both lanes
-    }
-    // the union of both rows' centre rows (the first centre row is not
-    // monotonic in y near the top edge: idivup truncates toward zero)
-    const int yfirst = two ? min(sy[0], sy[kRR - 1]) : sy[0], ylast = two ? max(ey[0], ey[kRR - 1]) : ey[0];
-    for (int iy = yfirst; iy <= ylast; ++iy) {
-        // uniform across the warp
-        const bool u0 = iy >= sy[0] && iy <= ey[0], u1 = two && iy >= sy[kRR - 1] && iy <= ey[kRR - 1];
+    const int sy = max(0, idivup(pyo - hw, sp));
+    const int ey = min((H - 1) / sp, (pyo + hw) / sp);
+
+    const float3 fa = ld3(imga, p), fb = ld3(imgb, p), al = ld3(albedo, p), nr = ld3(normal, p);
+    const f2 pf_x = pack(fa.x, fb.x), pf_y = pack(fa.y, fb.y), pf_z = pack(fa.z, fb.z);
+    const f2 pvar = pack(__ldg(vara + p), __ldg(varb + p)), psd = pack(__ldg(sda + p), __ldg(sdb + p));
+    const f2 k1e2 = pack(1e-2f, 1e-2f), k1e4 = pack(1e-4f, 1e-4f), k1e7 = pack(1e-7f, 1e-7f);
+    f2 o0 = 0ull, o1 = 0ull, o2 = 0ull, sw = 0ull;   // +0.0f in both lanes
+    for (int iy = sy; iy <= ey; ++iy) {
         const int nrow = (iy - cy_lo) * ncx - cx_lo;
         for (int ix = sx; ix <= ex; ++ix) {
-            const ulonglong2 *R = reinterpret_cast<const ulonglong2 *>(rec + (nrow + ix) * kRec);
-            RRec C;
-#pragma unroll
-            for (int j = 0; j < 12; ++j) C.c[j] = R[j];
-            C.l12 = rec[(nrow + ix) * kRec + 12];
-            if (u0) recon_pair(C, P[0]);
-            if (u1) recon_pair(C, P[kRR - 1]);
+            const float4 *R4 = rec + (nrow + ix) * kRec;
+            const ulonglong2 *R = reinterpret_cast<const ulonglong2 *>(R4);
+            const ulonglong2 F9 = R[9], F10 = R[10], F11 = R[11];
+            const float4 L12 = R4[12];
+            const float da0 = al.x - lo(F11.y), da1 = al.y - hi(F11.y), da2 = al.z - L12.x;
+            const float dn0 = nr.x - L12.y, dn1 = nr.y - L12.z, dn2 = nr.z - L12.w;
+            const f2 d0 = sub2(pf_x, F9.x), d1 = sub2(pf_y, F9.y), d2 = sub2(pf_z, F10.x);
+            const f2 den_r = add2(add2(psd, F11.x), k1e2);
+            const f2 rden = pack(__fdividef(1.f, lo(den_r)), __fdividef(1.f, hi(den_r)));
+            const f2 den_w = add2(add2(pvar, F10.y), k1e4);
+            const f2 q = mul2(sqnorm2(d0, d1, d2), pack(__fdividef(1.f, lo(den_w)), __fdividef(1.f, hi(den_w))));
+            const f2 w = add2(pack(__expf(-lo(q)), __expf(-hi(q))), k1e7);
+            const ulonglong2 c0 = R[0], c1 = R[1], c2 = R[2], c3 = R[3], c4 = R[4], c5 = R[5], c6 = R[6],
+                             c7 = R[7], c8 = R[8];
+            // coefficient j = r * 3 + ch sits in record j / 2, half j % 2:
+            // r 0: c0.x c0.y c1.x | r 1: c1.y c2.x c2.y | r 2: c3.x c3.y c4.x
+            // r 3: c4.y c5.x c5.y | r 4: c6.x c6.y c7.x | r 5: c7.y c8.x c8.y
+            f2 p0 = c0.x, p1 = c0.y, p2 = c1.x;
+            p0 = fma2(c1.y, mul2(d0, rden), p0);
+            p1 = fma2(c2.x, mul2(d1, rden), p1);
+            p2 = fma2(c2.y, mul2(d2, rden), p2);
+            p0 = fma2(c3.x, pack(da0, da0), p0);
+            p1 = fma2(c3.y, pack(da1, da1), p1);
+            p2 = fma2(c4.x, pack(da2, da2), p2);
+            const f2 n0 = pack(dn0, dn0), n1 = pack(dn1, dn1), n2 = pack(dn2, dn2);
+            p0 = fma2(c4.y, n0, p0);
+            p1 = fma2(c5.x, n0, p1);
+            p2 = fma2(c5.y, n0, p2);
+            p0 = fma2(c6.x, n1, p0);
+            p1 = fma2(c6.y, n1, p1);
+            p2 = fma2(c7.x, n1, p2);
+            p0 = fma2(c7.y, n2, p0);
+            p1 = fma2(c8.x, n2, p1);
+            p2 = fma2(c8.y, n2, p2);
+            o0 = fma2(w, p0, o0);
+            o1 = fma2(w, p1, o1);
+            o2 = fma2(w, p2, o2);
+            sw = add2(sw, w);
         }
     }
-#pragma unroll
-    for (int r = 0; r < kRR; ++r) {
-        if (r > 0 && !two) break;
-        const float dA = fmaxf(lo(P[r].sw), 1e-7f), dB = fmaxf(hi(P[r].sw), 1e-7f);
-        const size_t o = (size_t)b * Hr * Wr + (size_t)(cy0 + r) * Wr + cx;
-        st3(outa, o, make_float3(fmaxf(0.f, lo(P[r].o0) / dA), fmaxf(0.f, lo(P[r].o1) / dA), fmaxf(0.f, lo(P[r].o2) / dA)));
-        st3(outb, o, make_float3(fmaxf(0.f, hi(P[r].o0) / dB), fmaxf(0.f, hi(P[r].o1) / dB), fmaxf(0.f, hi(P[r].o2) / dB)));
-    }
+    const float dA = fmaxf(lo(sw), 1e-7f), dB = fmaxf(hi(sw), 1e-7f);
+    const size_t o = (size_t)b * Hr * Wr + (size_t)cy * Wr + cx;
+    st3(outa, o, make_float3(fmaxf(0.f, lo(o0) / dA), fmaxf(0.f, lo(o1) / dA), fmaxf(0.f, lo(o2) / dA)));
+    st3(outb, o, make_float3(fmaxf(0.f, hi(o0) / dB), fmaxf(0.f, hi(o1) / dB), fmaxf(0.f, hi(o2) / dB)));
 }
 
 }  // namespace
@@ -755,7 +702,7 @@ cudaError_t launch_recon(const float *imga, const float *imgb, const float *albe
     if (e != cudaSuccess) return e;
     const int Wr = W / rs, Hr = H / rs;
     dim3 block(kRX, kRY);
-    dim3 grid((Wr + kRX - 1) / kRX, (Hr + kRY * kRR - 1) / (kRY * kRR), B);
+    dim3 grid((Wr + kRX - 1) / kRX, (Hr + kRY - 1) / kRY, B);
     recon_kernel<<<grid, block, smem, st>>>(imga, imgb, albedo, normal, vara, varb, sda, sdb, beta, outa,
                                             outb, H, W, hw, sp, rs);
     return cudaGetLastError();
