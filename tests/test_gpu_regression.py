@@ -45,6 +45,37 @@ def test_vs_oracle(cd, cuda, win, sp, rs):
         assert_close(o[i], r[i], nm, atol=ATOL)
 
 
+def unaligned(x):
+    """x in a contiguous tensor whose data starts 4 bytes past a 16-byte
+    boundary."""
+    t = T(x)
+    buf = torch.empty(t.numel() + 1, dtype=t.dtype, device=t.device)
+    v = buf[1:].view(t.shape)
+    v.copy_(t)
+    return v
+
+
+@pytest.mark.parametrize("H,W,win,sp", [(50, 70, 7, 2), (45, 63, 5, 1), (36, 42, 9, 3)])
+def test_width_not_multiple_of_4(cd, cuda, H, W, win, sp):
+    """Widths with W % 4 != 0 take the per-pixel variance kernel."""
+    y1, y2, alb, nrm = inputs(cd, H, W, seed=H + W)
+    o = run(cd, y1, y2, alb, nrm, win, sp)
+    r = orc.cross_regression(y1, y2, alb, nrm, win, sp, 1)
+    for i, nm in enumerate(("outa", "outb", "vara", "varb")):
+        assert_close(o[i], r[i], f"{nm} {H}x{W}", atol=ATOL)
+
+
+def test_unaligned_images(cd, cuda):
+    """Images not 16-byte aligned take the per-pixel variance kernel and give
+    the same bits as aligned ones."""
+    y1, y2, alb, nrm = inputs(cd, 64, 96, seed=4)
+    o = cd.ops.cross_regression(unaligned(y1), unaligned(y2), T(alb), T(nrm), win_size=11, sparsity=4)
+    torch.cuda.synchronize()
+    r = run(cd, y1, y2, alb, nrm, 11, 4)
+    for x, y, nm in zip(o, r, ("outa", "outb", "vara", "varb")):
+        np.testing.assert_array_equal(N(x), y, err_msg=nm)
+
+
 def test_batches_are_independent(cd, cuda):
     a = inputs(cd, 64, 96, seed=1)
     b = inputs(cd, 64, 96, seed=2)

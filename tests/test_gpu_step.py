@@ -20,6 +20,15 @@ def test_prepare_input(cd, cuda):
     assert_close(N(y2), np.log1p(f["color2"]), "y2", rtol=4e-7, atol=0)
 
 
+@pytest.mark.parametrize("H,W", [(5, 7), (9, 13)])
+def test_prepare_input_odd_sizes(cd, cuda, H, W):
+    """3 x H x W not a multiple of 4: the scalar log1p kernel."""
+    _, f = frames(cd, H, W, seed=2)
+    y1, y2 = cd.ops.prepare_input(T(f["color"]), T(f["color2"]))
+    assert_close(N(y1), np.log1p(f["color"]), "y1", rtol=4e-7, atol=0)
+    assert_close(N(y2), np.log1p(f["color2"]), "y2", rtol=4e-7, atol=0)
+
+
 def agg_inputs(H, W, B, seed, device):
     g = torch.Generator(device="cpu").manual_seed(seed)
     r = lambda c, lo=0.0, hi=1.0: (lo + (hi - lo) * torch.rand((B, H, W, c), generator=g)).to(device)
