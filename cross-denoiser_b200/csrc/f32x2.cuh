@@ -2,8 +2,9 @@
 // instruction for two lanes of fp32 data, each lane rounded as the scalar
 // IEEE instruction, so packed code is bit-identical to scalar code with the
 // same operation order.  The FMA pipe executes a pair in two cycles: the gain
-// is issue bandwidth.  Used for the two regression buffers A and B, which
-// share every tap.
+// is issue bandwidth.  Used for the two buffers A and B of the spatial filter
+// (filter_sweep.cuh) and of the block reconstruction (regression.cu), which
+// share every tap or centre.
 #pragma once
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
