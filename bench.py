@@ -59,8 +59,10 @@ FLOP = {"regression_tap": 150, "recon_pair": 55, "variance_px": 20, "filter_tap"
 # Algorithmic HBM bytes per pixel (each input read once, each output written
 # once): reprojection 153, erosion + temporal screening 104.
 BYTES = {"reproject_px": 153, "temporal_px": 104}
-# DRAM bytes (read + write) per launch at 1920x1080, from one ncu capture of
-# the same workload (profiles/filter_aggregate_1080p_w11.md)
+# DRAM bytes (read + write) per launch of the dominant kernel at 1920x1080,
+# filter window 11: dram__bytes_read.sum + dram__bytes_write.sum of one
+# earlier ncu capture of this workload, not measured by this run (ncu is not
+# available to it); reported as roofline.traffic with that provenance.
 NCU_TRAFFIC = {"filter_aggregate": 328_594_688}
 
 
@@ -80,7 +82,8 @@ def args_parse():
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--serve", action="store_true",
                     help="serving run: 16 mixed-resolution streams (4x720p, 8x1080p, 3x1440p, 1x2160p)")
-    ap.add_argument("--serve-frames", type=int, default=60, help="frames per stream in the serving run")
+    ap.add_argument("--serve-frames", type=int, default=30, help="frames per stream in the serving run")
+    ap.add_argument("--no-serve", action="store_true", help="leave the serving run out of the default line")
     ap.add_argument("--ncu-region", choices=["fused", "full"], default=None,
                     help="bracket the timed steps of the fused ops step or of the full step (with the U-Net) "
                          "with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
@@ -101,39 +104,6 @@ def fixed_prediction(H, W, seed, device):
     band = synth.random_band((1, H, W), g, device=device)
     alpha = torch.sigmoid(torch.randn((1, H, W, 1), generator=g, device=device))
     return band, alpha
-
-
-# ---------------------------------------------------------------------------
-# the reference arm: the same step on the reference's own kernels
-# ---------------------------------------------------------------------------
-class ReferenceStep:
-    def __init__(self, cfg, band, alpha):
-        from oracle import reference as ref
-        self.ref, self.cfg, self.band, self.alpha = ref, cfg, band, alpha
-        self.history = None
-
-    def __call__(self, f):
-        ref, cfg = self.ref, self.cfg
-        B, H, W, _ = f["color"].shape
-        if self.history is None:
-            self.history = stepmod.History.zeros(B, H, W, f["color"].device)
-        h = self.history
-        y1, y2 = torch.log1p(f["color"]), torch.log1p(f["color2"])
-        ols1, ols2, _, _ = ref.cross_regression(y1, y2, f["albedo"], f["normal"], cfg.regression_width,
-                                                cfg.sparsity)
-        ones1 = torch.ones((B, H, W, 1), device=y1.device)
-        succ, rep = ref.reproject(f["mvec"], [h.out_log, h.ols1, h.ols2], f["linearZ"], h.linearZ, f["normal"],
-                                  h.normal, f["pnFwidth"], ones1, ones1)
-        ero = ref.erode3x3(succ)
-        po, p1, p2, sp = ref.temporal_screening(ols1, ols2, rep[0], rep[1], rep[2], ero, cfg.win_curr,
-                                                cfg.win_prev)
-        s1, s2, w1, w2 = ref.spatial_filter(ols1, ols2, f["albedo"], f["normal"], self.band, cfg.filter_width)
-        out_log, out, loss, avg, g1, gw1, g2, gw2, ga = stepmod.aggregation_forward_backward(
-            s1, w1, s2, w2, self.alpha, ero, sp, po, f["opacity"], ols2, ols1, p2, p1)
-        gb = ref.spatial_filter_grad(g1, g2, gw1, gw2, ols1, ols2, f["albedo"], f["normal"], self.band,
-                                     cfg.filter_width)
-        self.history = stepmod.History(out_log, ols1, ols2, f["linearZ"], f["normal"])
-        return {"out": out, "avg_loss": avg, "g_band": gb}
 
 
 # ---------------------------------------------------------------------------
@@ -389,6 +359,7 @@ def cpu_baseline(H, W, win, fwin, seed):
     """The oracle (C, OpenMP over all host threads) on a bounded sample: whole
     1080p frames through the same op sequence, until ~10 s have elapsed."""
     from oracle import oracle as orc
+    from oracle.reference_step import aggregation_forward_backward
     cores = len(os.sched_getaffinity(0))
     frames = make_frames(H, W, 3, seed, "cpu")
     f = [{k: v.numpy() for k, v in fr.items()} for fr in frames]
@@ -408,8 +379,8 @@ def cpu_baseline(H, W, win, fwin, seed):
         po, p1, p2, sp = orc.temporal_screening(o1, o2, rep[0], rep[1], rep[2], ero, 7, 1)
         s1, s2, w1, w2, pa, pb = orc.spatial_filter(o1, o2, fr["albedo"], fr["normal"], band, fwin, partials=True)
         tt = lambda a: torch.from_numpy(a)
-        agg = stepmod.aggregation_forward_backward(tt(s1), tt(w1), tt(s2), tt(w2), tt(alpha), tt(ero), tt(sp),
-                                                   tt(po), tt(fr["opacity"]), tt(o2), tt(o1), tt(p2), tt(p1))
+        agg = aggregation_forward_backward(tt(s1), tt(w1), tt(s2), tt(w2), tt(alpha), tt(ero), tt(sp),
+                                           tt(po), tt(fr["opacity"]), tt(o2), tt(o1), tt(p2), tt(p1))
         orc.spatial_filter_grad_from_partials(*[a.numpy() for a in (agg[4], agg[6], agg[5], agg[7])], pa, pb)
         hist = dict(out_log=agg[0].numpy(), ols1=o1, ols2=o2, linz=fr["linearZ"], nrm=fr["normal"])
         done += 1
@@ -564,10 +535,10 @@ def run_mine(a, rank, world, device):
 
     res["differentiation"] = differentiation_costs(device, stream)
 
-    # regression-width sweep (radius 5 / 7 / 9)
+    # regression-width sweep (radius 5 / 7 / 9, and 8: the reference's default 17)
     if not a.no_sweep:
         res["sweep_frames_per_s"] = {}
-        for win in (11, 15, 19):
+        for win in (11, 15, 17, 19):
             k = max(1, min(a.steps, 50))
             total, _ = timed_steps(stepper(True, win), frames, 2, k, stream)
             res["sweep_frames_per_s"][f"win{win}"] = round(k / (total * 1e-3), 2)
@@ -674,9 +645,12 @@ def run_reference(a, device):
     n = min(a.pool, a.warmup + a.steps)
     frames = make_frames(H, W, n, a.seed, device)
     band, alpha = fixed_prediction(H, W, a.seed, device)
+    from oracle.reference_step import ReferenceStep
     cfg = stepmod.StepConfig(regression_width=a.win, filter_width=a.filter_win)
+    mk = lambda: ReferenceStep(cfg.regression_width, cfg.sparsity, cfg.filter_width, cfg.win_curr, cfg.win_prev,
+                               band, alpha)
     stream = torch.cuda.current_stream()
-    rs = ReferenceStep(cfg, band, alpha)
+    rs = mk()
     with Clocks(device) as clk:
         total, ms = timed_steps(lambda f, t: rs(f), frames, a.warmup, a.steps, stream)
     res = {"value": a.steps / (total * 1e-3), "ms_per_step": total / a.steps, "p50_ms": pct(ms, 50),
@@ -684,7 +658,7 @@ def run_reference(a, device):
     host = [{k: v.cpu().pin_memory() for k, v in frames[i].items()} for i in range(min(4, n))]
     dev_in = [{k: torch.empty_like(v) for k, v in frames[0].items()} for _ in range(2)]
     out_host = torch.empty((1, H, W, 3), dtype=torch.float32).pin_memory()
-    rs2 = ReferenceStep(cfg, band, alpha)
+    rs2 = mk()
 
     def e2e_step(_f, t):
         slot = dev_in[t % 2]
@@ -761,6 +735,14 @@ def main():
                                              device_id=device)
     try:
         r = run_mine(a, rank, world, device)
+        serving = None
+        if world == 1 and not a.no_serve:
+            # the 16-stream serving run (bounded: serve_frames per stream), on
+            # a device emptied of the single-stream runs' buffers
+            import gc
+            gc.collect()
+            torch.cuda.empty_cache()
+            serving = run_serving(a, device)
         cpu = None
         if rank == 0 and world == 1 and not a.no_cpu_baseline:
             cpu = cpu_baseline(a.height, a.width, a.win, a.filter_win, a.seed)
@@ -770,7 +752,7 @@ def main():
                         roofline=r.get("roofline"), roofline_hbm=r.get("roofline_hbm"), cpu_baseline=cpu,
                         clocks=r["clocks"], per_op_ms=r["per_op_ms"],
                         sweep_frames_per_s=r.get("sweep_frames_per_s"), full_step=r.get("full_step"),
-                        differentiation=r.get("differentiation"))
+                        differentiation=r.get("differentiation"), serving=serving)
             print(json.dumps(line))
     finally:
         if world > 1:

@@ -56,6 +56,7 @@ SIGNATURES = {
     "cd_unet_conv3x3_wgrad_workspace_size": (_S, [_I] * 5),
     "cd_unet_conv3x3_wgrad": (_I, [_P] * 3 + [_I] * 5 + [_P, _S, _P]),
     "cd_fp32_fma_probe": (_I, [_P, _I, _I, _P]),
+    "cd_mbar_timeout_probe": (_I, [_P, _I, _I, _P]),
 }
 
 # kernels each entry point launches (for the launch count of bench.py)

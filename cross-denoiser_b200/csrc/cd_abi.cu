@@ -85,6 +85,22 @@ static cd_status check_regression(const char *op, int B, int H, int W, int win_s
     return CD_OK;
 }
 
+}  // extern "C"
+
+namespace cd {
+int check_cross_regression_args(const char *op, const float *imga, const float *imgb, const float *albedo,
+                                const float *normal, const float *outa, const float *outb, const float *vara,
+                                const float *varb, int B, int H, int W, int win_size, int sparsity,
+                                int recon_scale)
+{
+    if (!imga || !imgb || !albedo || !normal || !outa || !outb || !vara || !varb)
+        return fail(CD_EINVAL, "%s: null tensor pointer", op);
+    return check_regression(op, B, H, W, win_size, sparsity, recon_scale);
+}
+}  // namespace cd
+
+extern "C" {
+
 static cd_status cross_regression_impl(const char *op, const float *imga, const float *imgb, const float *albedo,
                                        const float *normal, float *outa, float *outb, float *vara, float *varb,
                                        int B, int H, int W, int win_size, int sparsity, int recon_scale,
@@ -92,9 +108,8 @@ static cd_status cross_regression_impl(const char *op, const float *imga, const 
                                        size_t workspace_bytes, cudaStream_t stream)
 {
     g_err[0] = 0;
-    if (!imga || !imgb || !albedo || !normal || !outa || !outb || !vara || !varb)
-        return fail(CD_EINVAL, "%s: null tensor pointer", op);
-    cd_status s = check_regression(op, B, H, W, win_size, sparsity, recon_scale);
+    cd_status s = static_cast<cd_status>(cd::check_cross_regression_args(
+        op, imga, imgb, albedo, normal, outa, outb, vara, varb, B, H, W, win_size, sparsity, recon_scale));
     if (s != CD_OK) return s;
     const size_t need = cd_cross_regression_workspace_size(B, H, W, sparsity);
     if (workspace_bytes < need || (need > 0 && !workspace))

@@ -101,6 +101,12 @@ cudaError_t launch_temporal(const float *c1, const float *c2, const float *prev,
 
 // Records msg as the calling thread's cd_get_last_error() message.
 void set_last_error(const char *msg);
+// The argument checks of cd_cross_regression (null pointers, shape and
+// attributes); sets the last-error message and returns CD_EINVAL on failure.
+int check_cross_regression_args(const char *op, const float *imga, const float *imgb, const float *albedo,
+                                const float *normal, const float *outa, const float *outb, const float *vara,
+                                const float *varb, int B, int H, int W, int win_size, int sparsity,
+                                int recon_scale);
 
 struct AggArgs {
     const float *s1, *w1, *s2, *w2, *alpha, *succ, *succ_prev, *prev, *opac, *l1, *l2, *pl1, *pl2;

@@ -18,7 +18,10 @@
 //     overlap on the GPU (different streams, or host threads racing) corrupt
 //     each other -- serialise them;
 //   * the first call on each device resolves the array's device address
-//     (cudaGetSymbolAddress); make that first call before any stream capture.
+//     (cudaGetSymbolAddress) and caches it; make that first call before any
+//     stream capture.  The cache is not invalidated by cudaDeviceReset, so a
+//     process that resets a device must not call this entry point on it
+//     afterwards.
 // Nothing in the array has to start at zero: the variance kernel writes
 // every standard deviation and the regression kernel every coefficient
 // before the reconstruction reads them.
@@ -65,12 +68,14 @@ extern "C" cd_status cd_cross_regression_noalloc(const float *imga, const float 
                                                  float *varb, int B, int H, int W, int win_size, int sparsity,
                                                  int recon_scale, cudaStream_t stream)
 {
-    // An invalid shape or sparsity needs no scratch lookup: the regular
-    // entry point reports it.  A valid problem must fit the static array.
+    // Invalid arguments are reported as the regular entry point reports
+    // them (CD_EINVAL), before the size check; a valid problem must then fit
+    // the static array.
+    cd::set_last_error("");
+    const int bad = cd::check_cross_regression_args("cross_regression_noalloc", imga, imgb, albedo, normal, outa,
+                                                    outb, vara, varb, B, H, W, win_size, sparsity, recon_scale);
+    if (bad != CD_OK) return static_cast<cd_status>(bad);
     const size_t need = cd_cross_regression_workspace_size(B, H, W, sparsity);
-    if (need == 0)
-        return cd_cross_regression(imga, imgb, albedo, normal, outa, outb, vara, varb, B, H, W, win_size,
-                                   sparsity, recon_scale, nullptr, 0, stream);
     if (need > kNoAllocBytes) {
         char g_msg[256];
         snprintf(g_msg, sizeof(g_msg),

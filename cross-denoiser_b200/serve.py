@@ -125,10 +125,16 @@ class Session:
                 self._body()
             if self.keep_outputs:
                 self.outputs.append(self.out.clone())
+            self.net.enqueue_error_readback()
             ev = torch.cuda.Event()
             ev.record(self.cuda_stream)
         self.next_frame = frame + 1
         return ev
+
+    def check(self):
+        """Raise if this stream's network reported a tensor-core time-out in
+        a frame whose done event has completed."""
+        self.net.raise_if_failed()
 
     def release(self):
         """Free the device state (outputs kept with keep_outputs survive)."""
@@ -221,6 +227,8 @@ class Server:
             for sid, s in list(self.sessions.items()):
                 if s.inflight is not None and s.inflight[1].query():
                     q, _, start = s.inflight
+                    if hasattr(s, "check"):
+                        s.check()
                     results.append(Result(sid, q.frame, q.arrival if realtime else 0.0, start, now()))
                     s.inflight = None
                     if s.next_frame >= frames_per_stream:

@@ -77,46 +77,6 @@ class History:
         return History(z(), z(), z(), z(), z())
 
 
-def aggregation_forward_backward(sum1, sumw1, sum2, sumw2, alpha, success, success_prev, prev_out,
-                                 opacity, label1, label2, prev_label1, prev_label2):
-    """Eager PyTorch restatement of aggregation_loss (scripts/main.py:214-248)
-    and its gradient with respect to (sum1, sumw1, sum2, sumw2, alpha), in
-    closed form: the FP32 reference the fused CUDA kernels are tested
-    against, and the glue of the baseline arm that drives the reference's
-    kernels.
-
-    Returns (out, out_linear, loss, avg_loss, g_sum1, g_sumw1, g_sum2, g_sumw2, g_alpha).
-    """
-    e = 1e-4
-    d1 = sumw1 + e
-    d2 = sumw2 + e
-    o1s = sum1 / d1
-    o2s = sum2 / d2
-    out = (sum1 + sum2) / (sumw1 + sumw2 + e)
-    op = torch.where(opacity > 0, 1.0, 0.0).to(sum1.dtype)
-    s = success * success_prev
-    a = s * alpha + (1 - s)
-    out = (a * out + (1 - a) * prev_out) * op
-    o1 = a * o1s + (1 - a) * prev_out
-    o2 = a * o2s + (1 - a) * prev_out
-    n1, n2 = label1 * label1 + 1e-2, label2 * label2 + 1e-2
-    p1, p2 = prev_label1 * prev_label1 + 1e-2, prev_label2 * prev_label2 + 1e-2
-    spatial = ((o1 - label1) ** 2 / n1 + (o2 - label2) ** 2 / n2) * 0.5
-    temporal = ((o1 - prev_label1) ** 2 / p1 + (o2 - prev_label2) ** 2 / p2) * 0.5
-    loss = (spatial + temporal) * 0.5 * op
-    avg = loss.mean()
-    c = 0.5 * 0.5 * op / loss.numel()
-    g_o1 = c * (2 * (o1 - label1) / n1 + 2 * (o1 - prev_label1) / p1)
-    g_o2 = c * (2 * (o2 - label2) / n2 + 2 * (o2 - prev_label2) / p2)
-    g_sum1 = g_o1 * a / d1
-    g_sum2 = g_o2 * a / d2
-    g_sumw1 = -(g_o1 * a * sum1).sum(-1, keepdim=True) / (d1 * d1)
-    g_sumw2 = -(g_o2 * a * sum2).sum(-1, keepdim=True) / (d2 * d2)
-    g_alpha = (s * (g_o1 * (o1s - prev_out) + g_o2 * (o2s - prev_out))).sum(-1, keepdim=True)
-    return (out, torch.clamp(torch.expm1(out), min=0.0), loss, avg,
-            g_sum1, g_sumw1, g_sum2, g_sumw2, g_alpha)
-
-
 class FrameStep:
     """One stream's per-frame denoise + loss + gradient step."""
 

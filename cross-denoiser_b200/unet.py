@@ -100,6 +100,9 @@ class UNet:
         self.step = torch.zeros((1,), dtype=torch.int32, device=self.device)   # optimizer iterations
         self._shape = None
         self.ws = None
+        # host copy of the workspace's error flag, refreshed asynchronously
+        # after every training update (enqueue_error_readback)
+        self.flag_host = torch.zeros((1,), dtype=torch.int32).pin_memory()
 
     def _workspace(self, B, H, W):
         if self._shape != (B, H, W):
@@ -111,10 +114,33 @@ class UNet:
         return self.ws
 
     def error_flag(self) -> int:
-        """1 if a tensor-core completion wait timed out since the workspace was made."""
+        """The workspace's error flag, read synchronously: 0 while every bounded
+        wait of the tensor-core kernels completed, 1 after a wait for a bulk
+        copy ran out, 2 after a wait for an MMA batch ran out.  Never cleared."""
         return int(self.ws[:4].view(torch.int32).item()) if self.ws is not None else 0
 
+    def enqueue_error_readback(self):
+        """Copy the error flag to pinned host memory on the current stream
+        (no synchronisation); raise_if_failed reads the copy.  Not for use
+        inside a CUDA-graph capture."""
+        if self.ws is not None:
+            self.flag_host.copy_(self.ws[:4].view(torch.int32), non_blocking=True)
+
+    def raise_if_failed(self):
+        """Raise UNetTimeoutError if the last flag copy that has landed is
+        nonzero.  Reads host memory only: an error is seen once the copy
+        enqueued after the failing frame has completed.  After an error the
+        network's outputs and parameters are invalid and later kernels of
+        the process are suspect (a timed-out CTA may have left copies or MMAs
+        writing its shared memory or TMEM)."""
+        f = int(self.flag_host[0])
+        if f:
+            what = "a bulk copy into shared memory" if f == 1 else "an MMA batch"
+            raise UNetTimeoutError(f"unet: a bounded tensor-core wait ran out (flag {f}: {what}); "
+                                   "the network's outputs and parameters are invalid")
+
     def forward(self, ols1, ols2, prev_out, albedo, normal):
+        self.raise_if_failed()
         B, H, W, _ = ols1.shape
         ws = self._workspace(B, H, W)
         ins = [t.contiguous() for t in (ols1, ols2, prev_out, albedo, normal)]
@@ -142,6 +168,12 @@ class UNet:
     def on_gradients(self, g_band, g_alpha):
         self.backward(g_band, g_alpha)
         self.apply_gradients()
+        if not torch.cuda.is_current_stream_capturing():
+            self.enqueue_error_readback()
+
+
+class UNetTimeoutError(RuntimeError):
+    """A bounded wait of the U-Net's tensor-core kernels ran out."""
 
 
 def to_planes(x):

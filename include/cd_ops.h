@@ -143,8 +143,11 @@ CD_API cd_status cd_cross_regression_grad(const float *imga, const float *imgb,
 /* needing more scratch than that (cd_cross_regression_workspace_size) fail  */
 /* with CD_ENOMEM.  All calls share the array: calls whose kernels overlap   */
 /* on the GPU race and must be serialised by the caller.  The first call on  */
-/* a device looks up the array's device address; make it before any stream  */
-/* capture.  Nothing in the array needs to start at zero.                    */
+/* a device looks up the array's device address and caches it; make it     */
+/* before any stream capture.  The cache survives cudaDeviceReset, so do not */
+/* call this entry point on a device after resetting it.  Invalid arguments  */
+/* give CD_EINVAL as in cd_cross_regression, checked before the size.        */
+/* Nothing in the array needs to start at zero.                              */
 /* ------------------------------------------------------------------------ */
 #define CD_NOALLOC_SCRATCH_MIB 40
 
@@ -346,10 +349,14 @@ CD_API cd_status cd_filter_aggregate(const float *ols1, const float *ols2, const
 /*  band : [B,H,W,5] = 1/(p^2 + 1e-4);  alpha : [B,H,W,1] = sigmoid(p)       */
 /* cd_unet_backward needs the workspace of the cd_unet_forward of the same   */
 /* frame and parameters; it writes dL/dparams (same layout) given dL/dband   */
-/* and dL/dalpha.  The first int32 of the workspace is an error flag that a */
-/* kernel sets to 1 when a tensor-core completion wait times out (the        */
-/* caller zeroes the workspace once and may poll it; outputs are then        */
-/* invalid).                                                                  */
+/* and dL/dalpha.  The first int32 of the workspace is an error flag: 0     */
+/* while every bounded wait of the tensor-core kernels completed; nonzero   */
+/* after one ran out (1: a bulk copy into shared memory, 2: an MMA batch).  */
+/* The caller zeroes the workspace once and tests the flag for != 0 (it is  */
+/* never cleared by the library).  Once it is set, the outputs of that call */
+/* and of every later call are invalid, and every later kernel of the       */
+/* process is suspect: the timed-out CTA left while its copies or MMAs      */
+/* could still be writing its shared memory or TMEM.                        */
 /* ------------------------------------------------------------------------ */
 CD_API size_t cd_unet_param_count(void);
 CD_API size_t cd_unet_workspace_size(int B, int H, int W);
@@ -398,6 +405,18 @@ CD_API cd_status cd_unet_conv3x3_wgrad(const void *x, const void *dz, float *gra
 /* the measured FP32 peak that bounds the filter and regression kernels.     */
 /* ------------------------------------------------------------------------ */
 CD_API cd_status cd_fp32_fma_probe(float *out, int blocks, int iters, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Bounded-wait probe (no counterpart in the reference): one warp waits on  */
+/* an mbarrier with the polling loop of the tensor-core kernels, for at     */
+/* most max_iter polls (1 <= max_iter <= CD_MBAR_PROBE_MAX_ITER).  With      */
+/* arrive = 0 nothing arrives, the wait runs out and *flag is set to 1;     */
+/* with arrive = 1 the barrier completes and *flag is left unchanged.  No   */
+/* copy or MMA is in flight, so the time-out leaves nothing behind.  Tests  */
+/* the error path of cd_unet_forward/backward without a faulty kernel.      */
+/* ------------------------------------------------------------------------ */
+#define CD_MBAR_PROBE_MAX_ITER 65536
+CD_API cd_status cd_mbar_timeout_probe(int *flag, int arrive, int max_iter, cudaStream_t stream);
 
 #ifdef __cplusplus
 }

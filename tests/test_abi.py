@@ -58,6 +58,24 @@ def test_invalid_arguments_are_rejected_without_a_device(cd):
     assert lib.cd_cross_regression_workspace_size(2, 64, 32, 4) == (2 * 2 * 16 * 8 * 18 + 2 * 2 * 64 * 32) * 4
 
 
+def test_noalloc_checks_arguments_before_capacity(cd):
+    """The entry point without a workspace reports invalid arguments as the
+    regular entry point does (CD_EINVAL), even for a frame too large for its
+    built-in array; a valid oversized frame is CD_ENOMEM.  Neither touches
+    the device."""
+    lib = cd._lib.lib()
+    p = ctypes.c_void_p(16)
+    st = ctypes.c_void_p(0)
+    H, W = 2160, 3840
+    assert lib.cd_cross_regression_workspace_size(1, H, W, 4) > lib.cd_cross_regression_noalloc_capacity()
+    rc = lib.cd_cross_regression_noalloc(*([p] * 8), 1, H, W, 15, 2, 4, st)     # recon_scale > sparsity
+    assert rc == cd._lib.CD_EINVAL and b"recon_scale" in lib.cd_get_last_error()
+    rc = lib.cd_cross_regression_noalloc(*([p] * 7), None, 1, H, W, 15, 4, 1, st)
+    assert rc == cd._lib.CD_EINVAL and b"null" in lib.cd_get_last_error()
+    rc = lib.cd_cross_regression_noalloc(*([p] * 8), 1, H, W, 15, 4, 1, st)
+    assert rc == cd._lib.CD_ENOMEM and b"built-in array" in lib.cd_get_last_error()
+
+
 def test_ops_refuse_cpu_tensors(cd):
     x = torch.zeros((1, 8, 8, 3))
     with pytest.raises(ValueError, match="CUDA"):

@@ -1,14 +1,16 @@
 """The rest of the frame step on the GPU: input preparation, the aggregation
 loss forward/backward against its eager PyTorch FP32 restatement and FP64,
 the fused filter + loss + gradient kernel against the plain op sequence,
-and whole frames of FrameStep against the CPU oracle."""
+plain against fused frame steps, overlapped training and the host-frame
+pipeline.  Whole sequences against the reference and the oracle are in
+test_gpu_chain.py."""
 import numpy as np
 import pytest
 import torch
 
 from gpu_util import N, T, frames
 from helpers import assert_close, assert_equal
-from oracle import oracle as orc
+from oracle.reference_step import aggregation_forward_backward
 
 pytestmark = pytest.mark.gpu
 
@@ -44,8 +46,8 @@ def agg_inputs(H, W, B, seed, device):
 def test_aggregation_vs_torch_and_fp64(cd, cuda, H, W, B):
     x = agg_inputs(H, W, B, seed=H, device=cuda)
     mine = cd.ops.aggregation_loss(*x)
-    ref32 = cd.step.aggregation_forward_backward(*x)
-    ref64 = cd.step.aggregation_forward_backward(*[t.double() for t in x])
+    ref32 = aggregation_forward_backward(*x)
+    ref64 = aggregation_forward_backward(*[t.double() for t in x])
     names = ("out_log", "out", "loss", "avg_loss", "g_sum1", "g_sumw1", "g_sum2", "g_sumw2", "g_alpha")
     for m, r32, r64, nm in zip(mine, ref32, ref64, names):
         scale = float(r64.abs().max())
@@ -96,41 +98,6 @@ def test_plain_and_fused_steps_agree(cd, cuda):
         for k in ("out_log", "out", "g_band", "g_alpha", "success"):
             assert_equal(N(a[k]), N(b[k]), k)
         assert float(a["avg_loss"]) == float(b["avg_loss"])
-
-
-def test_frames_vs_cpu_oracle(cd, cuda):
-    """Four consecutive frames of the plain step against the same sequence of
-    oracle ops on the CPU.  The reprojection masks match exactly; a value may
-    differ where a near-tie in temporal screening resolves differently after
-    the regression's last-bit differences, so the test bounds that share."""
-    H, W = 96, 128
-    seq = cd.synth.make_sequence(H, W, seed=8, object_motion=2.0)
-    band = cd.synth.random_band((1, H, W), torch.Generator().manual_seed(2))
-    alpha = torch.full((1, H, W, 1), 0.6)
-    st = cd.step.FrameStep(cd.step.StepConfig(regression_width=15))
-    st.set_fixed_prediction(band.to(cuda), alpha.to(cuda))
-    z3 = np.zeros((1, H, W, 3), np.float32)
-    hist = dict(out_log=z3, ols1=z3, ols2=z3, linz=z3, nrm=z3)
-    one = np.ones((1, H, W, 1), np.float32)
-    for t in range(4):
-        fr = {k: v.numpy() for k, v in seq.frame(t).items()}
-        o = st({k: T(v) for k, v in fr.items()})
-        torch.cuda.synchronize()
-        y1, y2 = np.log1p(fr["color"]), np.log1p(fr["color2"])
-        o1, o2, _, _ = orc.cross_regression(y1, y2, fr["albedo"], fr["normal"], 15, 4, 1)
-        s, rep = orc.reproject(fr["mvec"], [hist["out_log"], hist["ols1"], hist["ols2"]], fr["linearZ"],
-                               hist["linz"], fr["normal"], hist["nrm"], fr["pnFwidth"], one, one)
-        assert_equal(N(o["success"]), s, f"frame {t} reprojection mask")
-        ero = orc.erode3x3(s)
-        po, p1, p2, sp = orc.temporal_screening(o1, o2, rep[0], rep[1], rep[2], ero, 7, 1)
-        s1, s2, w1, w2 = orc.spatial_filter(o1, o2, fr["albedo"], fr["normal"], band.numpy(), 11)
-        tt = torch.from_numpy
-        agg = cd.step.aggregation_forward_backward(tt(s1), tt(w1), tt(s2), tt(w2), alpha, tt(ero), tt(sp), tt(po),
-                                                   tt(fr["opacity"]), tt(o2), tt(o1), tt(p2), tt(p1))
-        ol = agg[0].numpy()
-        bad = ~np.isclose(N(o["out_log"]), ol, rtol=1e-4, atol=1e-5)
-        assert bad.mean() < 2e-3, f"frame {t}: {bad.mean():.2e} of values differ"
-        hist = dict(out_log=ol, ols1=o1, ols2=o2, linz=fr["linearZ"], nrm=fr["normal"])
 
 
 def _unet_frames(cd, H, W, seed, n, cuda):

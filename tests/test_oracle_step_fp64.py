@@ -6,6 +6,7 @@ import numpy as np
 import torch
 
 from oracle import step_fp64 as s64
+from oracle.reference_step import aggregation_forward_backward
 
 
 def test_runs_and_learns(cd):
@@ -37,7 +38,7 @@ def test_aggregation_gradient_matches_closed_form(cd):
     _, _, _, avg = s64.aggregation_fp64(sums[0], sums[1], sums[2], sums[3], alpha, succ, succp, prev, op,
                                         l1, l2, p1, p2)
     avg.backward()
-    ref = cd.step.aggregation_forward_backward(s1.detach(), w1.detach(), s2.detach(), w2.detach(), alpha.detach(),
-                                               succ, succp, prev, op, l1, l2, p1, p2)
+    ref = aggregation_forward_backward(s1.detach(), w1.detach(), s2.detach(), w2.detach(), alpha.detach(),
+                                    succ, succp, prev, op, l1, l2, p1, p2)
     for got, want in zip([sums[0].grad, sums[1].grad, sums[2].grad, sums[3].grad, alpha.grad], ref[4:9]):
         torch.testing.assert_close(got, want, rtol=1e-10, atol=1e-14)

@@ -87,3 +87,21 @@ def test_summarize():
     s = serve.summarize(rs, res)
     assert s["frames"] == 3 and abs(s["seconds"] - 0.030) < 1e-9
     assert s["by_resolution"]["4x4"]["frames"] == 2 and s["by_resolution"]["8x8"]["frames"] == 1
+
+
+def test_session_failure_stops_the_loop():
+    """A session whose check() raises (its network reported a time-out) ends
+    the run with that error once its frame completes."""
+    class Boom(RuntimeError):
+        pass
+
+    class Failing(FakeSession):
+        def check(self):
+            if self.next_frame >= 2:
+                raise Boom(f"stream {self.sid}")
+
+    srv = serve.Server([(8, 8)] * 2, lambda sid, t: None, "cpu", hbm_budget=1 << 30, session_factory=Failing,
+                       memory_probe=lambda: 0)
+    import pytest
+    with pytest.raises(Boom):
+        srv.run(serve.poisson_schedule([50.0, 50.0], 4, seed=2), 4, realtime=False)
