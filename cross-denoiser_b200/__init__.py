@@ -10,7 +10,7 @@ The directory name is not a Python identifier; the package is registered as
 bench.py and smoke() do this), or by any importlib loader pointed at this
 directory.
 """
-from . import _lib, ops, replicas, serve, step, synth, unet  # noqa: F401
+from . import _lib, frames, ops, replicas, serve, step, synth, unet  # noqa: F401
 from .ops import (Reproject, cross_regression, erode3x3, erode_temporal_screening,  # noqa: F401
                   reproject, spatial_filter, spatial_filter_grad, temporal_screening)
 

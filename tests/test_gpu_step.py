@@ -160,3 +160,26 @@ def test_host_pipeline_equals_device_step(cd, cuda):
         got[t][2].synchronize()
         assert_equal(got[t][0].numpy(), want[t][0], f"frame {t} out (overlapped)")
         assert float(got[t][1]) == want[t][1]
+
+
+def test_npy_sequence_through_host_pipeline(cd, cuda, tmp_path):
+    """Frames written in the reference's NPY scene layout and read back by
+    frames.NpySequence (pinned, read ahead on a thread) denoise through
+    HostFramePipeline exactly as the same frames resident on the device."""
+    H, W = 64, 96
+    seq = cd.synth.make_sequence(H, W, seed=23, object_motion=2.0)
+    fr = [{k: v for k, v in seq.frame(t).items() if k in cd.frames.STEP_TYPES} for t in range(4)]
+    cd.frames.save_npy_sequence(str(tmp_path), fr)
+    band = cd.synth.random_band((1, H, W), torch.Generator().manual_seed(6)).to(cuda)
+    alpha = torch.full((1, H, W, 1), 0.6, device=cuda)
+    cfg = cd.step.StepConfig(regression_width=9, filter_width=7, fused=True)
+    ref = cd.step.FrameStep(cfg)
+    ref.set_fixed_prediction(band, alpha)
+    want = [N(ref({k: v.to(cuda) for k, v in f.items()})["out"]) for f in fr]
+    st = cd.step.FrameStep(cfg)
+    st.set_fixed_prediction(band, alpha)
+    pipe = cd.step.HostFramePipeline(st, cuda)
+    for t, f in cd.frames.NpySequence(str(tmp_path)).prefetch(depth=2):
+        out, loss, ev = pipe(f)
+        ev.synchronize()
+        assert_equal(out.numpy(), want[t], f"frame {t} out")
