@@ -57,6 +57,9 @@ SIGNATURES = {
     "cd_unet_conv3x3_wgrad": (_I, [_P] * 3 + [_I] * 5 + [_P, _S, _P]),
     "cd_fp32_fma_probe": (_I, [_P, _I, _I, _P]),
     "cd_mbar_timeout_probe": (_I, [_P, _I, _I, _P]),
+    "cd_image_kernel_error_flags": (_I, []),
+    "cd_set_persistent_kernels": (None, [_I]),
+    "cd_set_unet_conv_stacked": (None, [_I]),
 }
 
 # kernels each entry point launches (for the launch count of bench.py)

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
 #include "filter_sweep.cuh"
+#include "tma.cuh"
 
 namespace cd {
 namespace {
@@ -32,41 +33,51 @@ struct AggOut {
     float g_s1[3], g_w1, g_s2[3], g_w2, g_alpha;
 };
 
+// The 41 quotients of a pixel share 15 denominators: each denominator's
+// reciprocal is taken once (__fdividef, about 2 ulp; every denominator is at
+// least 1e-4) and the quotients become products.  The plain aggregation
+// kernel and the fused filter kernel both evaluate this function, so their
+// results stay identical to each other; against the eager FP32 formulas they
+// differ by a few ulp.
 CD_DEV AggOut aggregate(const AggIn &in, float inv_n)
 {
     AggOut r;
     const float d1 = in.w1 + 1e-4f, d2 = in.w2 + 1e-4f, d12 = (in.w1 + in.w2) + 1e-4f;
+    const float r1 = __fdividef(1.f, d1), r2 = __fdividef(1.f, d2), r12 = __fdividef(1.f, d12);
     const float op = in.opac > 0.f ? 1.f : 0.f;
     const float s = in.succ * in.succ_prev;
     const float a = s * in.alpha + (1.f - s);
     const float c = 0.25f * op * inv_n;
+    const float ar1 = a * r1, ar2 = a * r2;
     float ga = 0.f, gw1 = 0.f, gw2 = 0.f, loss = 0.f;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const float o1s = in.s1[k] / d1, o2s = in.s2[k] / d2;
-        const float oall = (in.s1[k] + in.s2[k]) / d12;
+        const float o1s = in.s1[k] * r1, o2s = in.s2[k] * r2;
+        const float oall = (in.s1[k] + in.s2[k]) * r12;
         const float pv = in.prev[k];
         const float ol = (a * oall + (1.f - a) * pv) * op;
         r.out_log[k] = ol;
         r.out[k] = fmaxf(0.f, expm1f(ol));
         const float o1 = a * o1s + (1.f - a) * pv, o2 = a * o2s + (1.f - a) * pv;
-        const float n1 = in.l1[k] * in.l1[k] + 1e-2f, n2 = in.l2[k] * in.l2[k] + 1e-2f;
-        const float p1 = in.pl1[k] * in.pl1[k] + 1e-2f, p2 = in.pl2[k] * in.pl2[k] + 1e-2f;
+        const float rn1 = __fdividef(1.f, in.l1[k] * in.l1[k] + 1e-2f), rn2 = __fdividef(1.f, in.l2[k] * in.l2[k] + 1e-2f);
+        const float rp1 = __fdividef(1.f, in.pl1[k] * in.pl1[k] + 1e-2f);
+        const float rp2 = __fdividef(1.f, in.pl2[k] * in.pl2[k] + 1e-2f);
         const float e1 = o1 - in.l1[k], e2 = o2 - in.l2[k], f1 = o1 - in.pl1[k], f2 = o2 - in.pl2[k];
-        const float spatial = (e1 * e1 / n1 + e2 * e2 / n2) * 0.5f;
-        const float temporal = (f1 * f1 / p1 + f2 * f2 / p2) * 0.5f;
+        const float e1n = e1 * rn1, e2n = e2 * rn2, f1p = f1 * rp1, f2p = f2 * rp2;
+        const float spatial = (e1 * e1n + e2 * e2n) * 0.5f;
+        const float temporal = (f1 * f1p + f2 * f2p) * 0.5f;
         r.loss_ch[k] = (spatial + temporal) * 0.5f * op;
         loss += r.loss_ch[k];
-        const float go1 = c * (2.f * e1 / n1 + 2.f * f1 / p1);
-        const float go2 = c * (2.f * e2 / n2 + 2.f * f2 / p2);
-        r.g_s1[k] = go1 * a / d1;
-        r.g_s2[k] = go2 * a / d2;
+        const float go1 = c * (2.f * e1n + 2.f * f1p);
+        const float go2 = c * (2.f * e2n + 2.f * f2p);
+        r.g_s1[k] = go1 * ar1;
+        r.g_s2[k] = go2 * ar2;
         gw1 += go1 * a * in.s1[k];
         gw2 += go2 * a * in.s2[k];
         ga += go1 * (o1s - pv) + go2 * (o2s - pv);
     }
-    r.g_w1 = -gw1 / (d1 * d1);
-    r.g_w2 = -gw2 / (d2 * d2);
+    r.g_w1 = -gw1 * (r1 * r1);
+    r.g_w2 = -gw2 * (r2 * r2);
     r.g_alpha = s * ga;
     r.loss = loss;
     return r;
@@ -74,7 +85,9 @@ CD_DEV AggOut aggregate(const AggIn &in, float inv_n)
 
 // Block-wide sum of v written to partial[block]; partial sums are reduced
 // in index order by loss_reduce_kernel, so the mean is deterministic.
-CD_DEV void block_partial(float v, float *partial, int nthreads)
+// block_partial_at writes it to partial[index] and ends with a barrier, so
+// a persistent CTA can call it once per tile.
+CD_DEV void block_partial_at(float v, float *partial, int index, int nthreads)
 {
     __shared__ float red[32];
     for (int m = 16; m > 0; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
@@ -84,8 +97,14 @@ CD_DEV void block_partial(float v, float *partial, int nthreads)
     if (tid < 32) {
         float u = tid < (nthreads + 31) / 32 ? red[tid] : 0.f;
         for (int m = 16; m > 0; m >>= 1) u += __shfl_xor_sync(0xffffffffu, u, m);
-        if (tid == 0) partial[(blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = u;
+        if (tid == 0) partial[index] = u;
     }
+    __syncthreads();
+}
+
+CD_DEV void block_partial(float v, float *partial, int nthreads)
+{
+    block_partial_at(v, partial, (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x, nthreads);
 }
 
 __global__ void __launch_bounds__(1024) loss_reduce_kernel(const float *__restrict__ partial, int n,
@@ -187,6 +206,47 @@ __global__ void __launch_bounds__(256) aggregation_kernel(AggPtrs P, int H, int 
     block_partial(loss, P.partial, blockDim.x * blockDim.y);
 }
 
+// Epilogue of the fused filter kernels at pixel p: the aggregation loss and
+// its gradient from the window sums, written outputs, dL/dband from the
+// partials; returns the pixel's loss (sum over its three channels).
+CD_DEV float filter_epilogue(const fsw::Sums &s, const fsw::Centre &c, const AggPtrs &P, size_t p,
+                             float *__restrict__ gband, float inv_n)
+{
+    AggIn in;
+    in.s1[0] = fsw::lo(s.acc_x);
+    in.s1[1] = fsw::lo(s.acc_y);
+    in.s1[2] = fsw::lo(s.acc_z);
+    in.s2[0] = fsw::hi(s.acc_x);
+    in.s2[1] = fsw::hi(s.acc_y);
+    in.s2[2] = fsw::hi(s.acc_z);
+    in.w1 = fsw::lo(s.acc_w);
+    in.w2 = fsw::hi(s.acc_w);
+    // labels crossed as train_step sets them: label1 = ols2, label2 = ols1
+    in.l1[0] = fsw::hi(c.ab_x);
+    in.l1[1] = fsw::hi(c.ab_y);
+    in.l1[2] = fsw::hi(c.ab_z);
+    in.l2[0] = fsw::lo(c.ab_x);
+    in.l2[1] = fsw::lo(c.ab_y);
+    in.l2[2] = fsw::lo(c.ab_z);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        in.prev[k] = __ldg(P.prev + 3 * p + k);
+        in.pl1[k] = __ldg(P.pl1 + 3 * p + k);      // prev_label1 = prev_ols2
+        in.pl2[k] = __ldg(P.pl2 + 3 * p + k);      // prev_label2 = prev_ols1
+    }
+    in.alpha = __ldg(P.alpha + p);
+    in.succ = __ldg(P.succ + p);
+    in.succ_prev = __ldg(P.succ_prev + p);
+    in.opac = __ldg(P.opac + p);
+    const AggOut r = aggregate(in, inv_n);
+    st3(P.out_log, p, make_float3(r.out_log[0], r.out_log[1], r.out_log[2]));
+    st3(P.out, p, make_float3(r.out[0], r.out[1], r.out[2]));
+    P.g_alpha[p] = r.g_alpha;
+    fsw::band_grad(s, make_float3(r.g_s1[0], r.g_s1[1], r.g_s1[2]), make_float3(r.g_s2[0], r.g_s2[1], r.g_s2[2]),
+                   r.g_w1, r.g_w2, gband + 5 * p);
+    return r.loss;
+}
+
 // ---------------------------------------------------------------------------
 // Chosen path: spatial filter + aggregation loss + band gradient in one pass.
 // The window sweep is the forward kernel's (same order, same arithmetic, so
@@ -217,44 +277,167 @@ __global__ void __launch_bounds__(256, 3) filter_aggregate_kernel(
         fsw::Sums s;
         fsw::zero(s);
         fsw::sweep<HW, true, true>(tile, pdtab, hw, c, s);
-        AggIn in;
-        in.s1[0] = fsw::lo(s.acc_x);
-        in.s1[1] = fsw::lo(s.acc_y);
-        in.s1[2] = fsw::lo(s.acc_z);
-        in.s2[0] = fsw::hi(s.acc_x);
-        in.s2[1] = fsw::hi(s.acc_y);
-        in.s2[2] = fsw::hi(s.acc_z);
-        in.w1 = fsw::lo(s.acc_w);
-        in.w2 = fsw::hi(s.acc_w);
-        // labels crossed as train_step sets them: label1 = ols2, label2 = ols1
-        in.l1[0] = fsw::hi(c.ab_x);
-        in.l1[1] = fsw::hi(c.ab_y);
-        in.l1[2] = fsw::hi(c.ab_z);
-        in.l2[0] = fsw::lo(c.ab_x);
-        in.l2[1] = fsw::lo(c.ab_y);
-        in.l2[2] = fsw::lo(c.ab_z);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            in.prev[k] = __ldg(P.prev + 3 * p + k);
-            in.pl1[k] = __ldg(P.pl1 + 3 * p + k);      // prev_label1 = prev_ols2
-            in.pl2[k] = __ldg(P.pl2 + 3 * p + k);      // prev_label2 = prev_ols1
-        }
-        in.alpha = __ldg(P.alpha + p);
-        in.succ = __ldg(P.succ + p);
-        in.succ_prev = __ldg(P.succ_prev + p);
-        in.opac = __ldg(P.opac + p);
-        const AggOut r = aggregate(in, inv_n);
-        st3(P.out_log, p, make_float3(r.out_log[0], r.out_log[1], r.out_log[2]));
-        st3(P.out, p, make_float3(r.out[0], r.out[1], r.out[2]));
-        P.g_alpha[p] = r.g_alpha;
-        loss = r.loss;
-        fsw::band_grad(s, make_float3(r.g_s1[0], r.g_s1[1], r.g_s1[2]), make_float3(r.g_s2[0], r.g_s2[1], r.g_s2[2]),
-                       r.g_w1, r.g_w2, gband + 5 * p);
+        loss = filter_epilogue(s, c, P, p, gband, inv_n);
     }
     block_partial(loss, P.partial, fsw::kBX * fsw::kBY);
 }
 
+
+// ---------------------------------------------------------------------------
+// Chosen path, persistent form: the same per-pixel work as
+// filter_aggregate_kernel (same records, sweep, epilogue and one loss
+// partial per 32x8 tile, so every output is bit-identical to it), with each
+// CTA walking the tiles with stride gridDim.x and the next tile's footprint
+// of the four images (the window's halo included) arriving by TMA while the
+// current tile is swept.  The copies land as raw NHWC rows; a repack pass
+// (shared memory to shared memory) forms the records, taking the reflect-101
+// neighbours from inside the box.  Three CTAs per SM.
+// ---------------------------------------------------------------------------
+template <int HW>
+struct FaGeom {
+    static constexpr int TW = fsw::kBX + 2 * HW, TH = fsw::kBY + 2 * HW;
+    static constexpr int OFF = (4 - (3 * HW) % 4) % 4;          // first float of the footprint in a box row
+    static constexpr int BOXW = (3 * TW + OFF + 3) & ~3;
+    static constexpr int PLANE = ((TH * BOXW * 4 + 127) / 128) * 128;
+    static constexpr int RAW = 4 * PLANE;
+    static constexpr int TX_BYTES = 4 * TH * BOXW * 4;
+    static constexpr int REC = 3 * TW * TH * 16;
+    static constexpr int PD = (2 * HW + 1) * (2 * HW + 1) * 8;
+    static constexpr int SMEM = RAW + REC + PD + 16;
+};
+
+struct FaMaps {
+    CUtensorMap ia, ib, al, nr;
+};
+
+__device__ int g_filter_stage_error = 0;   // sticky: a staging wait ran out
+
+template <int HW>
+__global__ void __launch_bounds__(256, 3) filter_aggregate_tma_kernel(
+    const __grid_constant__ FaMaps maps, const float *__restrict__ band, AggPtrs P, float *__restrict__ gband,
+    int H, int W, int ntx, int nty, int ntiles, float inv_n)
+{
+    using G = FaGeom<HW>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    ulonglong2 *tile = reinterpret_cast<ulonglong2 *>(smem + G::RAW);
+    fsw::f2 *pdtab = reinterpret_cast<fsw::f2 *>(smem + G::RAW + G::REC);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + G::RAW + G::REC + G::PD);
+    const int tid = threadIdx.y * fsw::kBX + threadIdx.x;
+    const int per_img = ntx * nty;
+    const size_t px = (size_t)H * W;
+
+    auto issue = [&](int t) {
+        const int b = t / per_img, r = t - b * per_img, by = r / ntx, bx = r - by * ntx;
+        const int xc = tma::floor_to(3 * (bx * fsw::kBX - HW), 4), yc = by * fsw::kBY - HW;
+        tc::mbar_expect_tx(bar, G::TX_BYTES);
+        tma::load3(smem, &maps.ia, xc, yc, b, bar);
+        tma::load3(smem + G::PLANE, &maps.ib, xc, yc, b, bar);
+        tma::load3(smem + 2 * G::PLANE, &maps.al, xc, yc, b, bar);
+        tma::load3(smem + 3 * G::PLANE, &maps.nr, xc, yc, b, bar);
+    };
+
+    if (tid == 0) tc::mbar_init(bar, 1);
+    {
+        // pd(ky, kx), rounded as fsw::stage rounds it
+        const int w = 2 * HW + 1;
+        for (int k = tid; k < w * w; k += fsw::kBX * fsw::kBY) {
+            const int ky = k / w, kx = k - ky * w;
+            const float dy = (float)(HW - ky) / (float)HW, dx = (float)(HW - kx) / (float)HW;
+            const float pd = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
+            pdtab[k] = fsw::pack(pd, pd);
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x);
+    uint32_t phase = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int b = t / per_img, rr = t - b * per_img, by = rr / ntx, bx = rr - by * ntx;
+        const bool landed = __syncthreads_and(tc::mbar_wait(bar, phase, 1 << 22)) != 0;
+        phase ^= 1u;
+        if (!landed) {
+            if (tid == 0) atomicOr(&g_filter_stage_error, 1);
+            return;
+        }
+        // raw rows -> records (reflect-101; every neighbour a centre of the
+        // tile reads lies inside the box, other positions are clamped into it)
+        const int x0 = bx * fsw::kBX - HW, y0 = by * fsw::kBY - HW;
+        const int xa = tma::floor_to(3 * x0, 4);
+        const float *ra = reinterpret_cast<const float *>(smem);
+        for (int q = tid; q < G::TW * G::TH; q += fsw::kBX * fsw::kBY) {
+            const int ty = q / G::TW, tx = q - ty * G::TW;
+            const int gx = min(max(mirror(x0 + tx, W), 0), W - 1);
+            const int gy = min(max(mirror(y0 + ty, H), 0), H - 1);
+            const int rx = min(max(3 * gx - xa, 0), G::BOXW - 3), ry = min(max(gy - y0, 0), G::TH - 1);
+            const float *a = ra + ry * G::BOXW + rx;
+            const float *c = a + G::PLANE / 4, *l = a + G::PLANE / 2, *n = a + 3 * (G::PLANE / 4);
+            tile[3 * q + 0] = make_ulonglong2(fsw::pack(a[0], c[0]), fsw::pack(a[1], c[1]));
+            tile[3 * q + 1] = make_ulonglong2(fsw::pack(a[2], c[2]), fsw::pack(l[0], n[0]));
+            tile[3 * q + 2] = make_ulonglong2(fsw::pack(l[1], n[1]), fsw::pack(l[2], n[2]));
+        }
+        __syncthreads();   // records ready; the raw rows are free for the next tile
+        if (tid == 0 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x);
+
+        const int cx = bx * fsw::kBX + threadIdx.x, cy = by * fsw::kBY + threadIdx.y;
+        float loss = 0.f;
+        if (cx < W && cy < H) {
+            const size_t p = b * px + (size_t)cy * W + cx;
+            const fsw::Centre c = fsw::centre(tile, HW, band + 5 * p);
+            fsw::Sums s;
+            fsw::zero(s);
+            fsw::sweep<HW, true, true>(tile, pdtab, HW, c, s);
+            loss = filter_epilogue(s, c, P, p, gband, inv_n);
+        }
+        block_partial_at(loss, P.partial, t, fsw::kBX * fsw::kBY);   // ends with a barrier
+    }
+}
+
+template <int HW>
+cudaError_t launch_filter_aggregate_tma(const float *imga, const float *imgb, const float *albedo,
+                                        const float *normal, const float *band, const AggPtrs &P, float *gband,
+                                        int B, int H, int W, float inv_n, cudaStream_t st, bool *done)
+{
+    using G = FaGeom<HW>;
+    *done = false;
+    FaMaps m;
+    if (!tma::encode_image(&m.ia, imga, false, 3, W, H, B, G::BOXW, G::TH) ||
+        !tma::encode_image(&m.ib, imgb, false, 3, W, H, B, G::BOXW, G::TH) ||
+        !tma::encode_image(&m.al, albedo, false, 3, W, H, B, G::BOXW, G::TH) ||
+        !tma::encode_image(&m.nr, normal, false, 3, W, H, B, G::BOXW, G::TH))
+        return cudaSuccess;   // not eligible: the caller takes the tile-per-CTA kernel
+    static int occ[8] = {};
+    static int sms[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(filter_aggregate_tma_kernel<HW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  G::SMEM)) != cudaSuccess)
+        return e;
+    if (!occ[HW]) {
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[HW], filter_aggregate_tma_kernel<HW>,
+                                                                fsw::kBX * fsw::kBY, G::SMEM)) != cudaSuccess)
+            return e;
+        if (occ[HW] < 1) return cudaSuccess;
+    }
+    if (dev < 64 && !sms[dev] &&
+        (e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return e;
+    const int nsm = dev < 64 ? sms[dev] : 148;
+    const int ntx = (W + fsw::kBX - 1) / fsw::kBX, nty = (H + fsw::kBY - 1) / fsw::kBY, ntiles = ntx * nty * B;
+    const int grid = min(ntiles, nsm * occ[HW]);
+    filter_aggregate_tma_kernel<HW><<<grid, dim3(fsw::kBX, fsw::kBY), G::SMEM, st>>>(m, band, P, gband, H, W, ntx,
+                                                                                     nty, ntiles, inv_n);
+    *done = true;
+    return cudaGetLastError();
+}
+
 }  // namespace
+
+int filter_stage_error_flag()
+{
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_filter_stage_error, sizeof(int)) != cudaSuccess) return -1;
+    return v;
+}
 
 size_t aggregation_partials(int B, int H, int W) { return (size_t)((W + 31) / 32) * ((H + 7) / 8) * B; }
 
@@ -306,8 +489,12 @@ cudaError_t launch_filter_aggregate(const float *imga, const float *imgb, const 
         kern<<<grid, block, smem, st>>>(imga, imgb, albedo, normal, band, P, gband, H, W, hw, inv_n);
         return cudaGetLastError();
     };
-    cudaError_t e;
-    switch (hw) {
+    cudaError_t e = cudaSuccess;
+    bool done = false;
+    if (hw == 5 && tma::persistent_enabled())
+        e = launch_filter_aggregate_tma<5>(imga, imgb, albedo, normal, band, P, gband, B, H, W, inv_n, st, &done);
+    if (e != cudaSuccess) return e;
+    if (!done) switch (hw) {
     case 3: e = go(filter_aggregate_kernel<3>); break;
     case 5: e = go(filter_aggregate_kernel<5>); break;
     case 7: e = go(filter_aggregate_kernel<7>); break;

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
 #include "unet.cuh"
+#include "tma.cuh"
 #include "../../include/cd_ops.h"
 
 namespace {
@@ -52,6 +53,17 @@ void set_last_error(const char *msg) { snprintf(g_err, sizeof(g_err), "%s", msg)
 extern "C" {
 
 int cd_abi_version(void) { return 1; }
+
+int cd_image_kernel_error_flags(void)
+{
+    const int t = cd::temporal_error_flag(), f = cd::filter_stage_error_flag();
+    if (t < 0 || f < 0) return -1;
+    return (t ? 1 : 0) | (f ? 2 : 0);
+}
+
+void cd_set_persistent_kernels(int enable) { cd::tma::set_persistent_enabled(enable != 0); }
+
+void cd_set_unet_conv_stacked(int enable) { cd::unet::set_conv_stacked(enable != 0); }
 
 const char *cd_get_last_error(void) { return g_err; }
 

@@ -99,6 +99,11 @@ cudaError_t launch_temporal(const float *c1, const float *c2, const float *prev,
                             float *out2, float *succ, int B, int H, int W, int win_curr,
                             int win_prev, cudaStream_t st);
 
+// Sticky error bits of the persistent TMA image kernels (a staging wait ran
+// out), read synchronously; -1 if the read fails.
+int temporal_error_flag();
+int filter_stage_error_flag();
+
 // Records msg as the calling thread's cd_get_last_error() message.
 void set_last_error(const char *msg);
 // The argument checks of cd_cross_regression (null pointers, shape and

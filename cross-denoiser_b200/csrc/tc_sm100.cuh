@@ -119,6 +119,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Warp-collective store of zeros to 16 consecutive fp32 columns of this
+// warp's 32 TMEM lanes; tmem_wait_st waits for the warp's stores.
+__device__ __forceinline__ void tmem_st16_zero(uint32_t taddr)
+{
+    const uint32_t z = 0u;
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(taddr),
+        "r"(z)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 // cp.async of 16 bytes with zero fill when src_bytes == 0.
 __device__ __forceinline__ void cp16(void *dst, const void *src, uint32_t src_bytes)
 {

@@ -15,8 +15,19 @@
 // along y.  Out-of-image taps are stored as NaN, which fminf/fmaxf skip, so
 // the result equals the reference's in-bounds loop.  The accept/reject
 // decisions are exact: they involve only additions, halvings and compares.
+//
+// Fused erosion + screening with a one-pixel history window (win_prev = 1,
+// the reference's setting) runs as a persistent kernel: each CTA walks the
+// 32x8 tiles with stride gridDim.x, and the next two tiles' inputs (both
+// colour footprints with the window's halo, the three history buffers and
+// the raw mask with a one-pixel halo) arrive by TMA into a double buffer
+// while the current tile computes, so the DRAM latency is off the critical
+// path.  Its row pass slides the window over four output columns per thread
+// in registers.  Other window sizes and images whose rows are not a multiple
+// of 16 bytes take the tile-per-CTA kernel above it.
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
+#include "tma.cuh"
 
 namespace cd {
 namespace {
@@ -229,7 +240,283 @@ __global__ void __launch_bounds__(kTX * kTY, 3) temporal_kernel(
     succ[p] = ok[2] ? 1.f : 0.f;
 }
 
+
+// ---------------------------------------------------------------------------
+// Persistent TMA kernel (fused erosion, win_prev = 1, HC = win_curr / 2).
+// ---------------------------------------------------------------------------
+struct TsMaps {
+    CUtensorMap c1, c2, h0, h1, h2, mk;   // current1/2 and prev/prev1/prev2 as (3W, H, B) floats; mask (W, H, B) bytes
+};
+
+template <int HC>
+struct TsGeom {
+    static constexpr int TW = kTX + 2 * HC, TH = kTY + 2 * HC;
+    // colour box: 3 floats per pixel, the start rounded down to 16 bytes;
+    // OFF = the footprint's first float within the box row
+    static constexpr int OFF = (4 - (3 * HC) % 4) % 4;
+    static constexpr int BOXC = (3 * TW + OFF + 3) & ~3;
+    static constexpr int CBYTES = ((TH * BOXC * 4 + 127) / 128) * 128;
+    static constexpr int HBOX = 3 * kTX;                 // history box: the tile's 32 pixels
+    static constexpr int HBYTES = kTY * HBOX * 4;
+    static constexpr int MBOXX = 64, MBOXY = kTY + 2;    // mask box: columns x0-16 .. x0+47, rows y0-1 .. y0+8
+    static constexpr int MBYTES = MBOXX * MBOXY;
+    static constexpr int STAGE = 2 * CBYTES + 3 * HBYTES + MBYTES;
+    static constexpr int TX_BYTES = 2 * TH * BOXC * 4 + 3 * HBYTES + MBYTES;
+    static constexpr int PLANES = 2 * kVals * TH * kTX * 4;   // row-pass minima and maxima
+    static constexpr int SMEM = 2 * STAGE + PLANES + 16;
+    static constexpr int NJ = 4 + 2 * HC;                  // input columns of a 4-output row segment
+};
+
+__device__ int g_image_kernel_error = 0;   // sticky: bit 0 = a temporal-screening staging wait ran out
+
+constexpr int kWaitPolls = 1 << 22;
+
+// min and max over the 2*HC+1 consecutive values starting at each of 4
+// positions of a[0 .. 4 + 2*HC); NaN (out-of-image) values are skipped.
+template <int HC>
+CD_DEV void window4(const float *a, float *mn, float *mx)
+{
+    if constexpr (HC == 3) {
+        float n2[9], x2[9], n4[7], x4[7];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            n2[i] = fminf(a[i], a[i + 1]);
+            x2[i] = fmaxf(a[i], a[i + 1]);
+        }
+#pragma unroll
+        for (int i = 0; i < 7; ++i) {
+            n4[i] = fminf(n2[i], n2[i + 2]);
+            x4[i] = fmaxf(x2[i], x2[i + 2]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            mn[i] = fminf(n4[i], n4[i + 3]);
+            mx[i] = fmaxf(x4[i], x4[i + 3]);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            float n = a[i], x = a[i];
+#pragma unroll
+            for (int d = 1; d <= 2 * HC; ++d) {
+                n = fminf(n, a[i + d]);
+                x = fmaxf(x, a[i + d]);
+            }
+            mn[i] = n;
+            mx[i] = x;
+        }
+    }
+}
+
+template <int HC>
+__global__ void __launch_bounds__(kTX * kTY, 2) temporal_tma_kernel(
+    const __grid_constant__ TsMaps maps, float *__restrict__ eroded, float *__restrict__ out,
+    float *__restrict__ out1, float *__restrict__ out2, float *__restrict__ succ, int H, int W, int ntx,
+    int nty, int ntiles)
+{
+    using G = TsGeom<HC>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    float *rmin = reinterpret_cast<float *>(smem + 2 * G::STAGE);
+    float *rmax = rmin + kVals * G::TH * kTX;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * G::STAGE + G::PLANES);
+    const int tid = threadIdx.y * kTX + threadIdx.x;
+    const int per_img = ntx * nty;
+    const float qnan = __int_as_float(0x7fffffff);
+
+    auto issue = [&](int t, int s) {
+        const int b = t / per_img, r = t - b * per_img, by = r / ntx, bx = r - by * ntx;
+        unsigned char *st = smem + s * G::STAGE;
+        tc::mbar_expect_tx(&bar[s], G::TX_BYTES);
+        const int xc = tma::floor_to(3 * (bx * kTX - HC), 4), yc = by * kTY - HC;
+        tma::load3(st, &maps.c1, xc, yc, b, &bar[s]);
+        tma::load3(st + G::CBYTES, &maps.c2, xc, yc, b, &bar[s]);
+        unsigned char *hs = st + 2 * G::CBYTES;
+        tma::load3(hs, &maps.h0, 3 * kTX * bx, by * kTY, b, &bar[s]);
+        tma::load3(hs + G::HBYTES, &maps.h1, 3 * kTX * bx, by * kTY, b, &bar[s]);
+        tma::load3(hs + 2 * G::HBYTES, &maps.h2, 3 * kTX * bx, by * kTY, b, &bar[s]);
+        tma::load3(hs + 3 * G::HBYTES, &maps.mk, bx * kTX - 16, by * kTY - 1, b, &bar[s]);
+    };
+
+    if (tid == 0) {
+        tc::mbar_init(&bar[0], 1);
+        tc::mbar_init(&bar[1], 1);
+    }
+    __syncthreads();
+    const int G0 = (int)gridDim.x;
+    if (tid == 0) {
+        if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+        if ((int)blockIdx.x + G0 < ntiles) issue(blockIdx.x + G0, 1);
+    }
+    int it = 0;
+    for (int t = blockIdx.x; t < ntiles; t += G0, ++it) {
+        const int s = it & 1;
+        const bool landed = __syncthreads_and(tc::mbar_wait(&bar[s], (uint32_t)(it >> 1) & 1u, kWaitPolls)) != 0;
+        if (!landed) {
+            // give the other stage's copy, if one was issued, a bounded wait
+            // before leaving, and report the time-out
+            if (tid == 0) {
+                atomicOr(&g_image_kernel_error, 1);
+                if (t + G0 < ntiles) tc::mbar_wait(&bar[s ^ 1], (uint32_t)((it + 1) >> 1) & 1u, kWaitPolls);
+            }
+            return;
+        }
+        const int b = t / per_img, rr = t - b * per_img, by = rr / ntx, bx = rr - by * ntx;
+        const size_t px = (size_t)H * W;
+        const float *C1 = reinterpret_cast<const float *>(smem + s * G::STAGE);
+        const float *C2 = reinterpret_cast<const float *>(smem + s * G::STAGE + G::CBYTES);
+        const float *H0 = reinterpret_cast<const float *>(smem + s * G::STAGE + 2 * G::CBYTES);
+        const float *H1 = H0 + kTY * G::HBOX, *H2 = H1 + kTY * G::HBOX;
+        const unsigned char *MK = smem + s * G::STAGE + 2 * G::CBYTES + 3 * G::HBYTES;
+
+        // row pass: item (r, q) = tile row r, output columns 4q .. 4q + 3
+        if (tid < G::TH * (kTX / 4)) {
+            const int r = tid >> 3, q = tid & 7;
+            const int gy = by * kTY - HC + r;
+            const int gx0 = bx * kTX - HC + 4 * q;
+            const bool row_in = gy >= 0 && gy < H;
+            const bool all_in = row_in && gx0 >= 0 && gx0 + G::NJ <= W;
+            const float *c1r = C1 + r * G::BOXC + G::OFF + 12 * q;
+            const float *c2r = C2 + r * G::BOXC + G::OFF + 12 * q;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                float a[G::NJ], bb[G::NJ], v[G::NJ];
+#pragma unroll
+                for (int j = 0; j < G::NJ; ++j) {
+                    const bool in = all_in || (row_in && gx0 + j >= 0 && gx0 + j < W);
+                    a[j] = in ? c1r[3 * j + c] : qnan;
+                    bb[j] = in ? c2r[3 * j + c] : qnan;
+                    v[j] = (a[j] + bb[j]) * 0.5f;
+                }
+                float mn[4], mx[4];
+                const int o = r * kTX + 4 * q;
+                window4<HC>(a, mn, mx);
+                *reinterpret_cast<float4 *>(rmin + c * G::TH * kTX + o) = make_float4(mn[0], mn[1], mn[2], mn[3]);
+                *reinterpret_cast<float4 *>(rmax + c * G::TH * kTX + o) = make_float4(mx[0], mx[1], mx[2], mx[3]);
+                window4<HC>(bb, mn, mx);
+                *reinterpret_cast<float4 *>(rmin + (3 + c) * G::TH * kTX + o) = make_float4(mn[0], mn[1], mn[2], mn[3]);
+                *reinterpret_cast<float4 *>(rmax + (3 + c) * G::TH * kTX + o) = make_float4(mx[0], mx[1], mx[2], mx[3]);
+                window4<HC>(v, mn, mx);
+                *reinterpret_cast<float4 *>(rmin + (6 + c) * G::TH * kTX + o) = make_float4(mn[0], mn[1], mn[2], mn[3]);
+                *reinterpret_cast<float4 *>(rmax + (6 + c) * G::TH * kTX + o) = make_float4(mx[0], mx[1], mx[2], mx[3]);
+            }
+        }
+        __syncthreads();
+
+        const int tx = threadIdx.x, ty = threadIdx.y;
+        const int cx = bx * kTX + tx, cy = by * kTY + ty;
+        if (cx < W && cy < H) {
+            const size_t p = b * px + (size_t)cy * W + cx;
+            // 3x3 erosion of the raw mask, image pixels only (the TMA fills
+            // out-of-image bytes with zeros; the min ignores them)
+            bool keep = true;
+#pragma unroll
+            for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const bool in = cx + dx >= 0 && cx + dx < W && cy + dy >= 0 && cy + dy < H;
+                    keep = keep && (!in || MK[(ty + 1 + dy) * G::MBOXX + tx + 16 + dx] != 0);
+                }
+            const float m = keep ? 1.f : 0.f;
+            eroded[p] = m;
+            const int co = (ty + HC) * G::BOXC + G::OFF + 3 * (tx + HC);
+            const float3 a1 = make_float3(C1[co], C1[co + 1], C1[co + 2]);
+            const float3 a2 = make_float3(C2[co], C2[co + 1], C2[co + 2]);
+            const float3 cu = make_float3((a1.x + a2.x) * 0.5f, (a1.y + a2.y) * 0.5f, (a1.z + a2.z) * 0.5f);
+            if (m + 1e-4f < 1.f) {
+                st3(out, p, cu);
+                st3(out1, p, a1);
+                st3(out2, p, a2);
+                succ[p] = 0.f;
+            } else {
+                float mnC[kVals], mxC[kVals];
+#pragma unroll
+                for (int k = 0; k < kVals; ++k) {
+                    float n = kBig, x = -kBig;
+#pragma unroll
+                    for (int dy = 0; dy <= 2 * HC; ++dy) {
+                        n = fminf(n, rmin[(k * G::TH + ty + dy) * kTX + tx]);
+                        x = fmaxf(x, rmax[(k * G::TH + ty + dy) * kTX + tx]);
+                    }
+                    mnC[k] = n;
+                    mxC[k] = x;
+                }
+                const int ho = ty * G::HBOX + 3 * tx;
+                const float3 h0 = make_float3(H0[ho], H0[ho + 1], H0[ho + 2]);
+                const float3 h1 = make_float3(H1[ho], H1[ho + 1], H1[ho + 2]);
+                const float3 h2 = make_float3(H2[ho], H2[ho + 1], H2[ho + 2]);
+                // the history window is the pixel itself (its mask is >= 1 here)
+                const float hv[kVals] = {h1.x, h1.y, h1.z, h2.x, h2.y, h2.z, h0.x, h0.y, h0.z};
+                bool ok[3];
+#pragma unroll
+                for (int g = 0; g < 3; ++g) {
+                    bool o = true;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const float mnP = fminf(kBig, hv[3 * g + k]), mxP = fmaxf(-kBig, hv[3 * g + k]);
+                        o = o && (mnP < mxC[3 * g + k]) && (mnC[3 * g + k] < mxP);
+                    }
+                    ok[g] = o;
+                }
+                st3(out1, p, ok[0] ? h1 : a1);
+                st3(out2, p, ok[1] ? h2 : a2);
+                st3(out, p, ok[2] ? h0 : cu);
+                succ[p] = ok[2] ? 1.f : 0.f;
+            }
+        }
+        __syncthreads();   // every read of stage s and of the row planes is done
+        if (tid == 0 && t + 2 * G0 < ntiles) issue(t + 2 * G0, s);
+    }
+}
+
+template <int HC>
+cudaError_t launch_temporal_tma(const float *c1, const float *c2, const float *prev, const float *prev1,
+                                const float *prev2, const uint8_t *raw, float *eroded, float *out, float *out1,
+                                float *out2, float *succ, int B, int H, int W, cudaStream_t st, bool *done)
+{
+    using G = TsGeom<HC>;
+    *done = false;
+    TsMaps m;
+    if (!tma::encode_image(&m.c1, c1, false, 3, W, H, B, G::BOXC, G::TH) ||
+        !tma::encode_image(&m.c2, c2, false, 3, W, H, B, G::BOXC, G::TH) ||
+        !tma::encode_image(&m.h0, prev, false, 3, W, H, B, G::HBOX, kTY) ||
+        !tma::encode_image(&m.h1, prev1, false, 3, W, H, B, G::HBOX, kTY) ||
+        !tma::encode_image(&m.h2, prev2, false, 3, W, H, B, G::HBOX, kTY) ||
+        !tma::encode_image(&m.mk, raw, true, 1, W, H, B, G::MBOXX, G::MBOXY))
+        return cudaSuccess;   // not eligible: the caller takes the tile-per-CTA kernel
+    static int occ[8] = {};
+    static int sms[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(temporal_tma_kernel<HC>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM)) !=
+        cudaSuccess)
+        return e;
+    if (!occ[HC]) {
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[HC], temporal_tma_kernel<HC>, kTX * kTY,
+                                                                G::SMEM)) != cudaSuccess)
+            return e;
+        if (occ[HC] < 1) return cudaSuccess;
+    }
+    if (dev < 64 && !sms[dev] &&
+        (e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return e;
+    const int nsm = dev < 64 ? sms[dev] : 148;
+    const int ntx = (W + kTX - 1) / kTX, nty = (H + kTY - 1) / kTY, ntiles = ntx * nty * B;
+    const int grid = min(ntiles, nsm * occ[HC]);
+    temporal_tma_kernel<HC><<<grid, dim3(kTX, kTY), G::SMEM, st>>>(m, eroded, out, out1, out2, succ, H, W, ntx, nty,
+                                                                   ntiles);
+    *done = true;
+    return cudaGetLastError();
+}
+
 }  // namespace
+
+int temporal_error_flag()
+{
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_image_kernel_error, sizeof(int)) != cudaSuccess) return -1;
+    return v;
+}
 
 cudaError_t launch_erode3x3(const uint8_t *mask, float *out, int B, int H, int W, cudaStream_t st)
 {
@@ -251,6 +538,16 @@ cudaError_t launch_temporal(const float *c1, const float *c2, const float *prev,
     dim3 block(kTX, kTY);
     dim3 grid((W + kTX - 1) / kTX, (H + kTY - 1) / kTY, B);
     cudaError_t e;
+    if (raw && hp == 0 && hc >= 1 && hc <= 3 && tma::persistent_enabled()) {
+        bool done = false;
+        e = hc == 3 ? launch_temporal_tma<3>(c1, c2, prev, prev1, prev2, raw, eroded, out, out1, out2, succ, B, H, W,
+                                             st, &done)
+          : hc == 2 ? launch_temporal_tma<2>(c1, c2, prev, prev1, prev2, raw, eroded, out, out1, out2, succ, B, H, W,
+                                             st, &done)
+                    : launch_temporal_tma<1>(c1, c2, prev, prev1, prev2, raw, eroded, out, out1, out2, succ, B, H, W,
+                                             st, &done);
+        if (e != cudaSuccess || done) return e;
+    }
     if (raw) {
         e = cudaFuncSetAttribute(temporal_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);

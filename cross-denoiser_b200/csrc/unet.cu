@@ -125,6 +125,7 @@ struct Ctx {
     int B, H, W;
     cudaStream_t st;
     const float *params;
+    bool stacked = conv_stacked_enabled();   // the convolution form of this call (packing and kernels agree)
     __nv_bfloat16 *buf(Buf b) const { return reinterpret_cast<__nv_bfloat16 *>(ws + L.buf[b]); }
     int *err() const { return reinterpret_cast<int *>(ws); }
     float *partial() const { return reinterpret_cast<float *>(ws + L.partial); }
@@ -149,8 +150,9 @@ cudaError_t pack_all(const Ctx &c, bool dgrad)
         if (d.kind != CONV) continue;
         PackJob &j = J.job[J.n++];
         KStep st[kMaxSteps];
-        j.T.nsteps =
-            dgrad ? build_steps(chunks(d.cout), 0, st, j.T.half) : build_steps(kSrc0[l], kSrc1[l], st, j.T.half);
+        auto steps = c.stacked ? build_steps_stacked : build_steps;
+        j.T.nsteps = dgrad ? steps(chunks(d.cout), 0, st, j.T.half) : steps(kSrc0[l], kSrc1[l], st, j.T.half);
+        j.T.stacked = c.stacked ? 1 : 0;
         j.T.nout = nout_of(dgrad ? d.cin : d.cout);
         j.T.cin = d.cin;
         j.T.cout = d.cout;
@@ -168,7 +170,8 @@ cudaError_t conv(const Ctx &c, int l, bool dgrad, int lvl, Buf s0, int c0, Buf s
     const LayerDef &d = kDef[l];
     ConvParams P{};
     StepHalf hf[kMaxSteps][2];
-    P.nsteps = build_steps(c0, c1, P.steps, hf);
+    P.nsteps = (c.stacked ? build_steps_stacked : build_steps)(c0, c1, P.steps, hf);
+    P.stacked = c.stacked ? 1 : 0;
     P.src0 = c.buf(s0);
     P.src1 = c1 ? c.buf(s1) : nullptr;
     P.c0 = c0;
@@ -356,17 +359,21 @@ cudaError_t conv_layer(const float *w, const float *bias, const __nv_bfloat16 *x
     uint8_t *base = static_cast<uint8_t *>(ws);
     __nv_bfloat16 *wp = reinterpret_cast<__nv_bfloat16 *>(base + 256);
     const int in_ch = dgrad ? cout : cin, out_ch = dgrad ? cin : cout;
+    const bool stacked = conv_stacked_enabled();
+    auto steps = stacked ? build_steps_stacked : build_steps;
     PackTable T{};
     KStep st_[kMaxSteps];
-    T.nsteps = build_steps(chunks(in_ch), 0, st_, T.half);
+    T.nsteps = steps(chunks(in_ch), 0, st_, T.half);
     T.nout = nout_of(out_ch);
     T.cin = cin;
     T.cout = cout;
     T.dgrad = dgrad;
+    T.stacked = stacked ? 1 : 0;
     CD_TRY(launch_pack(w, wp, T, st));
     ConvParams P{};
     StepHalf hf[kMaxSteps][2];
-    P.nsteps = build_steps(chunks(in_ch), 0, P.steps, hf);
+    P.nsteps = steps(chunks(in_ch), 0, P.steps, hf);
+    P.stacked = stacked ? 1 : 0;
     P.src0 = x;
     P.c0 = chunks(in_ch);
     P.wpack = wp;

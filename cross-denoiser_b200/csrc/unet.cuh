@@ -32,7 +32,9 @@ struct KStep {
     int ky, a_off, a_lbo, src;   // src: which input source's staged rows
 };
 // What each half of a K step multiplies: tap (ky, kx) of input chunk `chunk`
-// (-1: unused, zero weights).
+// (-1: unused, zero weights).  In a ky-stacked table (build_steps_stacked)
+// ky is -1: the step's B operand holds the three vertical taps stacked along
+// N (rows [0, n) ky = 2, [n, 2n) ky = 1, [2n, 3n) ky = 0).
 struct StepHalf {
     int ky, kx, chunk;
 };
@@ -48,11 +50,20 @@ struct ConvParams {
     __nv_bfloat16 *pool;                // fused 2x2 max pool of dst0, or null
     int relu;
     int H, W, nsteps;
+    int stacked;                        // 1: ky-stacked step table and B operand
     int *err;                           // set to 1 if an MMA wait times out
     KStep steps[kMaxSteps];
 };
 
 int build_steps(int c0, int c1, KStep *steps, StepHalf (*half)[2]);
+// The same taps as build_steps with the three vertical taps of each (kx,
+// chunk) pair in one step (a third of the steps, three times the B rows).
+int build_steps_stacked(int c0, int c1, KStep *steps, StepHalf (*half)[2]);
+// Process-wide choice of the convolution form (ky-stacked: one MMA per input
+// row and K step feeds three output rows; per-row: one MMA per output row,
+// tap and K step); set by cd_set_unet_conv_stacked, read once per call.
+bool conv_stacked_enabled();
+void set_conv_stacked(bool on);
 cudaError_t launch_conv3x3(const ConvParams &P, int B, int nout, cudaStream_t st);
 
 // Pack fp32 Keras weights W[3][3][cin][cout] into the B operand of a conv
@@ -60,7 +71,7 @@ cudaError_t launch_conv3x3(const ConvParams &P, int B, int nout, cudaStream_t st
 // the output gradient): conv input channel = layer output channel.
 struct PackTable {
     StepHalf half[kMaxSteps][2];
-    int nsteps, nout, cin, cout, dgrad;
+    int nsteps, nout, cin, cout, dgrad, stacked;   // stacked: 3 * nout B rows per half
 };
 cudaError_t launch_pack(const float *w, __nv_bfloat16 *dst, const PackTable &T, cudaStream_t st);
 

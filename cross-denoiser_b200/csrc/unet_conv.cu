@@ -26,6 +26,7 @@
 // outside the image copied from a page of zeros.  Every byte of the staged
 // planes is written by exactly one copy, so the mbarrier's transaction count
 // is the planes' total size.
+#include <atomic>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
@@ -85,16 +86,34 @@ __host__ __device__ inline size_t conv_smem(int nsteps, int nout, int c0, int c1
            align128((size_t)(R + 2) * c1 * kPlane) + 16;
 }
 
-template <int NOUT, int R>
+// TMEM columns of a CTA: R row groups of NOUT accumulators, or, ky-stacked,
+// R + 4 (input row i's MMAs write groups i .. i + 2, i = 0 .. R + 1; output
+// row r is group r + 2), rounded up to a power of two >= 32.
+template <int NOUT, int R, bool KYN>
+__host__ __device__ constexpr int conv_cols()
+{
+    constexpr int n = KYN ? (R + 4) * NOUT : R * NOUT;
+    return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : n <= 256 ? 256 : 512;
+}
+
+// ky-stacked form: D[128 px x 3 NOUT] += A_i[128 x 16] * B_s[3 NOUT x 16]^T
+// for staged input row i and K step s, with B_s's three NOUT-row blocks the
+// taps ky = 2, 1, 0 and D the TMEM groups i, i + 1, i + 2: output row r
+// (group r + 2) receives ky = 0 from input row r, ky = 1 from r + 1 and
+// ky = 2 from r + 2, accumulating in place (every MMA accumulates into
+// zero-initialised TMEM).  Compared with one MMA per output row and tap,
+// (R + 2) / (3 R) of the MMAs, each N = 3 NOUT wide (an MMA of M = 128,
+// K = 16 costs about the same for any N up to 64).
+template <int NOUT, int R, bool KYN>
 __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P)
 {
     extern __shared__ __align__(128) uint8_t smem[];
-    constexpr int kCols = (R * NOUT <= 32) ? 32 : (R * NOUT <= 64) ? 64 : (R * NOUT <= 128) ? 128
-                                                : (R * NOUT <= 256) ? 256 : 512;
-    static_assert(R * NOUT <= 512, "TMEM holds 512 columns");
+    constexpr int kCols = conv_cols<NOUT, R, KYN>();
+    static_assert((KYN ? (R + 4) * NOUT : R * NOUT) <= 512, "TMEM holds 512 columns");
+    constexpr int kRowsB = KYN ? 3 * NOUT : NOUT;   // B operand rows per step half
     const int tid = threadIdx.x, warp = tid >> 5;
     const int x0 = blockIdx.x * kPx, y0 = blockIdx.y * R, b = blockIdx.z;
-    const int bb = b_bytes(P.nsteps, NOUT);
+    const int bb = b_bytes(P.nsteps, kRowsB);
     // [packed weights][source 0 rows][source 1 rows], blocks 128-byte aligned
     const size_t blk0 = align128((size_t)(R + 2) * P.c0 * kPlane), blk1 = align128((size_t)(R + 2) * P.c1 * kPlane);
     uint8_t *sB = smem;
@@ -141,18 +160,39 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P)
         if (warp == 0) tc::tmem_dealloc(tbase, kCols);
         return;
     }
+    if (KYN) {
+        // zero the accumulators: each warp its 32 lanes, every group
+        const uint32_t lanes = tbase + ((uint32_t)(warp * 32) << 16);
+        for (int col = 0; col < (R + 4) * NOUT; col += 16) tc::tmem_st16_zero(lanes + col);
+        tc::tmem_wait_st();
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+    }
     if (tid == 0) {
-        const uint32_t idesc = tc::idesc_bf16(kPx, NOUT);
         const uint32_t a0 = tc::smem_u32(sA0), a1 = tc::smem_u32(sA1), b0 = tc::smem_u32(sB);
-        for (int r = 0; r < R; ++r)
-            for (int s = 0; s < P.nsteps; ++s) {
-                const KStep st = P.steps[s];
-                const uint32_t base = st.src ? a1 + (uint32_t)((r + st.ky) * P.c1) * kPlane
-                                             : a0 + (uint32_t)((r + st.ky) * P.c0) * kPlane;
-                const uint64_t ad = tc::sdesc(base + st.a_off, st.a_lbo, 128);
-                const uint64_t bd = tc::sdesc(b0 + (uint32_t)(s * 2 * NOUT * 16), NOUT * 16, 128);
-                tc::mma_bf16(tbase + r * NOUT, ad, bd, idesc, s > 0 ? 1u : 0u);
-            }
+        if (KYN) {
+            const uint32_t idesc = tc::idesc_bf16(kPx, 3 * NOUT);
+            for (int i = 0; i < R + 2; ++i)
+                for (int s = 0; s < P.nsteps; ++s) {
+                    const KStep st = P.steps[s];
+                    const uint32_t base = st.src ? a1 + (uint32_t)(i * P.c1) * kPlane : a0 + (uint32_t)(i * P.c0) * kPlane;
+                    const uint64_t ad = tc::sdesc(base + st.a_off, st.a_lbo, 128);
+                    const uint64_t bd = tc::sdesc(b0 + (uint32_t)(s * 2 * kRowsB * 16), kRowsB * 16, 128);
+                    tc::mma_bf16(tbase + i * NOUT, ad, bd, idesc, 1u);
+                }
+        } else {
+            const uint32_t idesc = tc::idesc_bf16(kPx, NOUT);
+            for (int r = 0; r < R; ++r)
+                for (int s = 0; s < P.nsteps; ++s) {
+                    const KStep st = P.steps[s];
+                    const uint32_t base = st.src ? a1 + (uint32_t)((r + st.ky) * P.c1) * kPlane
+                                                 : a0 + (uint32_t)((r + st.ky) * P.c0) * kPlane;
+                    const uint64_t ad = tc::sdesc(base + st.a_off, st.a_lbo, 128);
+                    const uint64_t bd = tc::sdesc(b0 + (uint32_t)(s * 2 * NOUT * 16), NOUT * 16, 128);
+                    tc::mma_bf16(tbase + r * NOUT, ad, bd, idesc, s > 0 ? 1u : 0u);
+                }
+        }
         tc::commit(bar);
     }
     // the commit completes the barrier's second phase (parity 1)
@@ -167,7 +207,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P)
         for (int r = 0; r < R; ++r) {
             float v[NOUT];
 #pragma unroll
-            for (int j = 0; j < NOUT; j += 16) tc::tmem_ld16(lane_base + r * NOUT + j, v + j);
+            for (int j = 0; j < NOUT; j += 16) tc::tmem_ld16(lane_base + (KYN ? r + 2 : r) * NOUT + j, v + j);
             const int y = y0 + r;
             const bool inside = x < P.W && y < P.H;
             const int yi = inside ? y : 0, xi = inside ? x : 0;
@@ -245,29 +285,36 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P)
     if (warp == 0) tc::tmem_dealloc(tbase, kCols);
 }
 
-template <int NOUT, int R>
+template <int NOUT, int R, bool KYN>
 cudaError_t launch_t(const ConvParams &P, int B, cudaStream_t st)
 {
-    constexpr int kCols = (R * NOUT <= 32) ? 32 : (R * NOUT <= 64) ? 64 : (R * NOUT <= 128) ? 128
-                                                : (R * NOUT <= 256) ? 256 : 512;
-    const size_t smem = smem_for_tmem(conv_smem(P.nsteps, NOUT, P.c0, P.c1, R), kCols);
-    cudaError_t e = cudaFuncSetAttribute(conv3x3_kernel<NOUT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    constexpr int kCols = conv_cols<NOUT, R, KYN>();
+    const size_t smem = smem_for_tmem(conv_smem(P.nsteps, KYN ? 3 * NOUT : NOUT, P.c0, P.c1, R), kCols);
+    cudaError_t e = cudaFuncSetAttribute(conv3x3_kernel<NOUT, R, KYN>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid((P.W + kPx - 1) / kPx, (P.H + R - 1) / R, B);
-    conv3x3_kernel<NOUT, R><<<grid, 128, smem, st>>>(P);
+    conv3x3_kernel<NOUT, R, KYN><<<grid, 128, smem, st>>>(P);
     return cudaGetLastError();
 }
 
 // Packed B operand: per step s, half h, conv output row n, element e
 // (dst[((s * 2 + h) * nout + n) * 8 + e]) the weight of tap (ky, kx) from
-// conv input channel 8 * chunk + e to conv output channel n.
+// conv input channel 8 * chunk + e to conv output channel n; in a ky-stacked
+// table the rows are 3 * nout, row n' holding tap ky = 2 - n' / nout of
+// output channel n' % nout.
 __device__ __forceinline__ void pack_one(const float *__restrict__ w, __nv_bfloat16 *__restrict__ dst,
                                          const PackTable &T, int i)
 {
-    if (i >= T.nsteps * 2 * T.nout * 8) return;
-    const int e = i & 7, n = (i >> 3) % T.nout, h = (i / (8 * T.nout)) & 1, s = i / (16 * T.nout);
-    const StepHalf hf = T.half[s][h];
+    const int rows = T.stacked ? 3 * T.nout : T.nout;
+    if (i >= T.nsteps * 2 * rows * 8) return;
+    const int e = i & 7, nr = (i >> 3) % rows, h = (i / (8 * rows)) & 1, s = i / (16 * rows);
+    StepHalf hf = T.half[s][h];
+    int n = nr;
+    if (T.stacked) {
+        hf.ky = 2 - nr / T.nout;   // rows [0, n): ky 2, [n, 2n): ky 1, [2n, 3n): ky 0
+        n = nr % T.nout;
+    }
     float v = 0.f;
     if (hf.chunk >= 0) {
         const int ci = 8 * hf.chunk + e;
@@ -688,6 +735,10 @@ cudaError_t launch_wgrad3_t(const WgradParams &P, int B, int grid, cudaStream_t 
 // Output rows per CTA: 4 (more CTAs per SM than 8-row tiles; measured faster
 // in the whole network although the row halo grows from 25 to 50 %).
 constexpr int kConvRows = 4;
+// Output rows per CTA of the ky-stacked form: its TMEM holds R + 4 row
+// groups (two junk groups on each side), and its MMA count per output row
+// falls with R ((R + 2) / R input rows per output row).
+constexpr int kConvRowsStacked = 4;
 
 
 // K-step table for input chunks split over two sources (c0 chunks of source
@@ -722,11 +773,48 @@ int build_steps(int c0, int c1, KStep *steps, StepHalf (*half)[2])
     return n;
 }
 
+int build_steps_stacked(int c0, int c1, KStep *steps, StepHalf (*half)[2])
+{
+    int n = 0;
+    for (int src = 0; src < 2; ++src) {
+        const int nc = src ? c1 : c0, g0 = src ? c0 : 0;
+        for (int c = 0; c + 1 < nc; c += 2)
+            for (int kx = 0; kx < 3; ++kx) {
+                steps[n] = KStep{0, c * kPlane + kx * 16, kPlane, src};
+                half[n][0] = StepHalf{-1, kx, g0 + c};
+                half[n][1] = StepHalf{-1, kx, g0 + c + 1};
+                ++n;
+            }
+        if (nc & 1) {
+            const int c = nc - 1;
+            for (int kx = 0; kx < 3; kx += 2) {
+                steps[n] = KStep{0, c * kPlane + kx * 16, 16, src};
+                half[n][0] = StepHalf{-1, kx, g0 + c};
+                half[n][1] = kx + 1 < 3 ? StepHalf{-1, kx + 1, g0 + c} : StepHalf{0, 0, -1};
+                ++n;
+            }
+        }
+    }
+    return n;
+}
+
+namespace {
+std::atomic<int> g_conv_stacked{1};
+}
+bool conv_stacked_enabled() { return g_conv_stacked.load(std::memory_order_relaxed) != 0; }
+void set_conv_stacked(bool on) { g_conv_stacked.store(on ? 1 : 0, std::memory_order_relaxed); }
+
 cudaError_t launch_conv3x3(const ConvParams &P, int B, int nout, cudaStream_t st)
 {
-    if (nout == 16) return launch_t<16, kConvRows>(P, B, st);
-    if (nout == 32) return launch_t<32, kConvRows>(P, B, st);
-    if (nout == 48) return launch_t<48, kConvRows>(P, B, st);
+    if (P.stacked) {
+        if (nout == 16) return launch_t<16, kConvRowsStacked, true>(P, B, st);
+        if (nout == 32) return launch_t<32, kConvRowsStacked, true>(P, B, st);
+        if (nout == 48) return launch_t<48, kConvRowsStacked, true>(P, B, st);
+        return cudaErrorInvalidValue;
+    }
+    if (nout == 16) return launch_t<16, kConvRows, false>(P, B, st);
+    if (nout == 32) return launch_t<32, kConvRows, false>(P, B, st);
+    if (nout == 48) return launch_t<48, kConvRows, false>(P, B, st);
     return cudaErrorInvalidValue;
 }
 
@@ -741,7 +829,7 @@ cudaError_t launch_pack_jobs(const PackJobs &J, cudaStream_t st)
     if (J.n < 1 || J.n > kMaxPackJobs) return cudaErrorInvalidValue;
     int most = 0;
     for (int j = 0; j < J.n; ++j) {
-        const int n = J.job[j].T.nsteps * 2 * J.job[j].T.nout * 8;
+        const int n = J.job[j].T.nsteps * 2 * J.job[j].T.nout * (J.job[j].T.stacked ? 3 : 1) * 8;
         most = n > most ? n : most;
     }
     pack_jobs_kernel<<<dim3((most + 255) / 256, J.n), 256, 0, st>>>(J);
@@ -750,7 +838,7 @@ cudaError_t launch_pack_jobs(const PackJobs &J, cudaStream_t st)
 
 cudaError_t launch_pack(const float *w, __nv_bfloat16 *dst, const PackTable &T, cudaStream_t st)
 {
-    const int n = T.nsteps * 2 * T.nout * 8;
+    const int n = T.nsteps * 2 * T.nout * (T.stacked ? 3 : 1) * 8;
     pack_kernel<<<(n + 255) / 256, 256, 0, st>>>(w, dst, T);
     return cudaGetLastError();
 }

@@ -4,11 +4,13 @@ through the float64 restatement oracle/regression_fp64.py.
 The reference has no gradient for this op, so the FP64 restatement of its
 forward (itself checked against central differences in
 test_oracle_regression_fp64.py) is the oracle.  FP32 gradient vs FP64
-gradient tolerance, per output tensor:
-    |g - g64| <= 5e-4 * max|g64| + 1e-3 * |g64|
-(the forward alone differs from FP64 by up to ~7e-5 relative; the backward
-passes through two 6x6 solves and the reconstruction's quotient; measured
-worst case 7e-5 of max|g64|).
+gradient tolerance, per element of each output tensor:
+    |g - g64| <= 1e-4 * |g64| + 1e-4 * max|g64|
+i.e. rtol 1e-4 with an absolute floor of 1e-4 of the tensor's largest
+magnitude (entries that are sums of many terms of both signs end near zero,
+where a relative bound alone is meaningless; the forward alone differs from
+FP64 by up to ~7e-5 relative, and the backward passes through two 6x6
+solves and the reconstruction's quotient).
 """
 import numpy as np
 import pytest
@@ -18,7 +20,7 @@ from gpu_util import T, N, frames
 from oracle import regression_fp64 as r64
 
 pytestmark = pytest.mark.gpu
-RTOL_MAX, RTOL_EL = 5e-4, 1e-3
+FLOOR_OF_MAX, RTOL_EL = 1e-4, 1e-4
 NAMES = ("grad_imga", "grad_imgb", "grad_albedo", "grad_normal")
 
 
@@ -51,7 +53,7 @@ def fp64_grads(ins, ups, win, sp, rs):
 def check(got, want, what):
     for g, w, nm in zip(got, want, NAMES):
         err = np.abs(g.astype(np.float64) - w)
-        bound = RTOL_MAX * np.abs(w).max() + RTOL_EL * np.abs(w)
+        bound = FLOOR_OF_MAX * np.abs(w).max() + RTOL_EL * np.abs(w)
         bad = err > bound
         assert not bad.any(), (f"{what} {nm}: {bad.sum()} of {bad.size} beyond tolerance, "
                                f"max err {err.max():.3g}, max|g64| {np.abs(w).max():.3g}")

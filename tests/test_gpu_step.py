@@ -183,3 +183,26 @@ def test_npy_sequence_through_host_pipeline(cd, cuda, tmp_path):
         out, loss, ev = pipe(f)
         ev.synchronize()
         assert_equal(out.numpy(), want[t], f"frame {t} out")
+
+
+@pytest.mark.parametrize("H,W,B", [(136, 200, 1), (6, 12, 1), (45, 68, 2), (1080, 1920, 1)])
+def test_persistent_filter_aggregate_equals_tile_kernel(cd, cuda, H, W, B):
+    """The persistent TMA-staged fused filter (window 11, rows a multiple of
+    16 bytes) gives the tile-per-CTA kernel's outputs bit for bit, with
+    partial tiles at the right and bottom edges, several images and boxes
+    reaching past the image; no staging wait ran out."""
+    L = cd._lib.lib()
+    x = [filter_inputs(cd, H, W, 3 + b, cuda) for b in range(B)]
+    args = [torch.cat([xi[k] for xi in x]) for k in range(12)]
+    outs = []
+    try:
+        for persistent in (1, 0):
+            L.cd_set_persistent_kernels(persistent)
+            o = cd.ops.filter_aggregate(*args, 11)
+            torch.cuda.synchronize()
+            outs.append([N(t) for t in o])
+    finally:
+        L.cd_set_persistent_kernels(1)
+    for a, b, nm in zip(outs[0], outs[1], ("out_log", "out", "avg_loss", "grad_band", "grad_alpha")):
+        assert_equal(a, b, nm)
+    assert L.cd_image_kernel_error_flags() == 0

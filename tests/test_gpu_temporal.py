@@ -61,6 +61,37 @@ def test_vs_oracle(cd, cuda, H, W, B, wc, wp):
         assert_equal(N(f[i]), ro[i], f"fused out{i}")
 
 
+@pytest.mark.parametrize("H,W,B,wc", [(37, 48, 3, 7), (8, 16, 1, 7), (5, 16, 2, 5), (70, 176, 1, 3),
+                                       (130, 272, 2, 7), (19, 80, 1, 5)])
+def test_persistent_tma_kernel(cd, cuda, H, W, B, wc):
+    """Rows a multiple of 16 bytes and win_prev = 1: the fused op takes the
+    persistent kernel with TMA-staged tiles (partial tiles at the right and
+    bottom edges, boxes reaching past the image, several images, more tiles
+    than CTAs and fewer).  Bit-exact against the oracle, the two-op
+    sequence and the tile-per-CTA fused kernel; no staging wait ran out."""
+    c1, c2, prev, p1, p2, mask = inputs(cd, H, W, B, seed=H + W)
+    ero = orc.erode3x3(mask)
+    ro = orc.temporal_screening(c1, c2, prev, p1, p2, ero, wc, 1)
+    ins = [T(x) for x in (c1, c2, prev, p1, p2)]
+    o = cd.ops.temporal_screening(*ins, cd.ops.erode3x3(T(mask)), wc, 1)
+    f = cd.ops.erode_temporal_screening(*ins, T(mask), wc, 1)
+    torch.cuda.synchronize()
+    L = cd._lib.lib()
+    try:
+        L.cd_set_persistent_kernels(0)
+        t = cd.ops.erode_temporal_screening(*ins, T(mask), wc, 1)
+        torch.cuda.synchronize()
+    finally:
+        L.cd_set_persistent_kernels(1)
+    assert_equal(N(f[4]), ero, "fused eroded mask")
+    for i in range(5):
+        assert_equal(N(f[i]), N(t[i]), f"fused out{i} vs the tile-per-CTA kernel")
+    for i in range(4):
+        assert_equal(N(f[i]), ro[i], f"fused out{i} vs oracle")
+        assert_equal(N(f[i]), N(o[i]), f"fused out{i} vs two-op sequence")
+    assert L.cd_image_kernel_error_flags() == 0
+
+
 def test_all_rejected_and_all_accepted(cd, cuda):
     c1, c2, prev, p1, p2, mask = inputs(cd, 32, 32, 1, seed=3)
     ins = [T(x) for x in (c1, c2, prev, p1, p2)]

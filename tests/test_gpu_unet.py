@@ -1,6 +1,10 @@
 """The tensor-core U-Net (cd_unet_* and cd_adam_update) against the PyTorch
 restatement oracle/unet_torch.py.
 
+Both forms of the 3x3 convolution kernels (ky-stacked MMAs, the default,
+and one MMA per output row and tap) are checked layer by layer and for the
+whole network.
+
 Tolerances (bf16 operands and stored activations, fp32 accumulation):
   single layer vs the same bf16-rounded operands in fp32:
       max |y - ref| <= 1e-2 * max |ref|   (one bf16 rounding of the output)
@@ -53,8 +57,17 @@ def close_to_max(got, ref, frac, what):
     assert err <= frac * m, f"{what}: max err {err:.4g} > {frac} * max|ref| {m:.4g}"
 
 
+@pytest.fixture(params=[1, 0], ids=["ky_stacked", "per_row"])
+def conv_form(request, cd):
+    """Both forms of the 3x3 convolution kernels (cd_set_unet_conv_stacked)."""
+    L = cd._lib.lib()
+    L.cd_set_unet_conv_stacked(request.param)
+    yield request.param
+    L.cd_set_unet_conv_stacked(1)
+
+
 @pytest.mark.parametrize("cin,cout", LAYER_SHAPES)
-def test_conv3x3_forward(cd, cuda, cin, cout):
+def test_conv3x3_forward(cd, cuda, conv_form, cin, cout):
     g = torch.Generator().manual_seed(cin * 100 + cout)
     B, H, W = 2, 21, 150                       # partial tiles in x and y
     x = bf16(rand_act(B, H, W, cin, g))
@@ -67,7 +80,7 @@ def test_conv3x3_forward(cd, cuda, cin, cout):
 
 
 @pytest.mark.parametrize("cin,cout", LAYER_SHAPES)
-def test_conv3x3_dgrad(cd, cuda, cin, cout):
+def test_conv3x3_dgrad(cd, cuda, conv_form, cin, cout):
     g = torch.Generator().manual_seed(cin * 10 + cout)
     B, H, W = 1, 18, 140
     dz = bf16(torch.randn((B, H, W, (cout + 7) // 8 * 8), generator=g))
@@ -141,7 +154,7 @@ def reference(params, ins, bf16_emulation, gb=None, ga=None):
     return p.grad.double()
 
 
-def test_unet_forward(cd, cuda):
+def test_unet_forward(cd, cuda, conv_form):
     B, H, W = 1, 36, 264
     ins = frame_inputs(B, H, W, 5)
     net = cd.unet.UNet(DEV, seed=3)
@@ -161,7 +174,7 @@ def well_conditioned_net(cd, seed):
     return cd.unet.UNet(DEV, params=p)
 
 
-def test_unet_backward_and_adam(cd, cuda):
+def test_unet_backward_and_adam(cd, cuda, conv_form):
     B, H, W = 1, 64, 264
     ins = frame_inputs(B, H, W, 7)
     net = well_conditioned_net(cd, 4)
