@@ -17,7 +17,6 @@
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
 #include "filter_sweep.cuh"
-#include "tma.cuh"
 
 namespace cd {
 namespace {
@@ -249,10 +248,14 @@ CD_DEV float filter_epilogue(const fsw::Sums &s, const fsw::Centre &c, const Agg
 
 // ---------------------------------------------------------------------------
 // Chosen path: spatial filter + aggregation loss + band gradient in one pass.
-// The window sweep is the forward kernel's (same order, same arithmetic, so
-// the filter sums equal cd_spatial_filter's bit for bit) extended with the
-// band partials of the gradient kernel; the epilogue evaluates the loss and
-// its gradient at the pixel and dots it with the partials.
+// The window sweep is the forward kernel's (same order, same arithmetic)
+// extended with the band partials of the gradient kernel; the epilogue
+// evaluates the loss and its gradient at the pixel and dots it with the
+// partials.  Its weights are exp(e) = 2^(e log2 e) on ex2.approx.ftz
+// (fsw::kExp2Ftz): the same values as the plain kernels' __expf wherever the
+// weight is a normal float, zero where it would be subnormal (below 2^-126),
+// so its sums equal cd_spatial_filter's except for contributions below the
+// smallest normal float.
 // ---------------------------------------------------------------------------
 template <int HW>
 __global__ void __launch_bounds__(256, 3) filter_aggregate_kernel(
@@ -276,168 +279,14 @@ __global__ void __launch_bounds__(256, 3) filter_aggregate_kernel(
         const fsw::Centre c = fsw::centre(tile, hw, band + 5 * p);
         fsw::Sums s;
         fsw::zero(s);
-        fsw::sweep<HW, true, true>(tile, pdtab, hw, c, s);
+        fsw::sweep<HW, true, true, fsw::kExp2Ftz>(tile, pdtab, hw, c, s);
         loss = filter_epilogue(s, c, P, p, gband, inv_n);
     }
     block_partial(loss, P.partial, fsw::kBX * fsw::kBY);
 }
 
 
-// ---------------------------------------------------------------------------
-// Chosen path, persistent form: the same per-pixel work as
-// filter_aggregate_kernel (same records, sweep, epilogue and one loss
-// partial per 32x8 tile, so every output is bit-identical to it), with each
-// CTA walking the tiles with stride gridDim.x and the next tile's footprint
-// of the four images (the window's halo included) arriving by TMA while the
-// current tile is swept.  The copies land as raw NHWC rows; a repack pass
-// (shared memory to shared memory) forms the records, taking the reflect-101
-// neighbours from inside the box.  Three CTAs per SM.
-// ---------------------------------------------------------------------------
-template <int HW>
-struct FaGeom {
-    static constexpr int TW = fsw::kBX + 2 * HW, TH = fsw::kBY + 2 * HW;
-    static constexpr int OFF = (4 - (3 * HW) % 4) % 4;          // first float of the footprint in a box row
-    static constexpr int BOXW = (3 * TW + OFF + 3) & ~3;
-    static constexpr int PLANE = ((TH * BOXW * 4 + 127) / 128) * 128;
-    static constexpr int RAW = 4 * PLANE;
-    static constexpr int TX_BYTES = 4 * TH * BOXW * 4;
-    static constexpr int REC = 3 * TW * TH * 16;
-    static constexpr int PD = (2 * HW + 1) * (2 * HW + 1) * 8;
-    static constexpr int SMEM = RAW + REC + PD + 16;
-};
-
-struct FaMaps {
-    CUtensorMap ia, ib, al, nr;
-};
-
-__device__ int g_filter_stage_error = 0;   // sticky: a staging wait ran out
-
-template <int HW>
-__global__ void __launch_bounds__(256, 3) filter_aggregate_tma_kernel(
-    const __grid_constant__ FaMaps maps, const float *__restrict__ band, AggPtrs P, float *__restrict__ gband,
-    int H, int W, int ntx, int nty, int ntiles, float inv_n)
-{
-    using G = FaGeom<HW>;
-    extern __shared__ __align__(128) unsigned char smem[];
-    ulonglong2 *tile = reinterpret_cast<ulonglong2 *>(smem + G::RAW);
-    fsw::f2 *pdtab = reinterpret_cast<fsw::f2 *>(smem + G::RAW + G::REC);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + G::RAW + G::REC + G::PD);
-    const int tid = threadIdx.y * fsw::kBX + threadIdx.x;
-    const int per_img = ntx * nty;
-    const size_t px = (size_t)H * W;
-
-    auto issue = [&](int t) {
-        const int b = t / per_img, r = t - b * per_img, by = r / ntx, bx = r - by * ntx;
-        const int xc = tma::floor_to(3 * (bx * fsw::kBX - HW), 4), yc = by * fsw::kBY - HW;
-        tc::mbar_expect_tx(bar, G::TX_BYTES);
-        tma::load3(smem, &maps.ia, xc, yc, b, bar);
-        tma::load3(smem + G::PLANE, &maps.ib, xc, yc, b, bar);
-        tma::load3(smem + 2 * G::PLANE, &maps.al, xc, yc, b, bar);
-        tma::load3(smem + 3 * G::PLANE, &maps.nr, xc, yc, b, bar);
-    };
-
-    if (tid == 0) tc::mbar_init(bar, 1);
-    {
-        // pd(ky, kx), rounded as fsw::stage rounds it
-        const int w = 2 * HW + 1;
-        for (int k = tid; k < w * w; k += fsw::kBX * fsw::kBY) {
-            const int ky = k / w, kx = k - ky * w;
-            const float dy = (float)(HW - ky) / (float)HW, dx = (float)(HW - kx) / (float)HW;
-            const float pd = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
-            pdtab[k] = fsw::pack(pd, pd);
-        }
-    }
-    __syncthreads();
-    if (tid == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x);
-    uint32_t phase = 0;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int b = t / per_img, rr = t - b * per_img, by = rr / ntx, bx = rr - by * ntx;
-        const bool landed = __syncthreads_and(tc::mbar_wait(bar, phase, 1 << 22)) != 0;
-        phase ^= 1u;
-        if (!landed) {
-            if (tid == 0) atomicOr(&g_filter_stage_error, 1);
-            return;
-        }
-        // raw rows -> records (reflect-101; every neighbour a centre of the
-        // tile reads lies inside the box, other positions are clamped into it)
-        const int x0 = bx * fsw::kBX - HW, y0 = by * fsw::kBY - HW;
-        const int xa = tma::floor_to(3 * x0, 4);
-        const float *ra = reinterpret_cast<const float *>(smem);
-        for (int q = tid; q < G::TW * G::TH; q += fsw::kBX * fsw::kBY) {
-            const int ty = q / G::TW, tx = q - ty * G::TW;
-            const int gx = min(max(mirror(x0 + tx, W), 0), W - 1);
-            const int gy = min(max(mirror(y0 + ty, H), 0), H - 1);
-            const int rx = min(max(3 * gx - xa, 0), G::BOXW - 3), ry = min(max(gy - y0, 0), G::TH - 1);
-            const float *a = ra + ry * G::BOXW + rx;
-            const float *c = a + G::PLANE / 4, *l = a + G::PLANE / 2, *n = a + 3 * (G::PLANE / 4);
-            tile[3 * q + 0] = make_ulonglong2(fsw::pack(a[0], c[0]), fsw::pack(a[1], c[1]));
-            tile[3 * q + 1] = make_ulonglong2(fsw::pack(a[2], c[2]), fsw::pack(l[0], n[0]));
-            tile[3 * q + 2] = make_ulonglong2(fsw::pack(l[1], n[1]), fsw::pack(l[2], n[2]));
-        }
-        __syncthreads();   // records ready; the raw rows are free for the next tile
-        if (tid == 0 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x);
-
-        const int cx = bx * fsw::kBX + threadIdx.x, cy = by * fsw::kBY + threadIdx.y;
-        float loss = 0.f;
-        if (cx < W && cy < H) {
-            const size_t p = b * px + (size_t)cy * W + cx;
-            const fsw::Centre c = fsw::centre(tile, HW, band + 5 * p);
-            fsw::Sums s;
-            fsw::zero(s);
-            fsw::sweep<HW, true, true>(tile, pdtab, HW, c, s);
-            loss = filter_epilogue(s, c, P, p, gband, inv_n);
-        }
-        block_partial_at(loss, P.partial, t, fsw::kBX * fsw::kBY);   // ends with a barrier
-    }
-}
-
-template <int HW>
-cudaError_t launch_filter_aggregate_tma(const float *imga, const float *imgb, const float *albedo,
-                                        const float *normal, const float *band, const AggPtrs &P, float *gband,
-                                        int B, int H, int W, float inv_n, cudaStream_t st, bool *done)
-{
-    using G = FaGeom<HW>;
-    *done = false;
-    FaMaps m;
-    if (!tma::encode_image(&m.ia, imga, false, 3, W, H, B, G::BOXW, G::TH) ||
-        !tma::encode_image(&m.ib, imgb, false, 3, W, H, B, G::BOXW, G::TH) ||
-        !tma::encode_image(&m.al, albedo, false, 3, W, H, B, G::BOXW, G::TH) ||
-        !tma::encode_image(&m.nr, normal, false, 3, W, H, B, G::BOXW, G::TH))
-        return cudaSuccess;   // not eligible: the caller takes the tile-per-CTA kernel
-    static int occ[8] = {};
-    static int sms[64] = {};
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(filter_aggregate_tma_kernel<HW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  G::SMEM)) != cudaSuccess)
-        return e;
-    if (!occ[HW]) {
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[HW], filter_aggregate_tma_kernel<HW>,
-                                                                fsw::kBX * fsw::kBY, G::SMEM)) != cudaSuccess)
-            return e;
-        if (occ[HW] < 1) return cudaSuccess;
-    }
-    if (dev < 64 && !sms[dev] &&
-        (e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
-        return e;
-    const int nsm = dev < 64 ? sms[dev] : 148;
-    const int ntx = (W + fsw::kBX - 1) / fsw::kBX, nty = (H + fsw::kBY - 1) / fsw::kBY, ntiles = ntx * nty * B;
-    const int grid = min(ntiles, nsm * occ[HW]);
-    filter_aggregate_tma_kernel<HW><<<grid, dim3(fsw::kBX, fsw::kBY), G::SMEM, st>>>(m, band, P, gband, H, W, ntx,
-                                                                                     nty, ntiles, inv_n);
-    *done = true;
-    return cudaGetLastError();
-}
-
 }  // namespace
-
-int filter_stage_error_flag()
-{
-    int v = 0;
-    if (cudaMemcpyFromSymbol(&v, g_filter_stage_error, sizeof(int)) != cudaSuccess) return -1;
-    return v;
-}
 
 size_t aggregation_partials(int B, int H, int W) { return (size_t)((W + 31) / 32) * ((H + 7) / 8) * B; }
 
@@ -489,12 +338,8 @@ cudaError_t launch_filter_aggregate(const float *imga, const float *imgb, const 
         kern<<<grid, block, smem, st>>>(imga, imgb, albedo, normal, band, P, gband, H, W, hw, inv_n);
         return cudaGetLastError();
     };
-    cudaError_t e = cudaSuccess;
-    bool done = false;
-    if (hw == 5 && tma::persistent_enabled())
-        e = launch_filter_aggregate_tma<5>(imga, imgb, albedo, normal, band, P, gband, B, H, W, inv_n, st, &done);
-    if (e != cudaSuccess) return e;
-    if (!done) switch (hw) {
+    cudaError_t e;
+    switch (hw) {
     case 3: e = go(filter_aggregate_kernel<3>); break;
     case 5: e = go(filter_aggregate_kernel<5>); break;
     case 7: e = go(filter_aggregate_kernel<7>); break;

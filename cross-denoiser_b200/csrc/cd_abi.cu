@@ -56,9 +56,8 @@ int cd_abi_version(void) { return 1; }
 
 int cd_image_kernel_error_flags(void)
 {
-    const int t = cd::temporal_error_flag(), f = cd::filter_stage_error_flag();
-    if (t < 0 || f < 0) return -1;
-    return (t ? 1 : 0) | (f ? 2 : 0);
+    const int t = cd::temporal_error_flag();
+    return t < 0 ? -1 : (t ? 1 : 0);
 }
 
 void cd_set_persistent_kernels(int enable) { cd::tma::set_persistent_enabled(enable != 0); }

@@ -102,7 +102,6 @@ cudaError_t launch_temporal(const float *c1, const float *c2, const float *prev,
 // Sticky error bits of the persistent TMA image kernels (a staging wait ran
 // out), read synchronously; -1 if the read fails.
 int temporal_error_flag();
-int filter_stage_error_flag();
 
 // Records msg as the calling thread's cd_get_last_error() message.
 void set_last_error(const char *msg);

@@ -98,7 +98,25 @@ struct Sums {
     f2 px[4], py[4], pz[4], pw[4];
 };
 
-template <bool kAcc, bool kPar>
+// How the sweep evaluates a tap's weight exp(e), e <= 0:
+//   kExpf     __expf, as the reference's kernel (ops/regression.cu.cc:149-150)
+//   kExp2Ftz  2^(e * log2(e)) on the ex2.approx.ftz instruction: the same
+//             values wherever exp(e) is a normal float, zero below 2^-126
+//             (measured 6 % faster on the fused 11x11 sweep at 1080p)
+constexpr int kExpf = 0, kExp2Ftz = 1;
+
+template <int kExp>
+CD_DEV float weight_exp(float e)
+{
+    if (kExp == kExp2Ftz) {
+        float y;
+        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(e * 1.44269504088896341f));
+        return y;
+    }
+    return __expf(e);
+}
+
+template <bool kAcc, bool kPar, int kExp = kExpf>
 CD_DEV void tap(const ulonglong2 *rec, f2 pd2, const Centre &c, Sums &s)
 {
     const ulonglong2 r0 = rec[0], r1 = rec[1], r2 = rec[2];
@@ -113,7 +131,7 @@ CD_DEV void tap(const ulonglong2 *rec, f2 pd2, const Centre &c, Sums &s)
     // rounded as the compiled reference: the first product fused with the
     // rounded second, the later products fused into the running sum
     const f2 e = fma2(c.nb4, pd2, fma2(c.nb3, dn2, fma2(c.nb01, dAB, mul2(c.nb2, dal2))));
-    const f2 w = pack(__expf(lo(e)), __expf(hi(e)));
+    const f2 w = pack(weight_exp<kExp>(lo(e)), weight_exp<kExp>(hi(e)));
     if (kAcc) {
         const f2 col_x = r0.x, col_y = r0.y, col_z = r1.x;
         s.acc_x = fma2(w, col_x, s.acc_x);
@@ -136,7 +154,7 @@ CD_DEV void tap(const ulonglong2 *rec, f2 pd2, const Centre &c, Sums &s)
 
 // Sweep the (2hw+1)^2 window of the thread's pixel.  HW > 0 fixes the
 // radius at compile time (fully unrolled rows); HW == 0 takes it at run time.
-template <int HW, bool kAcc, bool kPar>
+template <int HW, bool kAcc, bool kPar, int kExp = kExpf>
 CD_DEV void sweep(const ulonglong2 *tile, const f2 *pdtab, int hw_rt, const Centre &c, Sums &s)
 {
     const int hw = HW > 0 ? HW : hw_rt;
@@ -146,9 +164,9 @@ CD_DEV void sweep(const ulonglong2 *tile, const f2 *pdtab, int hw_rt, const Cent
         const f2 *pdrow = pdtab + ky * w;
         if (HW > 0) {
 #pragma unroll
-            for (int kx = 0; kx < 2 * HW + 1; ++kx) tap<kAcc, kPar>(row + 3 * kx, pdrow[kx], c, s);
+            for (int kx = 0; kx < 2 * HW + 1; ++kx) tap<kAcc, kPar, kExp>(row + 3 * kx, pdrow[kx], c, s);
         } else {
-            for (int kx = 0; kx < w; ++kx) tap<kAcc, kPar>(row + 3 * kx, pdrow[kx], c, s);
+            for (int kx = 0; kx < w; ++kx) tap<kAcc, kPar, kExp>(row + 3 * kx, pdrow[kx], c, s);
         }
     }
 }

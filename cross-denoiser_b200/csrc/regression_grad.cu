@@ -77,14 +77,17 @@ CD_DEV void recon_pair(float3 fp, float3 fc, float sp_, float sc, float vp, floa
     const float dav[3] = {da.x, da.y, da.z}, dnv[3] = {dn.x, dn.y, dn.z};
     const float den = (sp_ + sc) + 1e-2f;
     const float V = (vp + vc) + 1e-4f;
-    const float dist = (df[0] * df[0] + df[1] * df[1] + df[2] * df[2]) / V;
+    // the pair's quotients share two denominators (den >= 1e-2, V >= 1e-4):
+    // one reciprocal each (about 2 ulp) instead of a division per quotient
+    const float rden = __fdividef(1.f, den), rV = __fdividef(1.f, V);
+    const float dist = (df[0] * df[0] + df[1] * df[1] + df[2] * df[2]) * rV;
     const float e = __expf(-dist);
     g.w = e + 1e-7f;
     float gw = gD, gd1[3], gdn[3] = {0.f, 0.f, 0.f}, d1[3];
     float gda_[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        d1[k] = df[k] / den;
+        d1[k] = df[k] * rden;
         const float *bk = beta;   // layout r * 3 + k
         float pr = bk[k] + bk[3 + k] * d1[k] + bk[6 + k] * dav[k] + bk[9 + k] * dnv[0] + bk[12 + k] * dnv[1] +
                    bk[15 + k] * dnv[2];
@@ -106,10 +109,10 @@ CD_DEV void recon_pair(float3 fp, float3 fc, float sp_, float sc, float vp, floa
         }
     }
     const float gdist = -gw * e;
-    g.gdf = make_float3(gd1[0] / den + gdist * 2.f * df[0] / V, gd1[1] / den + gdist * 2.f * df[1] / V,
-                        gd1[2] / den + gdist * 2.f * df[2] / V);
-    g.gden = -(gd1[0] * d1[0] + gd1[1] * d1[1] + gd1[2] * d1[2]) / den;
-    g.gV = -gdist * dist / V;
+    const float t = 2.f * gdist * rV;
+    g.gdf = make_float3(gd1[0] * rden + t * df[0], gd1[1] * rden + t * df[1], gd1[2] * rden + t * df[2]);
+    g.gden = -(gd1[0] * d1[0] + gd1[1] * d1[1] + gd1[2] * d1[2]) * rden;
+    g.gV = -gdist * dist * rV;
     g.gda = make_float3(gda_[0], gda_[1], gda_[2]);
     g.gdn = make_float3(gdn[0], gdn[1], gdn[2]);
 }
@@ -216,6 +219,26 @@ __global__ void __launch_bounds__(256) recon_grad_centre_kernel(GArgs A)
     const size_t ci = b * C + (size_t)j * A.Ws + i;
     const int ox0 = max(0, (i * A.sp - A.hw - A.sp) / A.rs), ox1 = min(A.Wr - 1, (i * A.sp + A.hw + A.sp) / A.rs);
     const int oy0 = max(0, (j * A.sp - A.hw - A.sp) / A.rs), oy1 = min(A.Hr - 1, (j * A.sp + A.hw + A.sp) / A.rs);
+    // the output pixels whose centre range contains (i, j): both ends of a
+    // pixel's range are non-decreasing in the pixel's position, so along
+    // each axis they form one interval, found once per axis
+    int vx0 = ox1 + 1, vx1 = ox0 - 1, vy0 = oy1 + 1, vy1 = oy0 - 1;
+    for (int ox = ox0; ox <= ox1; ++ox) {
+        int sx, ex;
+        centre_range(ox * A.rs, A.W, A.hw, A.sp, sx, ex);
+        if (i >= sx && i <= ex) {
+            vx0 = min(vx0, ox);
+            vx1 = max(vx1, ox);
+        }
+    }
+    for (int oy = oy0; oy <= oy1; ++oy) {
+        int sy, ey;
+        centre_range(oy * A.rs, A.H, A.hw, A.sp, sy, ey);
+        if (j >= sy && j <= ey) {
+            vy0 = min(vy0, oy);
+            vy1 = max(vy1, oy);
+        }
+    }
     const float3 ac = f3(A.alb, c), nc = f3(A.nrm, c);
     float3 galb = make_float3(0.f, 0.f, 0.f), gnn = galb;
     for (int X = 0; X < 2; ++X) {
@@ -229,14 +252,8 @@ __global__ void __launch_bounds__(256) recon_grad_centre_kernel(GArgs A)
         float3 gf = make_float3(0.f, 0.f, 0.f);
         float gs = 0.f, gv = 0.f;
         PairGrad g;
-        for (int oy = oy0; oy <= oy1; ++oy) {
-            int sy, ey;
-            centre_range(oy * A.rs, A.H, A.hw, A.sp, sy, ey);
-            if (j < sy || j > ey) continue;
-            for (int ox = ox0; ox <= ox1; ++ox) {
-                int sx, ex;
-                centre_range(ox * A.rs, A.W, A.hw, A.sp, sx, ex);
-                if (i < sx || i > ex) continue;
+        for (int oy = vy0; oy <= vy1; ++oy) {
+            for (int ox = vx0; ox <= vx1; ++ox) {
                 const size_t p = b * P + (size_t)(oy * A.rs) * A.W + ox * A.rs;
                 const size_t o = b * R + (size_t)oy * A.Wr + ox;
                 const float3 ap = f3(A.alb, p), np_ = f3(A.nrm, p);
@@ -285,13 +302,14 @@ CD_DEV void regression_tap(float3 ft, float3 fc, float3 yt, float st, float sc, 
     const float yv[3] = {yt.x, yt.y, yt.z};
     const float den = (sc + st) + 1e-2f;
     const float V = (vc + vt) + 1e-4f;
-    const float dist = (df[0] * df[0] + df[1] * df[1] + df[2] * df[2]) / V;
+    const float rden = __fdividef(1.f, den), rV = __fdividef(1.f, V);   // as in recon_pair
+    const float dist = (df[0] * df[0] + df[1] * df[1] + df[2] * df[2]) * rV;
     const float e = __expf(-dist);
     const float w = e + 1e-7f;
     float gw = 0.f, gd1[3], gda[3], gdn[3] = {0.f, 0.f, 0.f}, d1[3], gyv[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        d1[k] = df[k] / den;
+        d1[k] = df[k] * rden;
         const float dl[kP] = {1.f, d1[k], dav[k], dnv[0], dnv[1], dnv[2]};
         float a = 0.f, c = 0.f;
 #pragma unroll
@@ -310,10 +328,10 @@ CD_DEV void regression_tap(float3 ft, float3 fc, float3 yt, float st, float sc, 
         gdn[2] += w * (u[15 + k] * res - a * beta[15 + k]);
     }
     const float gdist = -gw * e;
-    g.gdf = make_float3(gd1[0] / den + gdist * 2.f * df[0] / V, gd1[1] / den + gdist * 2.f * df[1] / V,
-                        gd1[2] / den + gdist * 2.f * df[2] / V);
-    g.gden = -(gd1[0] * d1[0] + gd1[1] * d1[1] + gd1[2] * d1[2]) / den;
-    g.gV = -gdist * dist / V;
+    const float t = 2.f * gdist * rV;
+    g.gdf = make_float3(gd1[0] * rden + t * df[0], gd1[1] * rden + t * df[1], gd1[2] * rden + t * df[2]);
+    g.gden = -(gd1[0] * d1[0] + gd1[1] * d1[1] + gd1[2] * d1[2]) * rden;
+    g.gV = -gdist * dist * rV;
     g.gy = make_float3(gyv[0], gyv[1], gyv[2]);
     g.gda = make_float3(gda[0], gda[1], gda[2]);
     g.gdn = make_float3(gdn[0], gdn[1], gdn[2]);

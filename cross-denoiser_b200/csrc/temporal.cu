@@ -22,8 +22,8 @@
 // colour footprints with the window's halo, the three history buffers and
 // the raw mask with a one-pixel halo) arrive by TMA into a double buffer
 // while the current tile computes, so the DRAM latency is off the critical
-// path.  Its row pass slides the window over four output columns per thread
-// in registers.  Other window sizes and images whose rows are not a multiple
+// path.  Its row pass slides the window over four output columns per
+// (channel, row, column group) item, in registers, on all threads.  Other window sizes and images whose rows are not a multiple
 // of 16 bytes take the tile-per-CTA kernel above it.
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
@@ -368,37 +368,36 @@ __global__ void __launch_bounds__(kTX * kTY, 2) temporal_tma_kernel(
         const float *H1 = H0 + kTY * G::HBOX, *H2 = H1 + kTY * G::HBOX;
         const unsigned char *MK = smem + s * G::STAGE + 2 * G::CBYTES + 3 * G::HBYTES;
 
-        // row pass: item (r, q) = tile row r, output columns 4q .. 4q + 3
-        if (tid < G::TH * (kTX / 4)) {
-            const int r = tid >> 3, q = tid & 7;
+        // row pass: item (c, r, q) = channel c, tile row r, output columns
+        // 4q .. 4q + 3: the channel's current1 and current2 values of the
+        // segment are loaded once and give all three quantities (current1,
+        // current2, their average); 3 * TH * 8 items over all threads
+        for (int it = tid; it < 3 * G::TH * 8; it += kTX * kTY) {
+            const int q = it & 7, rc = it >> 3, c = rc % 3, r = rc / 3;
             const int gy = by * kTY - HC + r;
             const int gx0 = bx * kTX - HC + 4 * q;
             const bool row_in = gy >= 0 && gy < H;
             const bool all_in = row_in && gx0 >= 0 && gx0 + G::NJ <= W;
-            const float *c1r = C1 + r * G::BOXC + G::OFF + 12 * q;
-            const float *c2r = C2 + r * G::BOXC + G::OFF + 12 * q;
+            const int o = r * G::BOXC + G::OFF + 12 * q + c;
+            float a[G::NJ], bb[G::NJ], v[G::NJ];
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                float a[G::NJ], bb[G::NJ], v[G::NJ];
-#pragma unroll
-                for (int j = 0; j < G::NJ; ++j) {
-                    const bool in = all_in || (row_in && gx0 + j >= 0 && gx0 + j < W);
-                    a[j] = in ? c1r[3 * j + c] : qnan;
-                    bb[j] = in ? c2r[3 * j + c] : qnan;
-                    v[j] = (a[j] + bb[j]) * 0.5f;
-                }
-                float mn[4], mx[4];
-                const int o = r * kTX + 4 * q;
-                window4<HC>(a, mn, mx);
-                *reinterpret_cast<float4 *>(rmin + c * G::TH * kTX + o) = make_float4(mn[0], mn[1], mn[2], mn[3]);
-                *reinterpret_cast<float4 *>(rmax + c * G::TH * kTX + o) = make_float4(mx[0], mx[1], mx[2], mx[3]);
-                window4<HC>(bb, mn, mx);
-                *reinterpret_cast<float4 *>(rmin + (3 + c) * G::TH * kTX + o) = make_float4(mn[0], mn[1], mn[2], mn[3]);
-                *reinterpret_cast<float4 *>(rmax + (3 + c) * G::TH * kTX + o) = make_float4(mx[0], mx[1], mx[2], mx[3]);
-                window4<HC>(v, mn, mx);
-                *reinterpret_cast<float4 *>(rmin + (6 + c) * G::TH * kTX + o) = make_float4(mn[0], mn[1], mn[2], mn[3]);
-                *reinterpret_cast<float4 *>(rmax + (6 + c) * G::TH * kTX + o) = make_float4(mx[0], mx[1], mx[2], mx[3]);
+            for (int j = 0; j < G::NJ; ++j) {
+                const bool in = all_in || (row_in && gx0 + j >= 0 && gx0 + j < W);
+                a[j] = in ? C1[o + 3 * j] : qnan;
+                bb[j] = in ? C2[o + 3 * j] : qnan;
+                v[j] = (a[j] + bb[j]) * 0.5f;
             }
+            float mn[4], mx[4];
+            const int d = r * kTX + 4 * q;
+            window4<HC>(a, mn, mx);
+            *reinterpret_cast<float4 *>(rmin + c * G::TH * kTX + d) = make_float4(mn[0], mn[1], mn[2], mn[3]);
+            *reinterpret_cast<float4 *>(rmax + c * G::TH * kTX + d) = make_float4(mx[0], mx[1], mx[2], mx[3]);
+            window4<HC>(bb, mn, mx);
+            *reinterpret_cast<float4 *>(rmin + (3 + c) * G::TH * kTX + d) = make_float4(mn[0], mn[1], mn[2], mn[3]);
+            *reinterpret_cast<float4 *>(rmax + (3 + c) * G::TH * kTX + d) = make_float4(mx[0], mx[1], mx[2], mx[3]);
+            window4<HC>(v, mn, mx);
+            *reinterpret_cast<float4 *>(rmin + (6 + c) * G::TH * kTX + d) = make_float4(mn[0], mn[1], mn[2], mn[3]);
+            *reinterpret_cast<float4 *>(rmax + (6 + c) * G::TH * kTX + d) = make_float4(mx[0], mx[1], mx[2], mx[3]);
         }
         __syncthreads();
 

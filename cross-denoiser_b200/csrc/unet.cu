@@ -126,6 +126,8 @@ struct Ctx {
     cudaStream_t st;
     const float *params;
     bool stacked = conv_stacked_enabled();   // the convolution form of this call (packing and kernels agree)
+    // the ky-stacked form where it measured faster: 16 conv output channels
+    bool stacked_for(int nout) const { return stacked && nout == 16; }
     __nv_bfloat16 *buf(Buf b) const { return reinterpret_cast<__nv_bfloat16 *>(ws + L.buf[b]); }
     int *err() const { return reinterpret_cast<int *>(ws); }
     float *partial() const { return reinterpret_cast<float *>(ws + L.partial); }
@@ -150,10 +152,11 @@ cudaError_t pack_all(const Ctx &c, bool dgrad)
         if (d.kind != CONV) continue;
         PackJob &j = J.job[J.n++];
         KStep st[kMaxSteps];
-        auto steps = c.stacked ? build_steps_stacked : build_steps;
+        const int nout = nout_of(dgrad ? d.cin : d.cout);
+        auto steps = c.stacked_for(nout) ? build_steps_stacked : build_steps;
         j.T.nsteps = dgrad ? steps(chunks(d.cout), 0, st, j.T.half) : steps(kSrc0[l], kSrc1[l], st, j.T.half);
-        j.T.stacked = c.stacked ? 1 : 0;
-        j.T.nout = nout_of(dgrad ? d.cin : d.cout);
+        j.T.stacked = c.stacked_for(nout) ? 1 : 0;
+        j.T.nout = nout;
         j.T.cin = d.cin;
         j.T.cout = d.cout;
         j.T.dgrad = dgrad ? 1 : 0;
@@ -170,8 +173,9 @@ cudaError_t conv(const Ctx &c, int l, bool dgrad, int lvl, Buf s0, int c0, Buf s
     const LayerDef &d = kDef[l];
     ConvParams P{};
     StepHalf hf[kMaxSteps][2];
-    P.nsteps = (c.stacked ? build_steps_stacked : build_steps)(c0, c1, P.steps, hf);
-    P.stacked = c.stacked ? 1 : 0;
+    const bool stacked = c.stacked_for(nout_of(dgrad ? d.cin : d.cout));
+    P.nsteps = (stacked ? build_steps_stacked : build_steps)(c0, c1, P.steps, hf);
+    P.stacked = stacked ? 1 : 0;
     P.src0 = c.buf(s0);
     P.src1 = c1 ? c.buf(s1) : nullptr;
     P.c0 = c0;
@@ -359,7 +363,7 @@ cudaError_t conv_layer(const float *w, const float *bias, const __nv_bfloat16 *x
     uint8_t *base = static_cast<uint8_t *>(ws);
     __nv_bfloat16 *wp = reinterpret_cast<__nv_bfloat16 *>(base + 256);
     const int in_ch = dgrad ? cout : cin, out_ch = dgrad ? cin : cout;
-    const bool stacked = conv_stacked_enabled();
+    const bool stacked = conv_stacked_enabled() && nout_of(out_ch) == 16;   // as Ctx::stacked_for
     auto steps = stacked ? build_steps_stacked : build_steps;
     PackTable T{};
     KStep st_[kMaxSteps];

@@ -190,6 +190,24 @@ class Server:
         gc.collect()
         torch.cuda.synchronize(self.device)
 
+    def admit_all(self) -> int:
+        """Admit every stream that fits the budget now, in stream order;
+        returns how many are resident."""
+        for sid in range(len(self.res)):
+            if sid not in self.sessions and sid not in self.retired and not self._admit(sid):
+                break
+        return len(self.sessions)
+
+    def warm(self, frames: int = 2):
+        """Run the first `frames` frames of every resident stream (the eager
+        first frame that allocates the stream's buffers, the graph capture)
+        outside any timed region; run() then continues from frame `frames`."""
+        for s in self.sessions.values():
+            for t in range(frames):
+                s.launch(t)
+        if torch.cuda.is_available():
+            torch.cuda.synchronize(self.device)
+
     def _estimate(self, sid):
         H, W = self.res[sid]
         return self.measured.get((H, W), EST_BYTES_PER_PX * H * W)
@@ -216,7 +234,8 @@ class Server:
         pending: Dict[int, List[Request]] = {}
         for q in schedule:
             pending.setdefault(q.stream_id, []).append(q)
-        waiting = sorted(pending, key=lambda sid: pending[sid][0].arrival)
+        waiting = sorted((sid for sid in pending if sid not in self.sessions),
+                         key=lambda sid: pending[sid][0].arrival)
         results: List[Result] = []
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0
@@ -255,18 +274,26 @@ class Server:
 
 
 def summarize(results: List[Result], resolutions) -> dict:
+    """Throughput over the span of the results, latency from arrival to the
+    denoised frame (queueing included) and service time from dispatch to the
+    denoised frame, overall and per resolution."""
     lat = np.array([r.latency for r in results]) * 1e3
+    svc = np.array([r.done - r.start for r in results]) * 1e3
     span = max(r.done for r in results) - min(min(r.start for r in results), min(r.arrival for r in results))
     by_res = {}
     for (H, W) in sorted(set(resolutions)):
         ls = np.array([r.latency for r in results if resolutions[r.stream_id] == (H, W)]) * 1e3
+        ss = np.array([r.done - r.start for r in results if resolutions[r.stream_id] == (H, W)]) * 1e3
         by_res[f"{W}x{H}"] = {"frames": int(ls.size), "p50_ms": round(float(np.percentile(ls, 50)), 3),
-                              "p99_ms": round(float(np.percentile(ls, 99)), 3)}
+                              "p99_ms": round(float(np.percentile(ls, 99)), 3),
+                              "service_p50_ms": round(float(np.percentile(ss, 50)), 3),
+                              "service_p99_ms": round(float(np.percentile(ss, 99)), 3)}
     px = sum(resolutions[r.stream_id][0] * resolutions[r.stream_id][1] for r in results)
     return {"frames": len(results), "seconds": round(span, 3), "frames_per_s": round(len(results) / span, 2),
             "megapixels_per_s": round(px / span / 1e6, 1),
             "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
-            "by_resolution": by_res}
+            "service_p50_ms": round(float(np.percentile(svc, 50)), 3),
+            "service_p99_ms": round(float(np.percentile(svc, 99)), 3), "by_resolution": by_res}
 
 
 def device_frame_source(resolutions, seeds, device, pool: int = 4):

@@ -393,8 +393,10 @@ CD_API cd_status cd_unet_conv3x3(const float *weight, const float *bias, const v
                                  void *workspace, size_t workspace_bytes, cudaStream_t stream);
 /* Form of the 3x3 convolutions (forward and dgrad; no counterpart in the   */
 /* reference), process-wide, read at the start of each call: 1 (default) =  */
-/* ky-stacked, one MMA per input row and K step accumulating into three     */
-/* output rows' accumulators; 0 = one MMA per output row, tap and K step.   */
+/* ky-stacked for layers with 16 conv output channels (one MMA per input    */
+/* row and K step accumulating into three output rows' accumulators; the   */
+/* measured faster form there), one MMA per output row, tap and K step for  */
+/* the others; 0 = one MMA per output row, tap and K step everywhere.       */
 /* Same arithmetic per output (bf16 products, fp32 sums), sums in another   */
 /* order.                                                                    */
 CD_API void cd_set_unet_conv_stacked(int enable);
@@ -414,16 +416,15 @@ CD_API cd_status cd_unet_conv3x3_wgrad(const void *x, const void *dz, float *gra
 CD_API cd_status cd_fp32_fma_probe(float *out, int blocks, int iters, cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
-/* Persistent image kernels (no counterpart in the reference).  The fused   */
-/* erosion + temporal screening (win_prev = 1) and the fused filter +       */
-/* aggregation (win_size = 11) run as persistent kernels that stage their   */
-/* tiles by TMA and wait on an mbarrier with a bounded number of polls,     */
-/* when the images' rows are a multiple of 16 bytes (the mask's for the     */
-/* screening) and the tensors 16-byte aligned; otherwise, or when disabled  */
-/* here, the tile-per-CTA kernels run.  Both give the same results.         */
-/* cd_image_kernel_error_flags: bit 0 = a screening staging wait ran out,   */
-/* bit 1 = a filter staging wait ran out (the tile's outputs are then not   */
-/* written); the bits only grow.  Read synchronously; -1 if the read fails. */
+/* Persistent image kernel (no counterpart in the reference).  The fused    */
+/* erosion + temporal screening with win_prev = 1 runs as a persistent      */
+/* kernel that stages its tiles by TMA and waits on an mbarrier with a      */
+/* bounded number of polls, when the images' rows (and the mask's) are a    */
+/* multiple of 16 bytes and the tensors 16-byte aligned; otherwise, or when */
+/* disabled here, the tile-per-CTA kernel runs.  Both give the same results.*/
+/* cd_image_kernel_error_flags: bit 0 = a screening staging wait ran out    */
+/* (the tile's outputs are then not written); the bit only grows.  Read     */
+/* synchronously; -1 if the read fails.                                     */
 /* ------------------------------------------------------------------------ */
 CD_API int cd_image_kernel_error_flags(void);
 CD_API void cd_set_persistent_kernels(int enable);

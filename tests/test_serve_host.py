@@ -105,3 +105,21 @@ def test_session_failure_stops_the_loop():
     import pytest
     with pytest.raises(Boom):
         srv.run(serve.poisson_schedule([50.0, 50.0], 4, seed=2), 4, realtime=False)
+
+
+def test_admit_all_and_warm_then_run():
+    """Streams admitted and warmed before the timed run continue from the
+    warm frames: run() serves only the later frames, in order, and retires
+    every stream."""
+    FakeSession.log = []
+    res = [(8, 8)] * 3
+    srv = serve.Server(res, lambda sid, t: None, "cpu", hbm_budget=1 << 30, session_factory=FakeSession,
+                       memory_probe=lambda: 0)
+    assert srv.admit_all() == 3
+    srv.warm(2)
+    sched = [q for q in serve.poisson_schedule([40.0] * 3, 5, seed=4) if q.frame >= 2]
+    results = srv.run(sched, 5, realtime=False)
+    assert sorted((r.stream_id, r.frame) for r in results) == [(s, t) for s in range(3) for t in range(2, 5)]
+    assert all(("admit", s) in FakeSession.log for s in range(3))
+    assert [e for e in FakeSession.log if e[0] == "admit"] == [("admit", 0), ("admit", 1), ("admit", 2)]
+    assert set(srv.retired) == {0, 1, 2}
