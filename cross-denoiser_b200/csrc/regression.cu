@@ -394,6 +394,15 @@ template <int N> CD_DEV void cp_async_wait() { asm volatile("cp.async.wait_group
 
 CD_DEV int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
 
+// exp(x) = 2^(x log2 e) on the ex2.approx.ftz instruction (subnormal results
+// flushed to zero).
+CD_DEV float exp_ftz(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x * 1.44269504088896341f));
+    return y;
+}
+
 __global__ void __launch_bounds__(kThreads, 8) regression_kernel(
     const float *__restrict__ imga, const float *__restrict__ imgb,
     const float *__restrict__ albedo, const float *__restrict__ normal,
@@ -617,7 +626,10 @@ __global__ void __launch_bounds__(kRX * kRY) recon_kernel(
             const f2 rden = pack(__fdividef(1.f, lo(den_r)), __fdividef(1.f, hi(den_r)));
             const f2 den_w = add2(add2(pvar, F10.y), k1e4);
             const f2 q = mul2(sqnorm2(d0, d1, d2), pack(__fdividef(1.f, lo(den_w)), __fdividef(1.f, hi(den_w))));
-            const f2 w = add2(pack(__expf(-lo(q)), __expf(-hi(q))), k1e7);
+            // exp(-q) + 1e-7 with exp as 2^(-q log2 e) on ex2.approx.ftz: the
+            // same weight as __expf wherever exp(-q) is a normal float, and
+            // where it is not, both round to 1e-7 after the addition
+            const f2 w = add2(pack(exp_ftz(-lo(q)), exp_ftz(-hi(q))), k1e7);
             const ulonglong2 c0 = R[0], c1 = R[1], c2 = R[2], c3 = R[3], c4 = R[4], c5 = R[5], c6 = R[6],
                              c7 = R[7], c8 = R[8];
             // coefficient j = r * 3 + ch sits in record j / 2, half j % 2:

@@ -219,26 +219,38 @@ __global__ void __launch_bounds__(256) recon_grad_centre_kernel(GArgs A)
     const size_t ci = b * C + (size_t)j * A.Ws + i;
     const int ox0 = max(0, (i * A.sp - A.hw - A.sp) / A.rs), ox1 = min(A.Wr - 1, (i * A.sp + A.hw + A.sp) / A.rs);
     const int oy0 = max(0, (j * A.sp - A.hw - A.sp) / A.rs), oy1 = min(A.Hr - 1, (j * A.sp + A.hw + A.sp) / A.rs);
-    // the output pixels whose centre range contains (i, j): both ends of a
-    // pixel's range are non-decreasing in the pixel's position, so along
-    // each axis they form one interval, found once per axis
-    int vx0 = ox1 + 1, vx1 = ox0 - 1, vy0 = oy1 + 1, vy1 = oy0 - 1;
-    for (int ox = ox0; ox <= ox1; ++ox) {
+    // which candidate output pixels have (i, j) in their centre range, tested
+    // once per axis (the range's lower end follows the reference's iDivUp,
+    // which is not monotone near the image's top and left edges, so the
+    // set need not be an interval); at most 64 candidates per axis are kept
+    // as bits, more fall back to testing inside the loop
+    const int nxc = ox1 - ox0 + 1, nyc = oy1 - oy0 + 1;
+    const bool use_bits = nxc <= 64 && nyc <= 64;
+    unsigned long long xbits = 0ull, ybits = 0ull;
+    if (use_bits) {
+        for (int ox = ox0; ox <= ox1; ++ox) {
+            int sx, ex;
+            centre_range(ox * A.rs, A.W, A.hw, A.sp, sx, ex);
+            if (i >= sx && i <= ex) xbits |= 1ull << (ox - ox0);
+        }
+        for (int oy = oy0; oy <= oy1; ++oy) {
+            int sy, ey;
+            centre_range(oy * A.rs, A.H, A.hw, A.sp, sy, ey);
+            if (j >= sy && j <= ey) ybits |= 1ull << (oy - oy0);
+        }
+    }
+    auto x_in = [&](int ox) {
+        if (use_bits) return ((xbits >> (ox - ox0)) & 1ull) != 0;
         int sx, ex;
         centre_range(ox * A.rs, A.W, A.hw, A.sp, sx, ex);
-        if (i >= sx && i <= ex) {
-            vx0 = min(vx0, ox);
-            vx1 = max(vx1, ox);
-        }
-    }
-    for (int oy = oy0; oy <= oy1; ++oy) {
+        return i >= sx && i <= ex;
+    };
+    auto y_in = [&](int oy) {
+        if (use_bits) return ((ybits >> (oy - oy0)) & 1ull) != 0;
         int sy, ey;
         centre_range(oy * A.rs, A.H, A.hw, A.sp, sy, ey);
-        if (j >= sy && j <= ey) {
-            vy0 = min(vy0, oy);
-            vy1 = max(vy1, oy);
-        }
-    }
+        return j >= sy && j <= ey;
+    };
     const float3 ac = f3(A.alb, c), nc = f3(A.nrm, c);
     float3 galb = make_float3(0.f, 0.f, 0.f), gnn = galb;
     for (int X = 0; X < 2; ++X) {
@@ -252,8 +264,10 @@ __global__ void __launch_bounds__(256) recon_grad_centre_kernel(GArgs A)
         float3 gf = make_float3(0.f, 0.f, 0.f);
         float gs = 0.f, gv = 0.f;
         PairGrad g;
-        for (int oy = vy0; oy <= vy1; ++oy) {
-            for (int ox = vx0; ox <= vx1; ++ox) {
+        for (int oy = oy0; oy <= oy1; ++oy) {
+            if (!y_in(oy)) continue;
+            for (int ox = ox0; ox <= ox1; ++ox) {
+                if (!x_in(ox)) continue;
                 const size_t p = b * P + (size_t)(oy * A.rs) * A.W + ox * A.rs;
                 const size_t o = b * R + (size_t)oy * A.Wr + ox;
                 const float3 ap = f3(A.alb, p), np_ = f3(A.nrm, p);

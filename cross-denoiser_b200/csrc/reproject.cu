@@ -28,13 +28,35 @@ namespace {
 // part is hoisted by the caller (it depends only on the rounded position).
 // The normal distance is sqrt(fma(dz,dz, fma(dx,dx, dy*dy))) and its ratio is
 // taken in double: the reference adds the double literal 1e-2 (line 46).
+//
+// Both tests compare a correctly rounded quotient with a constant c whose
+// significand is even (10 = 1.25 * 2^3, 4 = 2^2), and they are decided here
+// without the division.  Rounding to nearest is monotone and rounds the
+// midpoint between c and its successor to c, so for b > 0
+//     RN(a / b) > c   <=>   a / b > c + ulp(c) / 2   <=>   a - c b > b ulp(c) / 2.
+// Near the threshold a - c b is exact in the working precision: in float,
+// a >= 8b makes a a multiple of 8 ulp(b) and 10 b a multiple of 2 ulp(b),
+// so their difference, smaller than 2b there, fits 24 bits and the fused
+// multiply-add returns it exactly; in double, d and 4 S are within a factor
+// of two of each other (Sterbenz), so d - 4 S is exact.  Far from the
+// threshold a rounding error cannot move the difference across b ulp(c) / 2.
+// The scaled right-hand sides are exact (b >= 2^-100, S >= 2^-900).  Operands
+// outside these ranges (negative or non-finite) take the division.
 CD_DEV bool depth_normal_ok(float Z, float Zp, float fwZ, float3 n, float3 np, float fwN)
 {
-    if (__fdiv_rn(fabsf(__fsub_rn(Zp, Z)), __fadd_rn(fwZ, 1e-2f)) > 10.f) return false;
+    const float a = fabsf(__fsub_rn(Zp, Z)), b = __fadd_rn(fwZ, 1e-2f);
+    const bool depth_bad = (b >= 0x1p-100f && b <= 0x1p100f && a <= 0x1p100f)
+                               ? __fmaf_rn(-10.f, b, a) > __fmul_rn(b, 0x1p-21f)   // ulp(10) / 2 = 2^-21
+                               : __fdiv_rn(a, b) > 10.f;
+    if (depth_bad) return false;
     const float dx = __fsub_rn(n.x, np.x), dy = __fsub_rn(n.y, np.y), dz = __fsub_rn(n.z, np.z);
     const float dd = __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
     const float dist = __fsqrt_rn(dd);
-    return !(__ddiv_rn((double)dist, __dadd_rn((double)fwN, 1e-2)) > 4.0);
+    const double S = __dadd_rn((double)fwN, 1e-2);
+    const bool normal_bad = (S >= 0x1p-900 && S <= 0x1p900 && dist <= 0x1p100f)
+                                ? __fma_rn(-4.0, S, (double)dist) > __dmul_rn(S, 0x1p-51)   // ulp(4) / 2 = 2^-51
+                                : __ddiv_rn((double)dist, S) > 4.0;
+    return !normal_bad;
 }
 
 template <int kN, int kC>

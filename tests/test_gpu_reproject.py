@@ -120,3 +120,36 @@ def test_argument_errors(cd, cuda):
         cd.ops.Reproject(a[0], [T(lists[0][:, :8])], *a[1:])
     with pytest.raises(ValueError):
         cd.ops.Reproject(a[0].double(), [T(lists[0])], *a[1:])
+
+
+def test_depth_ratio_boundary(cd, cuda):
+    """Depth differences within a few ulps of the reference's threshold
+    |Zp - Z| / (fwidthZ + 1e-2f) > 10 (ops/reproject.cu.cc:42), which the
+    kernel decides without dividing: the previous depth is 0 everywhere and
+    every pixel's |Z| sits k ulps from 10 (fwidthZ + 1e-2), k in -4..4, so all
+    its taps (and its 3x3 fallback) take the same decision; the mask equals
+    the oracle's, which divides."""
+    rng = np.random.default_rng(11)
+    B, H, W = 1, 64, 96
+    fw = rng.uniform(0.0, 2.0, (B, H, W)).astype(np.float32)
+    den = (fw + np.float32(1e-2)).astype(np.float32)
+    k = rng.integers(-4, 5, (B, H, W))
+    z = np.float32(10.0) * den
+    z = np.nextafter(z, np.where(k > 0, np.float32(np.inf), np.float32(-np.inf)), dtype=np.float32)
+    for _ in range(3):   # up to 4 ulps either way
+        more = np.abs(k) > 1
+        z = np.where(more, np.nextafter(z, np.where(k > 0, np.float32(np.inf), np.float32(-np.inf)),
+                                        dtype=np.float32), z)
+        k = np.where(more, k - np.sign(k), k)
+    z = np.where(k == 0, np.float32(10.0) * den, z).astype(np.float32)
+    lin = np.stack([z, fw, np.zeros_like(z)], -1).astype(np.float32)
+    n = np.broadcast_to(np.array([0.0, 0.6, 0.8], np.float32), (B, H, W, 3)).copy()
+    d = dict(mvec=np.zeros((B, H, W, 3), np.float32), linear_z=lin, prev_linear_z=np.zeros_like(lin),
+             normal=n, prev_normal=n.copy(), pn_fwidth=np.zeros((B, H, W, 3), np.float32),
+             opacity=np.ones((B, H, W, 1), np.float32), prev_opacity=np.ones((B, H, W, 1), np.float32))
+    lists = [rng.uniform(0, 1, (B, H, W, 3)).astype(np.float32)]
+    s, _ = run(cd, d, lists)
+    rs, _ = orc.reproject(d["mvec"], lists, *[d[kk] for kk in KEYS[1:]])
+    inner = rs[:, 1:-1, 1:-1]
+    assert 0.2 < inner.mean() < 0.8, "the inputs straddle the threshold"
+    assert_equal(s, rs, "success at the depth-ratio boundary")
