@@ -204,6 +204,142 @@ __global__ void __launch_bounds__(256) recon_grad_pixel_kernel(GArgs A)
     add3(A.gn, p, gnn);
 }
 
+// Pass 2 with the tile's centres staged in shared memory: a CTA of 32 x 8
+// output pixels first copies, for every centre any of its pixels reaches
+// (the forward recon kernel's superset), both buffers' features, standard
+// deviation, variance and coefficients and the shared albedo and normal into
+// one record of kRecG floats; the per-pixel loops then read records instead
+// of global memory.  Same pairs, same order, same arithmetic as
+// recon_grad_pixel_kernel, so the same results.
+constexpr int kRecG = 52;   // fA[3] sA vA betaA[18] | fB[3] sB vB betaB[18] | alb[3] nrm[3]
+
+__host__ __device__ inline int floordiv_g(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+__host__ __device__ inline size_t recon_grad_smem(int hw, int sp, int rs)
+{
+    const int ncx = (31 * rs + 2 * hw) / sp + 2, ncy = (7 * rs + 2 * hw) / sp + 2;
+    return (size_t)ncx * ncy * kRecG * sizeof(float);
+}
+
+__global__ void __launch_bounds__(256) recon_grad_pixel_smem_kernel(GArgs A)
+{
+    extern __shared__ float recs[];
+    const int b = blockIdx.z;
+    const size_t P = (size_t)A.H * A.W, R = (size_t)A.Hr * A.Wr, C = (size_t)A.Hs * A.Ws;
+    const int ox0 = blockIdx.x * 32, oy0 = blockIdx.y * 8;
+    const int ox1 = min(ox0 + 31, A.Wr - 1), oy1 = min(oy0 + 7, A.Hr - 1);
+    const int cx_lo = max(0, floordiv_g(ox0 * A.rs - A.hw, A.sp)), cx_hi = min(A.Ws - 1, (ox1 * A.rs + A.hw) / A.sp);
+    const int cy_lo = max(0, floordiv_g(oy0 * A.rs - A.hw, A.sp)), cy_hi = min(A.Hs - 1, (oy1 * A.rs + A.hw) / A.sp);
+    const int ncx = cx_hi - cx_lo + 1, ncy = cy_hi - cy_lo + 1;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    // one thread per (centre, field group)
+    for (int e = tid; e < ncx * ncy * 4; e += 256) {
+        const int n = e >> 2, part = e & 3;
+        const int iy = cy_lo + n / ncx, ix = cx_lo + n % ncx;
+        const size_t c = b * P + (size_t)(iy * A.sp) * A.W + ix * A.sp;
+        const size_t ci = b * C + (size_t)iy * A.Ws + ix;
+        float *r = recs + (size_t)n * kRecG;
+        if (part < 2) {
+            const GBuf &B_ = A.bf[part];
+            float *q = r + 23 * part;
+            const float3 f = f3(B_.f, c);
+            q[0] = f.x;
+            q[1] = f.y;
+            q[2] = f.z;
+            q[3] = __ldg(B_.s + c);
+            q[4] = __ldg(B_.v + c);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) q[5 + k] = __ldg(B_.beta + ci * kBeta + k);
+        } else if (part == 2) {
+#pragma unroll
+            for (int X = 0; X < 2; ++X)
+#pragma unroll
+                for (int k = 9; k < kBeta; ++k) r[23 * X + 5 + k] = __ldg(A.bf[X].beta + ci * kBeta + k);
+        } else {
+            const float3 al = f3(A.alb, c), nr = f3(A.nrm, c);
+            r[46] = al.x;
+            r[47] = al.y;
+            r[48] = al.z;
+            r[49] = nr.x;
+            r[50] = nr.y;
+            r[51] = nr.z;
+        }
+    }
+    __syncthreads();
+
+    const int ox = ox0 + threadIdx.x, oy = oy0 + threadIdx.y;
+    if (ox >= A.Wr || oy >= A.Hr) return;
+    const int px = ox * A.rs, py = oy * A.rs;
+    const size_t p = b * P + (size_t)py * A.W + px, o = b * R + (size_t)oy * A.Wr + ox;
+    int sx, ex, sy, ey;
+    centre_range(px, A.W, A.hw, A.sp, sx, ex);
+    centre_range(py, A.H, A.hw, A.sp, sy, ey);
+    const float3 ap = f3(A.alb, p), np_ = f3(A.nrm, p);
+    float3 galb = make_float3(0.f, 0.f, 0.f), gnn = galb;
+    for (int X = 0; X < 2; ++X) {
+        const GBuf &B_ = A.bf[X];
+        const float3 fp = f3(B_.f, p);
+        const float vp = __ldg(B_.v + p), sp_ = __ldg(B_.s + p);
+        float N[3] = {0.f, 0.f, 0.f}, D = 0.f;
+        const float zero[3] = {0.f, 0.f, 0.f};
+        PairGrad g;
+        for (int iy = sy; iy <= ey; ++iy)
+            for (int ix = sx; ix <= ex; ++ix) {
+                const float *r = recs + (size_t)((iy - cy_lo) * ncx + (ix - cx_lo)) * kRecG;
+                const float *q = r + 23 * X;
+                const float3 da = make_float3(ap.x - r[46], ap.y - r[47], ap.z - r[48]);
+                const float3 dn = make_float3(np_.x - r[49], np_.y - r[50], np_.z - r[51]);
+                recon_pair<false>(fp, make_float3(q[0], q[1], q[2]), sp_, q[3], vp, q[4], da, dn, q + 5, zero, 0.f,
+                                  g);
+                N[0] += g.w * g.pred[0];
+                N[1] += g.w * g.pred[1];
+                N[2] += g.w * g.pred[2];
+                D += g.w;
+            }
+        const float Dt = fmaxf(D, 1e-7f);
+        const float3 G = f3(B_.gout, o);
+        const float Gv[3] = {G.x, G.y, G.z};
+        float gN[3], gD = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float ok = N[k] / Dt;
+            gN[k] = ok > 0.f ? Gv[k] / Dt : 0.f;
+            gD -= gN[k] * ok;
+        }
+        if (!(D > 1e-7f)) gD = 0.f;
+        B_.gN[3 * o] = gN[0];
+        B_.gN[3 * o + 1] = gN[1];
+        B_.gN[3 * o + 2] = gN[2];
+        B_.gD[o] = gD;
+        float3 gf = make_float3(0.f, 0.f, 0.f);
+        float gs = 0.f, gv = 0.f;
+        for (int iy = sy; iy <= ey; ++iy)
+            for (int ix = sx; ix <= ex; ++ix) {
+                const float *r = recs + (size_t)((iy - cy_lo) * ncx + (ix - cx_lo)) * kRecG;
+                const float *q = r + 23 * X;
+                const float3 da = make_float3(ap.x - r[46], ap.y - r[47], ap.z - r[48]);
+                const float3 dn = make_float3(np_.x - r[49], np_.y - r[50], np_.z - r[51]);
+                recon_pair<false>(fp, make_float3(q[0], q[1], q[2]), sp_, q[3], vp, q[4], da, dn, q + 5, gN, gD, g);
+                gf.x += g.gdf.x;
+                gf.y += g.gdf.y;
+                gf.z += g.gdf.z;
+                gs += g.gden;
+                gv += g.gV;
+                galb.x += g.gda.x;
+                galb.y += g.gda.y;
+                galb.z += g.gda.z;
+                gnn.x += g.gdn.x;
+                gnn.y += g.gdn.y;
+                gnn.z += g.gdn.z;
+            }
+        add3(B_.gf, p, gf);
+        B_.gs[p] += gs;
+        B_.gv[p] += gv;
+    }
+    add3(A.galb, p, galb);
+    add3(A.gn, p, gnn);
+}
+
 // ---------------------------------------------------------------------------
 // Pass 3: reconstruction backward, centre side (dL/dbeta and the centre's
 // own features).  The output pixels whose centre range contains c are found
@@ -299,6 +435,133 @@ __global__ void __launch_bounds__(256) recon_grad_centre_kernel(GArgs A)
     }
     add3(A.galb, c, galb);
     add3(A.gn, c, gnn);
+}
+
+// Pass 3 with the CTA's output pixels staged in shared memory, in bands of
+// kBandRows pixel rows, one buffer at a time.  A band holds, for every
+// candidate output pixel of the band's rows, the buffer's features, standard
+// deviation, variance, dL/dN and dL/dD and the shared albedo and normal, as
+// field planes whose pixel positions are de-interleaved by the sparsity
+// (position x at (x % sp) * q + x / sp), so that the 32 centres of a warp,
+// sp pixels apart, read consecutive words.  Every centre visits its pixels
+// in the same order as recon_grad_centre_kernel (buffer, then rows, then
+// columns), so the results are the same.
+constexpr int kBandRows = 8, kBandFields = 15;   // f[3] s v gN[3] gD alb[3] nrm[3]
+
+__host__ __device__ inline int band_width(int hw, int sp, int rs) { return (31 * sp + 2 * hw + 2 * sp) / rs + 2; }
+
+__host__ __device__ inline size_t centre_band_smem(int hw, int sp, int rs)
+{
+    const int w = band_width(hw, sp, rs), q = (w + sp - 1) / sp;
+    return (size_t)kBandFields * kBandRows * q * sp * sizeof(float);
+}
+
+__global__ void __launch_bounds__(256) recon_grad_centre_band_kernel(GArgs A)
+{
+    extern __shared__ float band[];
+    const int b = blockIdx.z;
+    const size_t P = (size_t)A.H * A.W, R = (size_t)A.Hr * A.Wr, C = (size_t)A.Hs * A.Ws;
+    const int i0c = blockIdx.x * 32, j0c = blockIdx.y * 8;
+    // candidate output pixels of the whole CTA
+    const int bx0 = max(0, (i0c * A.sp - A.hw - A.sp) / A.rs);
+    const int bx1 = min(A.Wr - 1, ((i0c + 31) * A.sp + A.hw + A.sp) / A.rs);
+    const int by0 = max(0, (j0c * A.sp - A.hw - A.sp) / A.rs);
+    const int by1 = min(A.Hr - 1, ((j0c + 7) * A.sp + A.hw + A.sp) / A.rs);
+    const int bw = bx1 - bx0 + 1, q = (band_width(A.hw, A.sp, A.rs) + A.sp - 1) / A.sp;
+    const int plane = kBandRows * q * A.sp;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+
+    const int i = i0c + threadIdx.x, j = j0c + threadIdx.y;
+    const bool active = i < A.Ws && j < A.Hs;
+    const int ic = min(i, A.Ws - 1), jc = min(j, A.Hs - 1);
+    const size_t c = b * P + (size_t)(jc * A.sp) * A.W + ic * A.sp;
+    const size_t ci = b * C + (size_t)jc * A.Ws + ic;
+    const int ox0 = max(0, (ic * A.sp - A.hw - A.sp) / A.rs), ox1 = min(A.Wr - 1, (ic * A.sp + A.hw + A.sp) / A.rs);
+    const int oy0 = max(0, (jc * A.sp - A.hw - A.sp) / A.rs), oy1 = min(A.Hr - 1, (jc * A.sp + A.hw + A.sp) / A.rs);
+    // the candidates whose centre range contains (i, j), as in recon_grad_centre_kernel
+    unsigned long long xbits = 0ull, ybits = 0ull;
+    for (int ox = ox0; ox <= ox1 && ox - ox0 < 64; ++ox) {
+        int sx, ex;
+        centre_range(ox * A.rs, A.W, A.hw, A.sp, sx, ex);
+        if (ic >= sx && ic <= ex) xbits |= 1ull << (ox - ox0);
+    }
+    for (int oy = oy0; oy <= oy1 && oy - oy0 < 64; ++oy) {
+        int sy, ey;
+        centre_range(oy * A.rs, A.H, A.hw, A.sp, sy, ey);
+        if (jc >= sy && jc <= ey) ybits |= 1ull << (oy - oy0);
+    }
+    const float3 ac = f3(A.alb, c), nc = f3(A.nrm, c);
+    float3 galb = make_float3(0.f, 0.f, 0.f), gnn = galb;
+    for (int X = 0; X < 2; ++X) {
+        const GBuf &B_ = A.bf[X];
+        const float3 fc = f3(B_.f, c);
+        const float vc = __ldg(B_.v + c), sc = __ldg(B_.s + c);
+        const float *beta = B_.beta + ci * kBeta;
+        float gb[kBeta];
+#pragma unroll
+        for (int k = 0; k < kBeta; ++k) gb[k] = 0.f;
+        float3 gf = make_float3(0.f, 0.f, 0.f);
+        float gs = 0.f, gv = 0.f;
+        PairGrad g;
+        for (int y0b = by0; y0b <= by1; y0b += kBandRows) {
+            const int nrows = min(kBandRows, by1 - y0b + 1);
+            __syncthreads();   // the previous band is no longer read
+            for (int e = tid; e < nrows * bw; e += 256) {
+                const int r = e / bw, x = e - r * bw;
+                const int oy = y0b + r, ox = bx0 + x;
+                const size_t p = b * P + (size_t)(oy * A.rs) * A.W + ox * A.rs;
+                const size_t o = b * R + (size_t)oy * A.Wr + ox;
+                const int si = r * q * A.sp + (x % A.sp) * q + x / A.sp;
+                const float3 f = f3(B_.f, p), al = f3(A.alb, p), nr = f3(A.nrm, p);
+                float v[kBandFields] = {f.x, f.y, f.z, __ldg(B_.s + p), __ldg(B_.v + p), B_.gN[3 * o],
+                                        B_.gN[3 * o + 1], B_.gN[3 * o + 2], B_.gD[o], al.x, al.y, al.z,
+                                        nr.x, nr.y, nr.z};
+#pragma unroll
+                for (int k = 0; k < kBandFields; ++k) band[k * plane + si] = v[k];
+            }
+            __syncthreads();
+            if (!active) continue;
+            const int ry0 = max(oy0, y0b), ry1 = min(oy1, y0b + nrows - 1);
+            for (int oy = ry0; oy <= ry1; ++oy) {
+                if (!((ybits >> (oy - oy0)) & 1ull)) continue;
+                const int r = oy - y0b;
+                for (int ox = ox0; ox <= ox1; ++ox) {
+                    if (!((xbits >> (ox - ox0)) & 1ull)) continue;
+                    const int x = ox - bx0;
+                    const float *pp = band + r * q * A.sp + (x % A.sp) * q + x / A.sp;
+                    const float3 fp = make_float3(pp[0], pp[plane], pp[2 * plane]);
+                    const float3 da = make_float3(pp[9 * plane] - ac.x, pp[10 * plane] - ac.y, pp[11 * plane] - ac.z);
+                    const float3 dn = make_float3(pp[12 * plane] - nc.x, pp[13 * plane] - nc.y, pp[14 * plane] - nc.z);
+                    const float gN[3] = {pp[5 * plane], pp[6 * plane], pp[7 * plane]};
+                    recon_pair<true>(fp, fc, pp[3 * plane], sc, pp[4 * plane], vc, da, dn, beta, gN, pp[8 * plane], g);
+#pragma unroll
+                    for (int k = 0; k < kBeta; ++k) gb[k] += g.gbeta[k];
+                    gf.x -= g.gdf.x;
+                    gf.y -= g.gdf.y;
+                    gf.z -= g.gdf.z;
+                    gs += g.gden;
+                    gv += g.gV;
+                    galb.x -= g.gda.x;
+                    galb.y -= g.gda.y;
+                    galb.z -= g.gda.z;
+                    gnn.x -= g.gdn.x;
+                    gnn.y -= g.gdn.y;
+                    gnn.z -= g.gdn.z;
+                }
+            }
+        }
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < kBeta; ++k) B_.gbeta[ci * kBeta + k] = gb[k];
+            add3(B_.gf, c, gf);
+            B_.gs[c] += gs;
+            B_.gv[c] += gv;
+        }
+    }
+    if (active) {
+        add3(A.galb, c, galb);
+        add3(A.gn, c, gnn);
+    }
 }
 
 // One regression tap of one buffer: the forward quantities and the
@@ -427,6 +690,134 @@ __global__ void __launch_bounds__(128) regression_grad_centre_kernel(GArgs A)
     add3(A.gn, c, gnn);
 }
 
+// Pass 4 with the CTA's window positions staged in shared memory, in bands
+// of kBandRows window rows, one buffer at a time.  A CTA of 32 x 8 centres
+// covers window positions x in [i0 sp - hw, (i0 + 31) sp + hw] and the
+// corresponding rows; the band stores, per position, the reflect-101 pixel's
+// features, target, standard deviation, variance, albedo and normal (the
+// mirror applied while staging), de-interleaved by the sparsity.  The solve
+// and the tap order (rows, then columns) are those of
+// regression_grad_centre_kernel, so the results are the same.
+constexpr int kTapFields = 14;   // f[3] y[3] s v alb[3] nrm[3]
+
+__host__ __device__ inline int tap_band_width(int hw, int sp) { return 31 * sp + 2 * hw + 1; }
+
+__host__ __device__ inline size_t tap_band_smem(int hw, int sp)
+{
+    const int w = tap_band_width(hw, sp), q = (w + sp - 1) / sp;
+    return (size_t)kTapFields * kBandRows * q * sp * sizeof(float);
+}
+
+__global__ void __launch_bounds__(256) regression_grad_centre_band_kernel(GArgs A)
+{
+    extern __shared__ float band[];
+    const int b = blockIdx.z;
+    const size_t P = (size_t)A.H * A.W, C = (size_t)A.Hs * A.Ws;
+    const int i0c = blockIdx.x * 32, j0c = blockIdx.y * 8;
+    const int wx0 = i0c * A.sp - A.hw;                           // first window column position
+    const int nrw = (min(j0c + 7, A.Hs - 1) - j0c) * A.sp + 2 * A.hw + 1;   // window row positions
+    const int wy0 = j0c * A.sp - A.hw;
+    const int bw = (min(i0c + 31, A.Ws - 1) - i0c) * A.sp + 2 * A.hw + 1;
+    const int q = (tap_band_width(A.hw, A.sp) + A.sp - 1) / A.sp;
+    const int plane = kBandRows * q * A.sp;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+
+    const int i = i0c + threadIdx.x, j = j0c + threadIdx.y;
+    const bool active = i < A.Ws && j < A.Hs;
+    const int ic = min(i, A.Ws - 1), jc = min(j, A.Hs - 1);
+    const int cx = ic * A.sp, cy = jc * A.sp;
+    const size_t c = b * P + (size_t)cy * A.W + cx;
+    const size_t ci = b * C + (size_t)jc * A.Ws + ic;
+    const float3 ac = f3(A.alb, c), nc = f3(A.nrm, c);
+    float3 galb = make_float3(0.f, 0.f, 0.f), gnn = galb;
+    for (int X = 0; X < 2; ++X) {
+        const GBuf &B_ = A.bf[X];
+        float u[kBeta], beta[kBeta];
+#pragma unroll
+        for (int k = 0; k < kBeta; ++k) beta[k] = __ldg(B_.beta + ci * kBeta + k);
+        // per channel: L z = g, L^T u = z (L lower triangular, row-major packed)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float *Lk = B_.L + ci * kL + 21 * k;
+            float z[kP];
+#pragma unroll
+            for (int r = 0; r < kP; ++r) {
+                float s = B_.gbeta[ci * kBeta + r * 3 + k];
+#pragma unroll
+                for (int qq = 0; qq < r; ++qq) s -= __ldg(Lk + r * (r + 1) / 2 + qq) * z[qq];
+                z[r] = s / __ldg(Lk + r * (r + 1) / 2 + r);
+            }
+#pragma unroll
+            for (int r = kP - 1; r >= 0; --r) {
+                float s = z[r];
+#pragma unroll
+                for (int qq = r + 1; qq < kP; ++qq) s -= __ldg(Lk + qq * (qq + 1) / 2 + r) * u[qq * 3 + k];
+                u[r * 3 + k] = s / __ldg(Lk + r * (r + 1) / 2 + r);
+            }
+        }
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < kBeta; ++k) B_.u[ci * kBeta + k] = u[k];
+        }
+        const float3 fc = f3(B_.f, c);
+        const float vc = __ldg(B_.v + c), sc = __ldg(B_.s + c);
+        float3 gf = make_float3(0.f, 0.f, 0.f);
+        float gs = 0.f, gv = 0.f;
+        TapGrad g;
+        for (int yb = 0; yb < nrw; yb += kBandRows) {
+            const int nrows = min(kBandRows, nrw - yb);
+            __syncthreads();   // the previous band is no longer read
+            for (int e = tid; e < nrows * bw; e += 256) {
+                const int r = e / bw, x = e - r * bw;
+                const int ty = mirror(wy0 + yb + r, A.H), tx = mirror(wx0 + x, A.W);
+                const size_t t = b * P + (size_t)ty * A.W + tx;
+                const int si = r * q * A.sp + (x % A.sp) * q + x / A.sp;
+                const float3 f = f3(B_.f, t), y = f3(B_.y, t), al = f3(A.alb, t), nr = f3(A.nrm, t);
+                const float v[kTapFields] = {f.x, f.y, f.z, y.x, y.y, y.z, __ldg(B_.s + t), __ldg(B_.v + t),
+                                             al.x, al.y, al.z, nr.x, nr.y, nr.z};
+#pragma unroll
+                for (int k = 0; k < kTapFields; ++k) band[k * plane + si] = v[k];
+            }
+            __syncthreads();
+            if (!active) continue;
+            // this centre's window rows cy - hw .. cy + hw, as band rows
+            const int rlo = max(0, cy - A.hw - wy0 - yb), rhi = min(nrows - 1, cy + A.hw - wy0 - yb);
+            for (int r = rlo; r <= rhi; ++r) {
+                for (int dx = -A.hw; dx <= A.hw; ++dx) {
+                    const int x = cx + dx - wx0;
+                    const float *pp = band + r * q * A.sp + (x % A.sp) * q + x / A.sp;
+                    regression_tap(make_float3(pp[0], pp[plane], pp[2 * plane]), fc,
+                                   make_float3(pp[3 * plane], pp[4 * plane], pp[5 * plane]), pp[6 * plane], sc,
+                                   pp[7 * plane], vc,
+                                   make_float3(pp[8 * plane] - ac.x, pp[9 * plane] - ac.y, pp[10 * plane] - ac.z),
+                                   make_float3(pp[11 * plane] - nc.x, pp[12 * plane] - nc.y, pp[13 * plane] - nc.z),
+                                   u, beta, g);
+                    gf.x -= g.gdf.x;
+                    gf.y -= g.gdf.y;
+                    gf.z -= g.gdf.z;
+                    gs += g.gden;
+                    gv += g.gV;
+                    galb.x -= g.gda.x;
+                    galb.y -= g.gda.y;
+                    galb.z -= g.gda.z;
+                    gnn.x -= g.gdn.x;
+                    gnn.y -= g.gdn.y;
+                    gnn.z -= g.gdn.z;
+                }
+            }
+        }
+        if (active) {
+            add3(B_.gf, c, gf);
+            B_.gs[c] += gs;
+            B_.gv[c] += gv;
+        }
+    }
+    if (active) {
+        add3(A.galb, c, galb);
+        add3(A.gn, c, gnn);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Pass 5: tap-side terms gathered per pixel q.  Window position t of
 // centre c maps to pixel mirror(t); along each axis the positions whose
@@ -479,6 +870,127 @@ __global__ void __launch_bounds__(256) regression_grad_tap_kernel(GArgs A)
                                        make_float3(at.x - ac.x, at.y - ac.y, at.z - ac.z),
                                        make_float3(nt.x - nc.x, nt.y - nc.y, nt.z - nc.z), B_.u + ci * kBeta,
                                        B_.beta + ci * kBeta, g);
+                        gf.x += g.gdf.x;
+                        gf.y += g.gdf.y;
+                        gf.z += g.gdf.z;
+                        gy.x += g.gy.x;
+                        gy.y += g.gy.y;
+                        gy.z += g.gy.z;
+                        gs += g.gden;
+                        gv += g.gV;
+                        galb.x += g.gda.x;
+                        galb.y += g.gda.y;
+                        galb.z += g.gda.z;
+                        gnn.x += g.gdn.x;
+                        gnn.y += g.gdn.y;
+                        gnn.z += g.gdn.z;
+                    }
+                }
+            }
+        }
+        add3(B_.gf, q, gf);
+        add3(B_.gy, q, gy);
+        B_.gs[q] += gs;
+        B_.gv[q] += gv;
+    }
+    add3(A.galb, q, galb);
+    add3(A.gn, q, gnn);
+}
+
+// Pass 5 with the tile's centres staged in shared memory.  Along each axis
+// the centres any pixel of a 32 x 8 tile reaches (directly, or through the
+// reflect-101 images -q near the low edge and 2n-2-q near the high edge,
+// which only occur when the direct range already reaches centre 0 or the
+// last centre) form one range [lo, hi]; a record per centre holds both
+// buffers' features, standard deviation, variance, u and coefficients and
+// the shared albedo and normal.  Same pairs, order and arithmetic as
+// regression_grad_tap_kernel.
+constexpr int kRecT = 88;   // per buffer X at 41 X: f[3] s v u[18] beta[18]; alb[3] at 82, nrm[3] at 85
+
+__host__ __device__ inline size_t tap_grad_smem(int hw, int sp)
+{
+    const int ncx = (31 + 2 * hw) / sp + 2, ncy = (7 + 2 * hw) / sp + 2;
+    return (size_t)ncx * ncy * kRecT * sizeof(float);
+}
+
+__global__ void __launch_bounds__(256) regression_grad_tap_smem_kernel(GArgs A)
+{
+    extern __shared__ float recs[];
+    const int b = blockIdx.z;
+    const size_t P = (size_t)A.H * A.W, C = (size_t)A.Hs * A.Ws;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
+    const int x1 = min(x0 + 31, A.W - 1), y1 = min(y0 + 7, A.H - 1);
+    const int cx_lo = x0 - A.hw > 0 ? (x0 - A.hw + A.sp - 1) / A.sp : 0;
+    const int cy_lo = y0 - A.hw > 0 ? (y0 - A.hw + A.sp - 1) / A.sp : 0;
+    const int cx_hi = min(A.Ws - 1, (x1 + A.hw) / A.sp), cy_hi = min(A.Hs - 1, (y1 + A.hw) / A.sp);
+    const int ncx = cx_hi - cx_lo + 1, ncy = cy_hi - cy_lo + 1;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    for (int e = tid; e < ncx * ncy * 5; e += 256) {
+        const int n = e / 5, part = e - 5 * n;
+        const int iy = cy_lo + n / ncx, ix = cx_lo + n % ncx;
+        const size_t c = b * P + (size_t)(iy * A.sp) * A.W + ix * A.sp;
+        const size_t ci = b * C + (size_t)iy * A.Ws + ix;
+        float *r = recs + (size_t)n * kRecT;
+        if (part < 2) {                       // features, sd, var, u of buffer `part`
+            const GBuf &B_ = A.bf[part];
+            float *q = r + 41 * part;
+            const float3 f = f3(B_.f, c);
+            q[0] = f.x;
+            q[1] = f.y;
+            q[2] = f.z;
+            q[3] = __ldg(B_.s + c);
+            q[4] = __ldg(B_.v + c);
+#pragma unroll
+            for (int k = 0; k < kBeta; ++k) q[5 + k] = B_.u[ci * kBeta + k];
+        } else if (part < 4) {                // coefficients of buffer part - 2
+            const GBuf &B_ = A.bf[part - 2];
+            float *q = r + 41 * (part - 2) + 23;
+#pragma unroll
+            for (int k = 0; k < kBeta; ++k) q[k] = __ldg(B_.beta + ci * kBeta + k);
+        } else {
+            const float3 al = f3(A.alb, c), nr = f3(A.nrm, c);
+            r[82] = al.x;
+            r[83] = al.y;
+            r[84] = al.z;
+            r[85] = nr.x;
+            r[86] = nr.y;
+            r[87] = nr.z;
+        }
+    }
+    __syncthreads();
+
+    const int qx = x0 + threadIdx.x, qy = y0 + threadIdx.y;
+    if (qx >= A.W || qy >= A.H) return;
+    const size_t q = b * P + (size_t)qy * A.W + qx;
+    int txs[3], tys[3];
+    const int ntx = tap_positions(qx, A.W, A.hw, (A.Ws - 1) * A.sp, txs);
+    const int nty = tap_positions(qy, A.H, A.hw, (A.Hs - 1) * A.sp, tys);
+    const float3 at = f3(A.alb, q), nt = f3(A.nrm, q);
+    float3 galb = make_float3(0.f, 0.f, 0.f), gnn = galb;
+    for (int X = 0; X < 2; ++X) {
+        const GBuf &B_ = A.bf[X];
+        const float3 ft = f3(B_.f, q), yt = f3(B_.y, q);
+        const float vt = __ldg(B_.v + q), st = __ldg(B_.s + q);
+        float3 gf = make_float3(0.f, 0.f, 0.f), gy = gf;
+        float gs = 0.f, gv = 0.f;
+        TapGrad g;
+        for (int a = 0; a < nty; ++a) {
+            const int ty = tys[a];
+            const int j0 = max(0, (ty - A.hw + A.sp - 1) >= 0 ? (ty - A.hw + A.sp - 1) / A.sp : 0);
+            const int j1 = min(A.Hs - 1, (ty + A.hw) >= 0 ? (ty + A.hw) / A.sp : -1);
+            for (int j = j0; j <= j1; ++j) {
+                if (abs(j * A.sp - ty) > A.hw) continue;
+                for (int bb = 0; bb < ntx; ++bb) {
+                    const int tx = txs[bb];
+                    const int i0 = max(0, (tx - A.hw + A.sp - 1) >= 0 ? (tx - A.hw + A.sp - 1) / A.sp : 0);
+                    const int i1 = min(A.Ws - 1, (tx + A.hw) >= 0 ? (tx + A.hw) / A.sp : -1);
+                    for (int i = i0; i <= i1; ++i) {
+                        if (abs(i * A.sp - tx) > A.hw) continue;
+                        const float *r = recs + (size_t)((j - cy_lo) * ncx + (i - cx_lo)) * kRecT;
+                        const float *rq = r + 41 * X;
+                        regression_tap(ft, make_float3(rq[0], rq[1], rq[2]), yt, st, rq[3], vt, rq[4],
+                                       make_float3(at.x - r[82], at.y - r[83], at.z - r[84]),
+                                       make_float3(nt.x - r[85], nt.y - r[86], nt.z - r[87]), rq + 5, rq + 23, g);
                         gf.x += g.gdf.x;
                         gf.y += g.gdf.y;
                         gf.z += g.gdf.z;
@@ -662,10 +1174,44 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
     dim3 blk(32, 8);
     dim3 g_out((A.Wr + 31) / 32, (A.Hr + 7) / 8, B), g_cen((A.Ws + 31) / 32, (A.Hs + 7) / 8, B);
     dim3 g_px((W + 31) / 32, (H + 7) / 8, B);
-    recon_grad_pixel_kernel<<<g_out, blk, 0, st>>>(A);
-    recon_grad_centre_kernel<<<g_cen, blk, 0, st>>>(A);
-    regression_grad_centre_kernel<<<dim3((A.Ws + 15) / 16, (A.Hs + 7) / 8, B), dim3(16, 8), 0, st>>>(A);
-    regression_grad_tap_kernel<<<g_px, blk, 0, st>>>(A);
+    const size_t rg_smem = recon_grad_smem(A.hw, A.sp, A.rs);
+    if (rg_smem <= 200 * 1024) {
+        if ((e = cudaFuncSetAttribute(recon_grad_pixel_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)rg_smem)) != cudaSuccess)
+            return e;
+        recon_grad_pixel_smem_kernel<<<g_out, blk, rg_smem, st>>>(A);
+    } else {
+        recon_grad_pixel_kernel<<<g_out, blk, 0, st>>>(A);
+    }
+    // the banded form needs every centre's candidate ranges within 64 positions
+    const int cand = (2 * A.hw + 2 * A.sp) / A.rs + 2;
+    const size_t cb_smem = centre_band_smem(A.hw, A.sp, A.rs);
+    if (cand <= 64 && cb_smem <= 200 * 1024) {
+        if ((e = cudaFuncSetAttribute(recon_grad_centre_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)cb_smem)) != cudaSuccess)
+            return e;
+        recon_grad_centre_band_kernel<<<g_cen, blk, cb_smem, st>>>(A);
+    } else {
+        recon_grad_centre_kernel<<<g_cen, blk, 0, st>>>(A);
+    }
+    const size_t tb_smem = tap_band_smem(A.hw, A.sp);
+    if (tb_smem <= 200 * 1024) {
+        if ((e = cudaFuncSetAttribute(regression_grad_centre_band_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb_smem)) != cudaSuccess)
+            return e;
+        regression_grad_centre_band_kernel<<<g_cen, blk, tb_smem, st>>>(A);
+    } else {
+        regression_grad_centre_kernel<<<dim3((A.Ws + 15) / 16, (A.Hs + 7) / 8, B), dim3(16, 8), 0, st>>>(A);
+    }
+    const size_t tg_smem = tap_grad_smem(A.hw, A.sp);
+    if (tg_smem <= 200 * 1024) {
+        if ((e = cudaFuncSetAttribute(regression_grad_tap_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)tg_smem)) != cudaSuccess)
+            return e;
+        regression_grad_tap_smem_kernel<<<g_px, blk, tg_smem, st>>>(A);
+    } else {
+        regression_grad_tap_kernel<<<g_px, blk, 0, st>>>(A);
+    }
     variance_grad_kernel<<<g_px, blk, 0, st>>>(A);
     assemble_grad_kernel<<<g_px, blk, 0, st>>>(A);
     return cudaGetLastError();
