@@ -437,133 +437,6 @@ __global__ void __launch_bounds__(256) recon_grad_centre_kernel(GArgs A)
     add3(A.gn, c, gnn);
 }
 
-// Pass 3 with the CTA's output pixels staged in shared memory, in bands of
-// kBandRows pixel rows, one buffer at a time.  A band holds, for every
-// candidate output pixel of the band's rows, the buffer's features, standard
-// deviation, variance, dL/dN and dL/dD and the shared albedo and normal, as
-// field planes whose pixel positions are de-interleaved by the sparsity
-// (position x at (x % sp) * q + x / sp), so that the 32 centres of a warp,
-// sp pixels apart, read consecutive words.  Every centre visits its pixels
-// in the same order as recon_grad_centre_kernel (buffer, then rows, then
-// columns), so the results are the same.
-constexpr int kBandRows = 8, kBandFields = 15;   // f[3] s v gN[3] gD alb[3] nrm[3]
-
-__host__ __device__ inline int band_width(int hw, int sp, int rs) { return (31 * sp + 2 * hw + 2 * sp) / rs + 2; }
-
-__host__ __device__ inline size_t centre_band_smem(int hw, int sp, int rs)
-{
-    const int w = band_width(hw, sp, rs), q = (w + sp - 1) / sp;
-    return (size_t)kBandFields * kBandRows * q * sp * sizeof(float);
-}
-
-__global__ void __launch_bounds__(256) recon_grad_centre_band_kernel(GArgs A)
-{
-    extern __shared__ float band[];
-    const int b = blockIdx.z;
-    const size_t P = (size_t)A.H * A.W, R = (size_t)A.Hr * A.Wr, C = (size_t)A.Hs * A.Ws;
-    const int i0c = blockIdx.x * 32, j0c = blockIdx.y * 8;
-    // candidate output pixels of the whole CTA
-    const int bx0 = max(0, (i0c * A.sp - A.hw - A.sp) / A.rs);
-    const int bx1 = min(A.Wr - 1, ((i0c + 31) * A.sp + A.hw + A.sp) / A.rs);
-    const int by0 = max(0, (j0c * A.sp - A.hw - A.sp) / A.rs);
-    const int by1 = min(A.Hr - 1, ((j0c + 7) * A.sp + A.hw + A.sp) / A.rs);
-    const int bw = bx1 - bx0 + 1, q = (band_width(A.hw, A.sp, A.rs) + A.sp - 1) / A.sp;
-    const int plane = kBandRows * q * A.sp;
-    const int tid = threadIdx.y * 32 + threadIdx.x;
-
-    const int i = i0c + threadIdx.x, j = j0c + threadIdx.y;
-    const bool active = i < A.Ws && j < A.Hs;
-    const int ic = min(i, A.Ws - 1), jc = min(j, A.Hs - 1);
-    const size_t c = b * P + (size_t)(jc * A.sp) * A.W + ic * A.sp;
-    const size_t ci = b * C + (size_t)jc * A.Ws + ic;
-    const int ox0 = max(0, (ic * A.sp - A.hw - A.sp) / A.rs), ox1 = min(A.Wr - 1, (ic * A.sp + A.hw + A.sp) / A.rs);
-    const int oy0 = max(0, (jc * A.sp - A.hw - A.sp) / A.rs), oy1 = min(A.Hr - 1, (jc * A.sp + A.hw + A.sp) / A.rs);
-    // the candidates whose centre range contains (i, j), as in recon_grad_centre_kernel
-    unsigned long long xbits = 0ull, ybits = 0ull;
-    for (int ox = ox0; ox <= ox1 && ox - ox0 < 64; ++ox) {
-        int sx, ex;
-        centre_range(ox * A.rs, A.W, A.hw, A.sp, sx, ex);
-        if (ic >= sx && ic <= ex) xbits |= 1ull << (ox - ox0);
-    }
-    for (int oy = oy0; oy <= oy1 && oy - oy0 < 64; ++oy) {
-        int sy, ey;
-        centre_range(oy * A.rs, A.H, A.hw, A.sp, sy, ey);
-        if (jc >= sy && jc <= ey) ybits |= 1ull << (oy - oy0);
-    }
-    const float3 ac = f3(A.alb, c), nc = f3(A.nrm, c);
-    float3 galb = make_float3(0.f, 0.f, 0.f), gnn = galb;
-    for (int X = 0; X < 2; ++X) {
-        const GBuf &B_ = A.bf[X];
-        const float3 fc = f3(B_.f, c);
-        const float vc = __ldg(B_.v + c), sc = __ldg(B_.s + c);
-        const float *beta = B_.beta + ci * kBeta;
-        float gb[kBeta];
-#pragma unroll
-        for (int k = 0; k < kBeta; ++k) gb[k] = 0.f;
-        float3 gf = make_float3(0.f, 0.f, 0.f);
-        float gs = 0.f, gv = 0.f;
-        PairGrad g;
-        for (int y0b = by0; y0b <= by1; y0b += kBandRows) {
-            const int nrows = min(kBandRows, by1 - y0b + 1);
-            __syncthreads();   // the previous band is no longer read
-            for (int e = tid; e < nrows * bw; e += 256) {
-                const int r = e / bw, x = e - r * bw;
-                const int oy = y0b + r, ox = bx0 + x;
-                const size_t p = b * P + (size_t)(oy * A.rs) * A.W + ox * A.rs;
-                const size_t o = b * R + (size_t)oy * A.Wr + ox;
-                const int si = r * q * A.sp + (x % A.sp) * q + x / A.sp;
-                const float3 f = f3(B_.f, p), al = f3(A.alb, p), nr = f3(A.nrm, p);
-                float v[kBandFields] = {f.x, f.y, f.z, __ldg(B_.s + p), __ldg(B_.v + p), B_.gN[3 * o],
-                                        B_.gN[3 * o + 1], B_.gN[3 * o + 2], B_.gD[o], al.x, al.y, al.z,
-                                        nr.x, nr.y, nr.z};
-#pragma unroll
-                for (int k = 0; k < kBandFields; ++k) band[k * plane + si] = v[k];
-            }
-            __syncthreads();
-            if (!active) continue;
-            const int ry0 = max(oy0, y0b), ry1 = min(oy1, y0b + nrows - 1);
-            for (int oy = ry0; oy <= ry1; ++oy) {
-                if (!((ybits >> (oy - oy0)) & 1ull)) continue;
-                const int r = oy - y0b;
-                for (int ox = ox0; ox <= ox1; ++ox) {
-                    if (!((xbits >> (ox - ox0)) & 1ull)) continue;
-                    const int x = ox - bx0;
-                    const float *pp = band + r * q * A.sp + (x % A.sp) * q + x / A.sp;
-                    const float3 fp = make_float3(pp[0], pp[plane], pp[2 * plane]);
-                    const float3 da = make_float3(pp[9 * plane] - ac.x, pp[10 * plane] - ac.y, pp[11 * plane] - ac.z);
-                    const float3 dn = make_float3(pp[12 * plane] - nc.x, pp[13 * plane] - nc.y, pp[14 * plane] - nc.z);
-                    const float gN[3] = {pp[5 * plane], pp[6 * plane], pp[7 * plane]};
-                    recon_pair<true>(fp, fc, pp[3 * plane], sc, pp[4 * plane], vc, da, dn, beta, gN, pp[8 * plane], g);
-#pragma unroll
-                    for (int k = 0; k < kBeta; ++k) gb[k] += g.gbeta[k];
-                    gf.x -= g.gdf.x;
-                    gf.y -= g.gdf.y;
-                    gf.z -= g.gdf.z;
-                    gs += g.gden;
-                    gv += g.gV;
-                    galb.x -= g.gda.x;
-                    galb.y -= g.gda.y;
-                    galb.z -= g.gda.z;
-                    gnn.x -= g.gdn.x;
-                    gnn.y -= g.gdn.y;
-                    gnn.z -= g.gdn.z;
-                }
-            }
-        }
-        if (active) {
-#pragma unroll
-            for (int k = 0; k < kBeta; ++k) B_.gbeta[ci * kBeta + k] = gb[k];
-            add3(B_.gf, c, gf);
-            B_.gs[c] += gs;
-            B_.gv[c] += gv;
-        }
-    }
-    if (active) {
-        add3(A.galb, c, galb);
-        add3(A.gn, c, gnn);
-    }
-}
-
 // One regression tap of one buffer: the forward quantities and the
 // derivatives of dL with respect to the tap's inputs, given u and beta.
 struct TapGrad {
@@ -688,134 +561,6 @@ __global__ void __launch_bounds__(128) regression_grad_centre_kernel(GArgs A)
     }
     add3(A.galb, c, galb);
     add3(A.gn, c, gnn);
-}
-
-// Pass 4 with the CTA's window positions staged in shared memory, in bands
-// of kBandRows window rows, one buffer at a time.  A CTA of 32 x 8 centres
-// covers window positions x in [i0 sp - hw, (i0 + 31) sp + hw] and the
-// corresponding rows; the band stores, per position, the reflect-101 pixel's
-// features, target, standard deviation, variance, albedo and normal (the
-// mirror applied while staging), de-interleaved by the sparsity.  The solve
-// and the tap order (rows, then columns) are those of
-// regression_grad_centre_kernel, so the results are the same.
-constexpr int kTapFields = 14;   // f[3] y[3] s v alb[3] nrm[3]
-
-__host__ __device__ inline int tap_band_width(int hw, int sp) { return 31 * sp + 2 * hw + 1; }
-
-__host__ __device__ inline size_t tap_band_smem(int hw, int sp)
-{
-    const int w = tap_band_width(hw, sp), q = (w + sp - 1) / sp;
-    return (size_t)kTapFields * kBandRows * q * sp * sizeof(float);
-}
-
-__global__ void __launch_bounds__(256) regression_grad_centre_band_kernel(GArgs A)
-{
-    extern __shared__ float band[];
-    const int b = blockIdx.z;
-    const size_t P = (size_t)A.H * A.W, C = (size_t)A.Hs * A.Ws;
-    const int i0c = blockIdx.x * 32, j0c = blockIdx.y * 8;
-    const int wx0 = i0c * A.sp - A.hw;                           // first window column position
-    const int nrw = (min(j0c + 7, A.Hs - 1) - j0c) * A.sp + 2 * A.hw + 1;   // window row positions
-    const int wy0 = j0c * A.sp - A.hw;
-    const int bw = (min(i0c + 31, A.Ws - 1) - i0c) * A.sp + 2 * A.hw + 1;
-    const int q = (tap_band_width(A.hw, A.sp) + A.sp - 1) / A.sp;
-    const int plane = kBandRows * q * A.sp;
-    const int tid = threadIdx.y * 32 + threadIdx.x;
-
-    const int i = i0c + threadIdx.x, j = j0c + threadIdx.y;
-    const bool active = i < A.Ws && j < A.Hs;
-    const int ic = min(i, A.Ws - 1), jc = min(j, A.Hs - 1);
-    const int cx = ic * A.sp, cy = jc * A.sp;
-    const size_t c = b * P + (size_t)cy * A.W + cx;
-    const size_t ci = b * C + (size_t)jc * A.Ws + ic;
-    const float3 ac = f3(A.alb, c), nc = f3(A.nrm, c);
-    float3 galb = make_float3(0.f, 0.f, 0.f), gnn = galb;
-    for (int X = 0; X < 2; ++X) {
-        const GBuf &B_ = A.bf[X];
-        float u[kBeta], beta[kBeta];
-#pragma unroll
-        for (int k = 0; k < kBeta; ++k) beta[k] = __ldg(B_.beta + ci * kBeta + k);
-        // per channel: L z = g, L^T u = z (L lower triangular, row-major packed)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const float *Lk = B_.L + ci * kL + 21 * k;
-            float z[kP];
-#pragma unroll
-            for (int r = 0; r < kP; ++r) {
-                float s = B_.gbeta[ci * kBeta + r * 3 + k];
-#pragma unroll
-                for (int qq = 0; qq < r; ++qq) s -= __ldg(Lk + r * (r + 1) / 2 + qq) * z[qq];
-                z[r] = s / __ldg(Lk + r * (r + 1) / 2 + r);
-            }
-#pragma unroll
-            for (int r = kP - 1; r >= 0; --r) {
-                float s = z[r];
-#pragma unroll
-                for (int qq = r + 1; qq < kP; ++qq) s -= __ldg(Lk + qq * (qq + 1) / 2 + r) * u[qq * 3 + k];
-                u[r * 3 + k] = s / __ldg(Lk + r * (r + 1) / 2 + r);
-            }
-        }
-        if (active) {
-#pragma unroll
-            for (int k = 0; k < kBeta; ++k) B_.u[ci * kBeta + k] = u[k];
-        }
-        const float3 fc = f3(B_.f, c);
-        const float vc = __ldg(B_.v + c), sc = __ldg(B_.s + c);
-        float3 gf = make_float3(0.f, 0.f, 0.f);
-        float gs = 0.f, gv = 0.f;
-        TapGrad g;
-        for (int yb = 0; yb < nrw; yb += kBandRows) {
-            const int nrows = min(kBandRows, nrw - yb);
-            __syncthreads();   // the previous band is no longer read
-            for (int e = tid; e < nrows * bw; e += 256) {
-                const int r = e / bw, x = e - r * bw;
-                const int ty = mirror(wy0 + yb + r, A.H), tx = mirror(wx0 + x, A.W);
-                const size_t t = b * P + (size_t)ty * A.W + tx;
-                const int si = r * q * A.sp + (x % A.sp) * q + x / A.sp;
-                const float3 f = f3(B_.f, t), y = f3(B_.y, t), al = f3(A.alb, t), nr = f3(A.nrm, t);
-                const float v[kTapFields] = {f.x, f.y, f.z, y.x, y.y, y.z, __ldg(B_.s + t), __ldg(B_.v + t),
-                                             al.x, al.y, al.z, nr.x, nr.y, nr.z};
-#pragma unroll
-                for (int k = 0; k < kTapFields; ++k) band[k * plane + si] = v[k];
-            }
-            __syncthreads();
-            if (!active) continue;
-            // this centre's window rows cy - hw .. cy + hw, as band rows
-            const int rlo = max(0, cy - A.hw - wy0 - yb), rhi = min(nrows - 1, cy + A.hw - wy0 - yb);
-            for (int r = rlo; r <= rhi; ++r) {
-                for (int dx = -A.hw; dx <= A.hw; ++dx) {
-                    const int x = cx + dx - wx0;
-                    const float *pp = band + r * q * A.sp + (x % A.sp) * q + x / A.sp;
-                    regression_tap(make_float3(pp[0], pp[plane], pp[2 * plane]), fc,
-                                   make_float3(pp[3 * plane], pp[4 * plane], pp[5 * plane]), pp[6 * plane], sc,
-                                   pp[7 * plane], vc,
-                                   make_float3(pp[8 * plane] - ac.x, pp[9 * plane] - ac.y, pp[10 * plane] - ac.z),
-                                   make_float3(pp[11 * plane] - nc.x, pp[12 * plane] - nc.y, pp[13 * plane] - nc.z),
-                                   u, beta, g);
-                    gf.x -= g.gdf.x;
-                    gf.y -= g.gdf.y;
-                    gf.z -= g.gdf.z;
-                    gs += g.gden;
-                    gv += g.gV;
-                    galb.x -= g.gda.x;
-                    galb.y -= g.gda.y;
-                    galb.z -= g.gda.z;
-                    gnn.x -= g.gdn.x;
-                    gnn.y -= g.gdn.y;
-                    gnn.z -= g.gdn.z;
-                }
-            }
-        }
-        if (active) {
-            add3(B_.gf, c, gf);
-            B_.gs[c] += gs;
-            B_.gv[c] += gv;
-        }
-    }
-    if (active) {
-        add3(A.galb, c, galb);
-        add3(A.gn, c, gnn);
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1183,26 +928,8 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
     } else {
         recon_grad_pixel_kernel<<<g_out, blk, 0, st>>>(A);
     }
-    // the banded form needs every centre's candidate ranges within 64 positions
-    const int cand = (2 * A.hw + 2 * A.sp) / A.rs + 2;
-    const size_t cb_smem = centre_band_smem(A.hw, A.sp, A.rs);
-    if (cand <= 64 && cb_smem <= 200 * 1024) {
-        if ((e = cudaFuncSetAttribute(recon_grad_centre_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)cb_smem)) != cudaSuccess)
-            return e;
-        recon_grad_centre_band_kernel<<<g_cen, blk, cb_smem, st>>>(A);
-    } else {
-        recon_grad_centre_kernel<<<g_cen, blk, 0, st>>>(A);
-    }
-    const size_t tb_smem = tap_band_smem(A.hw, A.sp);
-    if (tb_smem <= 200 * 1024) {
-        if ((e = cudaFuncSetAttribute(regression_grad_centre_band_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb_smem)) != cudaSuccess)
-            return e;
-        regression_grad_centre_band_kernel<<<g_cen, blk, tb_smem, st>>>(A);
-    } else {
-        regression_grad_centre_kernel<<<dim3((A.Ws + 15) / 16, (A.Hs + 7) / 8, B), dim3(16, 8), 0, st>>>(A);
-    }
+    recon_grad_centre_kernel<<<g_cen, blk, 0, st>>>(A);
+    regression_grad_centre_kernel<<<dim3((A.Ws + 15) / 16, (A.Hs + 7) / 8, B), dim3(16, 8), 0, st>>>(A);
     const size_t tg_smem = tap_grad_smem(A.hw, A.sp);
     if (tg_smem <= 200 * 1024) {
         if ((e = cudaFuncSetAttribute(regression_grad_tap_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

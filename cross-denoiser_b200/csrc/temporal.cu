@@ -25,6 +25,7 @@
 // path.  Its row pass slides the window over four output columns per
 // (channel, row, column group) item, in registers, on all threads.  Other window sizes and images whose rows are not a multiple
 // of 16 bytes take the tile-per-CTA kernel above it.
+#include <atomic>
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
 #include "tma.cuh"
@@ -482,26 +483,30 @@ cudaError_t launch_temporal_tma(const float *c1, const float *c2, const float *p
         !tma::encode_image(&m.h2, prev2, false, 3, W, H, B, G::HBOX, kTY) ||
         !tma::encode_image(&m.mk, raw, true, 1, W, H, B, G::MBOXX, G::MBOXY))
         return cudaSuccess;   // not eligible: the caller takes the tile-per-CTA kernel
-    static int occ[8] = {};
-    static int sms[64] = {};
+    // per-process caches (every thread computes the same values)
+    static std::atomic<int> occ_cache{0};
+    static std::atomic<int> sm_cache[64];
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(temporal_tma_kernel<HC>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM)) !=
         cudaSuccess)
         return e;
-    if (!occ[HC]) {
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[HC], temporal_tma_kernel<HC>, kTX * kTY,
-                                                                G::SMEM)) != cudaSuccess)
+    int occ = occ_cache.load(std::memory_order_relaxed);
+    if (!occ) {
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, temporal_tma_kernel<HC>, kTX * kTY, G::SMEM)) !=
+            cudaSuccess)
             return e;
-        if (occ[HC] < 1) return cudaSuccess;
+        if (occ < 1) return cudaSuccess;
+        occ_cache.store(occ, std::memory_order_relaxed);
     }
-    if (dev < 64 && !sms[dev] &&
-        (e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
-        return e;
-    const int nsm = dev < 64 ? sms[dev] : 148;
+    int nsm = dev < 64 ? sm_cache[dev].load(std::memory_order_relaxed) : 0;
+    if (!nsm) {
+        if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        if (dev < 64) sm_cache[dev].store(nsm, std::memory_order_relaxed);
+    }
     const int ntx = (W + kTX - 1) / kTX, nty = (H + kTY - 1) / kTY, ntiles = ntx * nty * B;
-    const int grid = min(ntiles, nsm * occ[HC]);
+    const int grid = min(ntiles, nsm * occ);
     temporal_tma_kernel<HC><<<grid, dim3(kTX, kTY), G::SMEM, st>>>(m, eroded, out, out1, out2, succ, H, W, ntx, nty,
                                                                    ntiles);
     *done = true;
