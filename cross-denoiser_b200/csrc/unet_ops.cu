@@ -220,29 +220,43 @@ __global__ void __launch_bounds__(kN) tconv_bwd_kernel(const __nv_bfloat16 *__re
     }
 }
 
-// Head: param = Kh^T c5_1 + bh (Kh[ci][co], 8 x 6), band = 1 / (p^2 + 1e-4), alpha = sigmoid(p5)
+// Head: param = Kh^T c5_1 + bh (Kh[ci][co], 8 x 6), band = 1 / (p^2 + 1e-4), alpha = sigmoid(p5).
+// A block's band values (five per pixel) go out through shared memory as
+// float4 stores.
 __global__ void __launch_bounds__(256) head_fwd_kernel(const __nv_bfloat16 *__restrict__ x, const float *__restrict__ K,
                                                        const float *__restrict__ bias, float *__restrict__ band,
                                                        float *__restrict__ alpha, size_t n)
 {
     __shared__ float sK[54];
-    if (threadIdx.x < 54) sK[threadIdx.x] = threadIdx.x < 48 ? K[threadIdx.x] : bias[threadIdx.x - 48];
+    __shared__ __align__(16) float sb[256 * 5];   // the block's band values, written out as float4
+    const int tid = threadIdx.x;
+    if (tid < 54) sK[tid] = tid < 48 ? K[tid] : bias[tid - 48];
     __syncthreads();
-    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    float v[8];
-    ld8(x + 8 * p, v);
-    float q[6];
+    const size_t p0 = (size_t)blockIdx.x * 256, p = p0 + tid;
+    if (p < n) {
+        float v[8];
+        ld8(x + 8 * p, v);
+        float q[6];
 #pragma unroll
-    for (int co = 0; co < 6; ++co) {
-        float s = sK[48 + co];
+        for (int co = 0; co < 6; ++co) {
+            float s = sK[48 + co];
 #pragma unroll
-        for (int ci = 0; ci < 8; ++ci) s = fmaf(sK[ci * 6 + co], v[ci], s);
-        q[co] = s;
+            for (int ci = 0; ci < 8; ++ci) s = fmaf(sK[ci * 6 + co], v[ci], s);
+            q[co] = s;
+        }
+#pragma unroll
+        for (int k = 0; k < 5; ++k) sb[5 * tid + k] = 1.f / (q[k] * q[k] + 1e-4f);
+        alpha[p] = 1.f / (1.f + expf(-q[5]));
     }
-#pragma unroll
-    for (int k = 0; k < 5; ++k) band[5 * p + k] = 1.f / (q[k] * q[k] + 1e-4f);
-    alpha[p] = 1.f / (1.f + expf(-q[5]));
+    __syncthreads();
+    const int cnt = 5 * (int)(n - p0 < 256 ? n - p0 : 256);
+    float *dst = band + 5 * p0;
+    int i = tid;
+    if (!(reinterpret_cast<uintptr_t>(dst) & 15)) {
+        for (; i < cnt / 4; i += 256) reinterpret_cast<float4 *>(dst)[i] = reinterpret_cast<const float4 *>(sb)[i];
+        i = (cnt / 4) * 4 + tid;
+    }
+    for (; i < cnt; i += 256) dst[i] = sb[i];
 }
 
 // Head backward: dZ of c5_1 (times its ReLU derivative) and the block's
@@ -263,13 +277,14 @@ __global__ void __launch_bounds__(kHeadThreads) head_bwd_kernel(const __nv_bfloa
 {
     __shared__ float sK[54];
     __shared__ float red[kHeadThreads / 32][54];
-    if (threadIdx.x < 54) sK[threadIdx.x] = threadIdx.x < 48 ? K[threadIdx.x] : bias[threadIdx.x - 48];
+    const int tid = threadIdx.x;
+    if (tid < 54) sK[tid] = tid < 48 ? K[tid] : bias[tid - 48];
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = tid & 31, warp = tid >> 5;
     float acc[54];
 #pragma unroll
     for (int j = 0; j < 54; ++j) acc[j] = 0.f;
-    for (size_t p = (size_t)blockIdx.x * kHeadThreads + threadIdx.x; p < n; p += (size_t)gridDim.x * kHeadThreads) {
+    for (size_t p = (size_t)blockIdx.x * kHeadThreads + tid; p < n; p += (size_t)gridDim.x * kHeadThreads) {
         float v[8], g[6];
         ld8(x + 8 * p, v);
 #pragma unroll
@@ -309,10 +324,10 @@ __global__ void __launch_bounds__(kHeadThreads) head_bwd_kernel(const __nv_bfloa
         if (lane == 0) red[warp][j] = s;
     }
     __syncthreads();
-    if (threadIdx.x < 54) {
+    if (tid < 54) {
         float s = 0.f;
-        for (int w = 0; w < kHeadThreads / 32; ++w) s += red[w][threadIdx.x];
-        partial[(size_t)blockIdx.x * 54 + threadIdx.x] = s;
+        for (int w = 0; w < kHeadThreads / 32; ++w) s += red[w][tid];
+        partial[(size_t)blockIdx.x * 54 + tid] = s;
     }
 }
 
