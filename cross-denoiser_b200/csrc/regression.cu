@@ -159,23 +159,30 @@ __global__ void __launch_bounds__(256) variance_px_kernel(const float *__restric
 //   shared (10): A00 A03 A04 A05 A33 A34 A35 A44 A45 A55
 //   per channel (11 x 3): A01 A02 A11 A12 A13 A14 A15 A22 A23 A24 A25
 //   right-hand side (6 x 3): X0..X5
+// The per-channel terms of channels 0 and 1 are packed FP32x2 pairs (low
+// lane channel 0) updated by one fma.rn.f32x2 each, channel 2 stays scalar:
+// every lane is rounded as the scalar update, in the same order.
 // ---------------------------------------------------------------------------
 struct Normal {
     float a00, a03, a04, a05, a33, a34, a35, a44, a45, a55;
-    float a01[3], a02[3], a11[3], a12[3], a13[3], a14[3], a15[3], a22[3], a23[3], a24[3], a25[3];
-    float x0[3], x1[3], x2[3], x3[3], x4[3], x5[3];
+    x2::f2 p01, p02, p11, p12, p13, p14, p15, p22, p23, p24, p25;   // channels 0, 1
+    x2::f2 px0, px1, px2, px3, px4, px5;
+    float q01, q02, q11, q12, q13, q14, q15, q22, q23, q24, q25;      // channel 2
+    float qx0, qx1, qx2, qx3, qx4, qx5;
 };
 
 CD_DEV void normal_zero(Normal &n)
 {
     n.a00 = n.a03 = n.a04 = n.a05 = n.a33 = n.a34 = n.a35 = n.a44 = n.a45 = n.a55 = 0.f;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        n.a01[k] = n.a02[k] = n.a11[k] = n.a12[k] = n.a13[k] = n.a14[k] = n.a15[k] = 0.f;
-        n.a22[k] = n.a23[k] = n.a24[k] = n.a25[k] = 0.f;
-        n.x0[k] = n.x1[k] = n.x2[k] = n.x3[k] = n.x4[k] = n.x5[k] = 0.f;
-    }
+    const x2::f2 z = x2::pack(0.f, 0.f);
+    n.p01 = n.p02 = n.p11 = n.p12 = n.p13 = n.p14 = n.p15 = n.p22 = n.p23 = n.p24 = n.p25 = z;
+    n.px0 = n.px1 = n.px2 = n.px3 = n.px4 = n.px5 = z;
+    n.q01 = n.q02 = n.q11 = n.q12 = n.q13 = n.q14 = n.q15 = n.q22 = n.q23 = n.q24 = n.q25 = 0.f;
+    n.qx0 = n.qx1 = n.qx2 = n.qx3 = n.qx4 = n.qx5 = 0.f;
 }
+
+// channel k (0, 1: a lane of the pair; 2: the scalar) of a per-channel term
+CD_DEV float chan(x2::f2 p, float q, int k) { return k == 0 ? x2::lo(p) : k == 1 ? x2::hi(p) : q; }
 
 // |v|^2 as the reference's compiled norm2 rounds it: fma(z, z, fma(x, x, y*y))
 // (the contraction the reference kernels were observed to use for
@@ -189,6 +196,7 @@ CD_DEV float sqnorm(float x, float y, float z) { return fmaf(z, z, fmaf(x, x, y 
 CD_DEV void normal_tap(Normal &n, float3 ft, float3 fc, float3 y, float vt, float vc, float sdt,
                        float sdc, const float da[3], const float dn[3])
 {
+    using namespace x2;
     const float df[3] = {ft.x - fc.x, ft.y - fc.y, ft.z - fc.z};
     const float den = (sdc + sdt) + 1e-2f;
     const float dist = sqnorm(df[0], df[1], df[2]) / ((vc + vt) + 1e-4f);
@@ -204,29 +212,48 @@ CD_DEV void normal_tap(Normal &n, float3 ft, float3 fc, float3 y, float vt, floa
     n.a44 = fmaf(wn1, dn[1], n.a44);
     n.a45 = fmaf(wn1, dn[2], n.a45);
     n.a55 = fmaf(wn2, dn[2], n.a55);
-    const float yv[3] = {y.x, y.y, y.z};
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float d1 = df[k] / den;
-        const float wd1 = w * d1, wd2 = w * da[k];
-        n.a01[k] = fmaf(w, d1, n.a01[k]);
-        n.a02[k] = fmaf(w, da[k], n.a02[k]);
-        n.a11[k] = fmaf(wd1, d1, n.a11[k]);
-        n.a12[k] = fmaf(wd1, da[k], n.a12[k]);
-        n.a13[k] = fmaf(wd1, dn[0], n.a13[k]);
-        n.a14[k] = fmaf(wd1, dn[1], n.a14[k]);
-        n.a15[k] = fmaf(wd1, dn[2], n.a15[k]);
-        n.a22[k] = fmaf(wd2, da[k], n.a22[k]);
-        n.a23[k] = fmaf(wd2, dn[0], n.a23[k]);
-        n.a24[k] = fmaf(wd2, dn[1], n.a24[k]);
-        n.a25[k] = fmaf(wd2, dn[2], n.a25[k]);
-        n.x0[k] = fmaf(w, yv[k], n.x0[k]);
-        n.x1[k] = fmaf(wd1, yv[k], n.x1[k]);
-        n.x2[k] = fmaf(wd2, yv[k], n.x2[k]);
-        n.x3[k] = fmaf(wn0, yv[k], n.x3[k]);
-        n.x4[k] = fmaf(wn1, yv[k], n.x4[k]);
-        n.x5[k] = fmaf(wn2, yv[k], n.x5[k]);
-    }
+    // channels 0 and 1
+    const f2 wP = pack(w, w), d1P = pack(df[0] / den, df[1] / den), daP = pack(da[0], da[1]);
+    const f2 wd1P = mul2(wP, d1P), wd2P = mul2(wP, daP);
+    const f2 dn0P = pack(dn[0], dn[0]), dn1P = pack(dn[1], dn[1]), dn2P = pack(dn[2], dn[2]);
+    const f2 yP = pack(y.x, y.y);
+    n.p01 = fma2(wP, d1P, n.p01);
+    n.p02 = fma2(wP, daP, n.p02);
+    n.p11 = fma2(wd1P, d1P, n.p11);
+    n.p12 = fma2(wd1P, daP, n.p12);
+    n.p13 = fma2(wd1P, dn0P, n.p13);
+    n.p14 = fma2(wd1P, dn1P, n.p14);
+    n.p15 = fma2(wd1P, dn2P, n.p15);
+    n.p22 = fma2(wd2P, daP, n.p22);
+    n.p23 = fma2(wd2P, dn0P, n.p23);
+    n.p24 = fma2(wd2P, dn1P, n.p24);
+    n.p25 = fma2(wd2P, dn2P, n.p25);
+    n.px0 = fma2(wP, yP, n.px0);
+    n.px1 = fma2(wd1P, yP, n.px1);
+    n.px2 = fma2(wd2P, yP, n.px2);
+    n.px3 = fma2(pack(wn0, wn0), yP, n.px3);
+    n.px4 = fma2(pack(wn1, wn1), yP, n.px4);
+    n.px5 = fma2(pack(wn2, wn2), yP, n.px5);
+    // channel 2
+    const float d1 = df[2] / den;
+    const float wd1 = w * d1, wd2 = w * da[2];
+    n.q01 = fmaf(w, d1, n.q01);
+    n.q02 = fmaf(w, da[2], n.q02);
+    n.q11 = fmaf(wd1, d1, n.q11);
+    n.q12 = fmaf(wd1, da[2], n.q12);
+    n.q13 = fmaf(wd1, dn[0], n.q13);
+    n.q14 = fmaf(wd1, dn[1], n.q14);
+    n.q15 = fmaf(wd1, dn[2], n.q15);
+    n.q22 = fmaf(wd2, da[2], n.q22);
+    n.q23 = fmaf(wd2, dn[0], n.q23);
+    n.q24 = fmaf(wd2, dn[1], n.q24);
+    n.q25 = fmaf(wd2, dn[2], n.q25);
+    n.qx0 = fmaf(w, y.z, n.qx0);
+    n.qx1 = fmaf(wd1, y.z, n.qx1);
+    n.qx2 = fmaf(wd2, y.z, n.qx2);
+    n.qx3 = fmaf(wn0, y.z, n.qx3);
+    n.qx4 = fmaf(wn1, y.z, n.qx4);
+    n.qx5 = fmaf(wn2, y.z, n.qx5);
 }
 
 // Cholesky factorisation + forward / backward substitution of one channel's
@@ -280,15 +307,19 @@ CD_DEV void solve_channel(const Normal &n, int k, float *beta, float *Lo, float 
                           unsigned *fallbacks = nullptr)
 {
     float A[kP][kP];
-    A[0][0] = n.a00; A[0][1] = n.a01[k]; A[0][2] = n.a02[k]; A[0][3] = n.a03; A[0][4] = n.a04; A[0][5] = n.a05;
-    A[1][1] = n.a11[k]; A[1][2] = n.a12[k]; A[1][3] = n.a13[k]; A[1][4] = n.a14[k]; A[1][5] = n.a15[k];
-    A[2][2] = n.a22[k]; A[2][3] = n.a23[k]; A[2][4] = n.a24[k]; A[2][5] = n.a25[k];
+    A[0][0] = n.a00; A[0][1] = chan(n.p01, n.q01, k); A[0][2] = chan(n.p02, n.q02, k);
+    A[0][3] = n.a03; A[0][4] = n.a04; A[0][5] = n.a05;
+    A[1][1] = chan(n.p11, n.q11, k); A[1][2] = chan(n.p12, n.q12, k); A[1][3] = chan(n.p13, n.q13, k);
+    A[1][4] = chan(n.p14, n.q14, k); A[1][5] = chan(n.p15, n.q15, k);
+    A[2][2] = chan(n.p22, n.q22, k); A[2][3] = chan(n.p23, n.q23, k); A[2][4] = chan(n.p24, n.q24, k);
+    A[2][5] = chan(n.p25, n.q25, k);
     A[3][3] = n.a33; A[3][4] = n.a34; A[3][5] = n.a35;
     A[4][4] = n.a44; A[4][5] = n.a45;
     A[5][5] = n.a55;
 #pragma unroll
     for (int r = 0; r < kP; ++r) A[r][r] += 1e-3f;
-    const float X[kP] = {n.x0[k], n.x1[k], n.x2[k], n.x3[k], n.x4[k], n.x5[k]};
+    const float X[kP] = {chan(n.px0, n.qx0, k), chan(n.px1, n.qx1, k), chan(n.px2, n.qx2, k),
+                         chan(n.px3, n.qx3, k), chan(n.px4, n.qx4, k), chan(n.px5, n.qx5, k)};
     float L[kP][kP];
 #pragma unroll
     for (int i = 0; i < kP; ++i) {
