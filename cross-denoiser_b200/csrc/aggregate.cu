@@ -255,10 +255,12 @@ CD_DEV float filter_epilogue(const fsw::Sums &s, const fsw::Centre &c, const Agg
 // (fsw::kExp2Ftz): the same values as the plain kernels' __expf wherever the
 // weight is a normal float, zero where it would be subnormal (below 2^-126),
 // so its sums equal cd_spatial_filter's except for contributions below the
-// smallest normal float.
+// smallest normal float.  Launch bound 2 CTAs per SM: 120 registers without
+// spills (a bound of 3 allows 80 and spills in the sweep); measured 736
+// against 745 us at 1920x1080, window 11.
 // ---------------------------------------------------------------------------
 template <int HW>
-__global__ void __launch_bounds__(256, 3) filter_aggregate_kernel(
+__global__ void __launch_bounds__(256, 2) filter_aggregate_kernel(
     const float *__restrict__ imga, const float *__restrict__ imgb, const float *__restrict__ albedo,
     const float *__restrict__ normal, const float *__restrict__ band, AggPtrs P,
     float *__restrict__ gband, int H, int W, int hw_rt, float inv_n)
