@@ -191,7 +191,10 @@ __device__ __forceinline__ void conv_out_row(const ConvParams &P, float (&v)[NOU
 // zero-initialised TMEM).  Compared with one MMA per output row and tap,
 // (R + 2) / (3 R) of the MMAs, each N = 3 NOUT wide (an MMA of M = 128,
 // K = 16 costs about the same for any N up to 64).
-template <int NOUT, int R, bool KYN>
+// NST > 0 (per-row form): P.nsteps as a template parameter, so that the
+// MMA thread builds every step's descriptors once, in registers, and issues
+// the R x NST MMAs without rebuilding them.
+template <int NOUT, int R, bool KYN, int NST = 0>
 __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P)
 {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -268,6 +271,25 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P)
                     const uint64_t bd = tc::sdesc(b0 + (uint32_t)(s * 2 * kRowsB * 16), kRowsB * 16, 128);
                     tc::mma_bf16(tbase + i * NOUT, ad, bd, idesc, 1u);
                 }
+        } else if (NST > 0) {
+            constexpr int kN = NST > 0 ? NST : 1;
+            const uint32_t idesc = tc::idesc_bf16(kPx, NOUT);
+            // row-0 A descriptor of each step, its row stride (16-byte units), B descriptor
+            uint64_t ad[kN], bd[kN];
+            uint32_t rs[kN];
+#pragma unroll
+            for (int s = 0; s < kN; ++s) {
+                const KStep st = P.steps[s];
+                const uint32_t base = st.src ? a1 + (uint32_t)(st.ky * P.c1) * kPlane : a0 + (uint32_t)(st.ky * P.c0) * kPlane;
+                ad[s] = tc::sdesc(base + st.a_off, st.a_lbo, 128);
+                rs[s] = (uint32_t)((st.src ? P.c1 : P.c0) * kPlane) >> 4;
+                bd[s] = tc::sdesc(b0 + (uint32_t)(s * 2 * NOUT * 16), NOUT * 16, 128);
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int s = 0; s < kN; ++s)
+                    tc::mma_bf16(tbase + r * NOUT, ad[s] + (uint64_t)(r * rs[s]), bd[s], idesc, s > 0 ? 1u : 0u);
         } else {
             const uint32_t idesc = tc::idesc_bf16(kPx, NOUT);
             for (int r = 0; r < R; ++r)
@@ -303,17 +325,32 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const ConvParams P)
     if (warp == 0) tc::tmem_dealloc(tbase, kCols);
 }
 
-template <int NOUT, int R, bool KYN>
+template <int NOUT, int R, bool KYN, int NST = 0>
 cudaError_t launch_t(const ConvParams &P, int B, cudaStream_t st)
 {
     constexpr int kCols = conv_cols<NOUT, R, KYN>();
     const size_t smem = smem_for_tmem(conv_smem(P.nsteps, KYN ? 3 * NOUT : NOUT, P.c0, P.c1, R), kCols);
-    cudaError_t e = cudaFuncSetAttribute(conv3x3_kernel<NOUT, R, KYN>,
+    cudaError_t e = cudaFuncSetAttribute(conv3x3_kernel<NOUT, R, KYN, NST>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid((P.W + kPx - 1) / kPx, (P.H + R - 1) / R, B);
-    conv3x3_kernel<NOUT, R, KYN><<<grid, 128, smem, st>>>(P);
+    conv3x3_kernel<NOUT, R, KYN, NST><<<grid, 128, smem, st>>>(P);
     return cudaGetLastError();
+}
+
+// Per-row form with the step count as a template parameter for the
+// network's 32- and 48-output layers (5, 6, 9 or 18 steps), the run-time
+// loop otherwise.
+template <int NOUT, int R>
+cudaError_t launch_rows(const ConvParams &P, int B, cudaStream_t st)
+{
+    switch (P.nsteps) {
+    case 5: return launch_t<NOUT, R, false, 5>(P, B, st);
+    case 6: return launch_t<NOUT, R, false, 6>(P, B, st);
+    case 9: return launch_t<NOUT, R, false, 9>(P, B, st);
+    case 18: return launch_t<NOUT, R, false, 18>(P, B, st);
+    default: return launch_t<NOUT, R, false>(P, B, st);
+    }
 }
 
 // Persistent, pipelined form of the ky-stacked convolution.  The same MMAs
@@ -1156,8 +1193,8 @@ cudaError_t launch_conv3x3(const ConvParams &P, int B, int nout, cudaStream_t st
         return cudaErrorInvalidValue;
     }
     if (nout == 16) return launch_t<16, kConvRows, false>(P, B, st);
-    if (nout == 32) return launch_t<32, kConvRows, false>(P, B, st);
-    if (nout == 48) return launch_t<48, kConvRows, false>(P, B, st);
+    if (nout == 32) return launch_rows<32, kConvRows>(P, B, st);
+    if (nout == 48) return launch_rows<48, kConvRows>(P, B, st);
     return cudaErrorInvalidValue;
 }
 
