@@ -111,10 +111,11 @@ __global__ void __launch_bounds__(256) tconv_fwd_kernel(const __nv_bfloat16 *__r
     }
 }
 
-// Conv2DTranspose backward: a block of kN input pixels computes
-// d_in = K^T d_out[2i,2j] (times the ReLU derivative of `in`), and the
-// block's partial sums of dK[co][ci] and db[co] (db over all four output
-// positions of each input pixel).
+// Conv2DTranspose backward: for every chunk of kN input pixels, d_in =
+// K^T d_out[2i,2j] (times the ReLU derivative of `in`) and the chunk's
+// contribution to dK[co][ci] and db[co] (db over all four output positions
+// of each input pixel).  Blocks walk chunks blockIdx.x, + gridDim.x, ...
+// and keep their dK / db sums in registers: one partial row per block.
 template <int CI, int CO, int kN>
 __global__ void __launch_bounds__(kN) tconv_bwd_kernel(const __nv_bfloat16 *__restrict__ in,
                                                         const __nv_bfloat16 *__restrict__ dout,
@@ -122,82 +123,86 @@ __global__ void __launch_bounds__(kN) tconv_bwd_kernel(const __nv_bfloat16 *__re
                                                         __nv_bfloat16 *__restrict__ dz_in, float *__restrict__ partial,
                                                         int Hi, int Wi, int B)
 {
+    // dK in 4 x 4 register tiles: kTiles tiles cover CO x CI, and the
+    // threads split into kGroups pixel groups, each summing its share of a
+    // chunk's pixels (in order) into every tile; the groups' sums are added
+    // in group order at the end.  Then db.
+    constexpr int TM = 4, TN = 4, kTiles = (CO / TM) * (CI / TN), kGroups = kN / kTiles;
+    static_assert(kGroups >= 1 && kGroups * kTiles == kN && kN % kGroups == 0, "tiles x groups cover the block");
     __shared__ __align__(16) float sK[CO * CI];
     __shared__ float sx[kN][CI + 1], sd[kN][CO + 1], sb[kN][CO + 1];
     for (int i = threadIdx.x; i < CO * CI; i += blockDim.x) sK[i] = K[i];
-    const size_t n = (size_t)B * Hi * Wi;
-    const size_t p = (size_t)blockIdx.x * kN + threadIdx.x;
+    const size_t n = (size_t)B * Hi * Wi, nchunk = (n + kN - 1) / kN;
     const int t = threadIdx.x;
-    float x[CI], d[CO];
+    const int tile = t % kTiles, grp = t / kTiles;
+    const int tci = tile % (CI / TN), tco = tile / (CI / TN);
+    const int ci0 = TN * tci, co0 = TM * tco;
+    constexpr int kPer = kN / kGroups;   // pixels of a chunk per group
+    float acc[TM][TN];
 #pragma unroll
-    for (int c = 0; c < CI; ++c) x[c] = 0.f;
+    for (int a = 0; a < TM; ++a)
 #pragma unroll
-    for (int c = 0; c < CO; ++c) d[c] = 0.f;
-    float bsum[CO];
+        for (int c = 0; c < TN; ++c) acc[a][c] = 0.f;
+    float bacc = 0.f;
+    for (size_t chunk = blockIdx.x; chunk < nchunk; chunk += gridDim.x) {
+        const size_t p = chunk * kN + t;
+        float x[CI], d[CO];
 #pragma unroll
-    for (int c = 0; c < CO; ++c) bsum[c] = 0.f;
-    const int xi = (int)(p % Wi), yi = (int)((p / Wi) % Hi), b = (int)(p / ((size_t)Wi * Hi));
-    if (p < n) {
+        for (int c = 0; c < CI; ++c) x[c] = 0.f;
 #pragma unroll
-        for (int c = 0; c < CI; c += 8) ld8(in + act_idx(b, yi, c / 8, xi, Hi, Wi, CI / 8) * 8, x + c);
-        const int Wo = 2 * Wi, Ho = 2 * Hi;
-        for (int a = 0; a < 4; ++a) {
-            const int yo = 2 * yi + (a >> 1), xo = 2 * xi + (a & 1);
-            float g[CO];
+        for (int c = 0; c < CO; ++c) d[c] = 0.f;
+        float bsum[CO];
 #pragma unroll
-            for (int c = 0; c < CO; c += 8) ld8(dout + act_idx(b, yo, c / 8, xo, Ho, Wo, CO / 8) * 8, g + c);
+        for (int c = 0; c < CO; ++c) bsum[c] = 0.f;
+        const int xi = (int)(p % Wi), yi = (int)((p / Wi) % Hi), b = (int)(p / ((size_t)Wi * Hi));
+        if (p < n) {
 #pragma unroll
-            for (int c = 0; c < CO; ++c) {
-                bsum[c] += g[c];
-                if (a == 0) d[c] = g[c];
-            }
-        }
-    }
+            for (int c = 0; c < CI; c += 8) ld8(in + act_idx(b, yi, c / 8, xi, Hi, Wi, CI / 8) * 8, x + c);
+            const int Wo = 2 * Wi, Ho = 2 * Hi;
+            for (int a = 0; a < 4; ++a) {
+                const int yo = 2 * yi + (a >> 1), xo = 2 * xi + (a & 1);
+                float g[CO];
 #pragma unroll
-    for (int c = 0; c < CI; ++c) sx[t][c] = x[c];
+                for (int c = 0; c < CO; c += 8) ld8(dout + act_idx(b, yo, c / 8, xo, Ho, Wo, CO / 8) * 8, g + c);
 #pragma unroll
-    for (int c = 0; c < CO; ++c) {
-        sd[t][c] = d[c];
-        sb[t][c] = bsum[c];
-    }
-    __syncthreads();
-    if (p < n) {
-        // co outer, ci inner: each g[ci] still sums over co in order, and a
-        // row of K is read as float4s
-        float g[CI];
-#pragma unroll
-        for (int ci = 0; ci < CI; ++ci) g[ci] = 0.f;
-#pragma unroll
-        for (int co = 0; co < CO; ++co) {
-            const float4 *kr = reinterpret_cast<const float4 *>(sK + co * CI);
-#pragma unroll
-            for (int c4 = 0; c4 < CI / 4; ++c4) {
-                const float4 k4 = kr[c4];
-                g[4 * c4] = fmaf(k4.x, d[co], g[4 * c4]);
-                g[4 * c4 + 1] = fmaf(k4.y, d[co], g[4 * c4 + 1]);
-                g[4 * c4 + 2] = fmaf(k4.z, d[co], g[4 * c4 + 2]);
-                g[4 * c4 + 3] = fmaf(k4.w, d[co], g[4 * c4 + 3]);
+                for (int c = 0; c < CO; ++c) {
+                    bsum[c] += g[c];
+                    if (a == 0) d[c] = g[c];
+                }
             }
         }
 #pragma unroll
-        for (int ci = 0; ci < CI; ++ci) g[ci] = x[ci] > 0.f ? g[ci] : 0.f;
+        for (int c = 0; c < CI; ++c) sx[t][c] = x[c];
 #pragma unroll
-        for (int c = 0; c < CI; c += 8) st8(dz_in + act_idx(b, yi, c / 8, xi, Hi, Wi, CI / 8) * 8, g + c);
-    }
-    float *out = partial + (size_t)blockIdx.x * (CO * CI + CO);
-    // dK in TM x TN register tiles (each output sums over the block's pixels
-    // in order), then db
-    constexpr int TN = (CO * CI) / kN >= 4 ? 4 : (CO * CI) / kN, TM = (CO * CI) / (kN * TN);
-    static_assert(TM >= 1 && TM * TN * kN == CO * CI && CI % TN == 0 && CO % TM == 0, "register tiles cover dK");
-    {
-        const int tci = t % (CI / TN), tco = t / (CI / TN);
-        const int ci0 = TN * tci, co0 = TM * tco;
-        float s[TM][TN];
+        for (int c = 0; c < CO; ++c) {
+            sd[t][c] = d[c];
+            sb[t][c] = bsum[c];
+        }
+        __syncthreads();
+        if (p < n) {
+            // co outer, ci inner: each g[ci] still sums over co in order, and a
+            // row of K is read as float4s
+            float g[CI];
 #pragma unroll
-        for (int a = 0; a < TM; ++a)
+            for (int ci = 0; ci < CI; ++ci) g[ci] = 0.f;
 #pragma unroll
-            for (int c = 0; c < TN; ++c) s[a][c] = 0.f;
-        for (int k = 0; k < kN; ++k) {
+            for (int co = 0; co < CO; ++co) {
+                const float4 *kr = reinterpret_cast<const float4 *>(sK + co * CI);
+#pragma unroll
+                for (int c4 = 0; c4 < CI / 4; ++c4) {
+                    const float4 k4 = kr[c4];
+                    g[4 * c4] = fmaf(k4.x, d[co], g[4 * c4]);
+                    g[4 * c4 + 1] = fmaf(k4.y, d[co], g[4 * c4 + 1]);
+                    g[4 * c4 + 2] = fmaf(k4.z, d[co], g[4 * c4 + 2]);
+                    g[4 * c4 + 3] = fmaf(k4.w, d[co], g[4 * c4 + 3]);
+                }
+            }
+#pragma unroll
+            for (int ci = 0; ci < CI; ++ci) g[ci] = x[ci] > 0.f ? g[ci] : 0.f;
+#pragma unroll
+            for (int c = 0; c < CI; c += 8) st8(dz_in + act_idx(b, yi, c / 8, xi, Hi, Wi, CI / 8) * 8, g + c);
+        }
+        for (int k = grp * kPer; k < (grp + 1) * kPer; ++k) {
             float dv[TM], xv[TN];
 #pragma unroll
             for (int a = 0; a < TM; ++a) dv[a] = sd[k][co0 + a];
@@ -206,18 +211,35 @@ __global__ void __launch_bounds__(kN) tconv_bwd_kernel(const __nv_bfloat16 *__re
 #pragma unroll
             for (int a = 0; a < TM; ++a)
 #pragma unroll
-                for (int c = 0; c < TN; ++c) s[a][c] = fmaf(dv[a], xv[c], s[a][c]);
+                for (int c = 0; c < TN; ++c) acc[a][c] = fmaf(dv[a], xv[c], acc[a][c]);
         }
+        if (t < CO)
+            for (int k = 0; k < kN; ++k) bacc += sb[k][t];
+        __syncthreads();   // the chunk's tiles are read before the next one is written
+    }
+    float *out = partial + (size_t)blockIdx.x * (CO * CI + CO);
+    if (kGroups == 1) {
 #pragma unroll
         for (int a = 0; a < TM; ++a)
 #pragma unroll
-            for (int c = 0; c < TN; ++c) out[(co0 + a) * CI + ci0 + c] = s[a][c];
+            for (int c = 0; c < TN; ++c) out[(co0 + a) * CI + ci0 + c] = acc[a][c];
+    } else {
+        // the groups' tiles through shared memory (sx is free now: kN x (CI + 1)
+        // floats hold the kGroups x CO x CI sums)
+        float *red = &sx[0][0];
+        static_assert(kGroups * CO * CI <= kN * (CI + 1), "the group sums fit sx");
+#pragma unroll
+        for (int a = 0; a < TM; ++a)
+#pragma unroll
+            for (int c = 0; c < TN; ++c) red[(grp * CO + co0 + a) * CI + ci0 + c] = acc[a][c];
+        __syncthreads();
+        for (int j = t; j < CO * CI; j += kN) {
+            float v = 0.f;
+            for (int g = 0; g < kGroups; ++g) v += red[g * CO * CI + j];
+            out[j] = v;
+        }
     }
-    if (t < CO) {
-        float s = 0.f;
-        for (int k = 0; k < kN; ++k) s += sb[k][t];
-        out[CO * CI + t] = s;
-    }
+    if (t < CO) out[CO * CI + t] = bacc;
 }
 
 // Head: param = Kh^T c5_1 + bh (Kh[ci][co], 8 x 6), band = 1 / (p^2 + 1e-4), alpha = sigmoid(p5).
@@ -293,8 +315,11 @@ __global__ void __launch_bounds__(kHeadThreads) head_bwd_kernel(const __nv_bfloa
 #pragma unroll
             for (int ci = 0; ci < 8; ++ci) s = fmaf(sK[ci * 6 + co], v[ci], s);
             if (co < 5) {
-                const float den = s * s + 1e-4f;
-                g[co] = __ldg(gband + 5 * p + co) * (-2.f * s / (den * den));
+                // d band / d s = -2 s / (s^2 + 1e-4)^2, with one fast
+                // reciprocal (a gradient: FP32 tolerance, not the forward's
+                // rounding)
+                const float r = __fdividef(1.f, s * s + 1e-4f);
+                g[co] = __ldg(gband + 5 * p + co) * (-2.f * s * r * r);
             } else {
                 const float a = 1.f / (1.f + expf(-s));
                 g[co] = __ldg(galpha + p) * a * (1.f - a);
@@ -448,10 +473,14 @@ cudaError_t launch_tconv_fwd(int ci, int co, const __nv_bfloat16 *in, const floa
 // pixels per block of the transposed-conv backward (static shared memory < 48 KB)
 static int tconv_bwd_px(int ci) { return ci == 32 ? 64 : 128; }
 
+// Blocks of the transposed-conv backward (and partial rows it writes): one
+// per chunk of input pixels up to 8 per SM of a 148-SM part.
+constexpr size_t kTconvMaxBlocks = 1184;
 size_t tconv_blocks(int ci, int Hi, int Wi, int B)
 {
     const int k = tconv_bwd_px(ci);
-    return ((size_t)B * Hi * Wi + k - 1) / k;
+    const size_t chunks = ((size_t)B * Hi * Wi + k - 1) / k;
+    return chunks < kTconvMaxBlocks ? chunks : kTconvMaxBlocks;
 }
 
 cudaError_t launch_tconv_bwd(int ci, int co, const __nv_bfloat16 *in, const __nv_bfloat16 *dout, const float *K,
