@@ -416,12 +416,15 @@ CD_API cd_status cd_unet_conv3x3_wgrad(const void *x, const void *dz, float *gra
 CD_API cd_status cd_fp32_fma_probe(float *out, int blocks, int iters, cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
-/* Persistent image kernel (no counterpart in the reference).  The fused    */
-/* erosion + temporal screening with win_prev = 1 runs as a persistent      */
-/* kernel that stages its tiles by TMA and waits on an mbarrier with a      */
-/* bounded number of polls, when the images' rows (and the mask's) are a    */
-/* multiple of 16 bytes and the tensors 16-byte aligned; otherwise, or when */
-/* disabled here, the tile-per-CTA kernel runs.  Both give the same results.*/
+/* Persistent kernels (no counterpart in the reference).  The fused erosion */
+/* + temporal screening with win_prev = 1 runs as a persistent kernel that  */
+/* stages its tiles by TMA and waits on an mbarrier with a bounded number   */
+/* of polls, when the images' rows (and the mask's) are a multiple of 16    */
+/* bytes and the tensors 16-byte aligned; the U-Net's convolutions with 16  */
+/* outputs run as a persistent warp-specialised kernel (staging ring, MMA   */
+/* thread, epilogue warps over two TMEM accumulator buffers) in the same    */
+/* arithmetic order as the one-tile-per-CTA kernel.  Otherwise, or when     */
+/* disabled here, the tile-per-CTA kernels run.  Both give the same results.*/
 /* cd_image_kernel_error_flags: bit 0 = a screening staging wait ran out    */
 /* (the tile's outputs are then not written); the bit only grows.  Read     */
 /* synchronously; -1 if the read fails.                                     */

@@ -3,7 +3,8 @@ restatement oracle/unet_torch.py.
 
 Both forms of the 3x3 convolution kernels (ky-stacked MMAs, the default,
 and one MMA per output row and tap) are checked layer by layer and for the
-whole network.
+whole network, and the persistent ky-stacked kernel against the
+one-tile-per-CTA one (bit-identical).
 
 Tolerances (bf16 operands and stored activations, fp32 accumulation):
   single layer vs the same bf16-rounded operands in fp32:
@@ -202,6 +203,34 @@ def test_unet_backward_and_adam(cd, cuda, conv_form):
         net.apply_gradients()
     torch.cuda.synchronize()
     np.testing.assert_allclose(N(net.params), w64.numpy(), rtol=1e-5, atol=1e-7)
+
+
+def test_persistent_conv_matches_per_tile(cd, cuda):
+    """The persistent warp-specialised convolution (16-output layers) issues
+    the one-tile-per-CTA kernel's MMAs in the same order into the same
+    accumulator layout: forward outputs and every parameter gradient are
+    bit-identical with the persistent kernels on and off, at a shape with
+    ragged tiles (H not a multiple of 4 rows at every level, W of 128)."""
+    L = cd._lib.lib()
+    B, H, W = 2, 76, 392
+    ins = [t.to(DEV) for t in frame_inputs(B, H, W, 11)]
+    g = torch.Generator().manual_seed(12)
+    gb = torch.randn((B, H, W, 5), generator=g).to(DEV)
+    ga = torch.randn((B, H, W, 1), generator=g).to(DEV)
+    out = {}
+    try:
+        for on in (1, 0):
+            L.cd_set_persistent_kernels(on)
+            net = well_conditioned_net(cd, 9)
+            band, alpha = net(*ins)
+            grads = net.backward(gb, ga)
+            torch.cuda.synchronize()
+            assert net.error_flag() == 0
+            out[on] = (band.clone(), alpha.clone(), grads.clone())
+    finally:
+        L.cd_set_persistent_kernels(1)
+    for a, b, what in zip(out[1], out[0], ("band", "alpha", "parameter gradients")):
+        assert torch.equal(a, b), f"{what} differ between the persistent and per-tile convolutions"
 
 
 def test_shape_errors(cd, cuda):
