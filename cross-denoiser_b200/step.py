@@ -86,6 +86,7 @@ class FrameStep:
         self.predictor = predictor
         self.on_gradients = on_gradients
         self.history: Optional[History] = None
+        self._ones: Optional[torch.Tensor] = None
         self.fixed_band: Optional[torch.Tensor] = None
         self.fixed_alpha: Optional[torch.Tensor] = None
         self._train_stream: Optional[torch.cuda.Stream] = None
@@ -138,8 +139,13 @@ class FrameStep:
         h = self.history
         albedo, normal = f["albedo"], f["normal"]
 
+        # the reference reprojects with opacity 1 everywhere (scripts/main.py:266):
+        # one constant tensor per shape, not a fill per frame
+        if self._ones is None or self._ones.shape != (B, H, W, 1) or self._ones.device != color.device:
+            self._ones = torch.ones((B, H, W, 1), dtype=torch.float32, device=color.device)
+        ones1 = self._ones
+
         def reproject():
-            ones1 = torch.ones((B, H, W, 1), dtype=torch.float32, device=color.device)
             return ops.Reproject(f["mvec"], [h.out_log, h.ols1, h.ols2], f["linearZ"], h.linearZ, normal,
                                  h.normal, f["pnFwidth"], ones1, ones1)
 
