@@ -303,8 +303,9 @@ def differentiation_costs(device, stream):
     """512x512, batch 4, radius 7: the spatial filter's band gradient by
     recomputation (this repository's design) against the reference's design
     (the forward stores 128 B/px of partials, the gradient reads them), and
-    the regression backward: time per call and the extra device memory each
-    needs beyond the op's inputs and outputs."""
+    the regression backward, recomputing its forward or reusing a kept one:
+    time per call and the extra device memory each needs beyond the op's
+    inputs and outputs."""
     B, H, W, win = 4, 512, 512, 15
     frames = make_frames(H, W, 2, 77, device)
     f = frames[1]
@@ -340,7 +341,12 @@ def differentiation_costs(device, stream):
     gu = [torch.randn((B, H, W, c), generator=g, device=device) for c in (3, 3, 1, 1)]
     rb = timed(lambda: ops.cross_regression_grad(*gu, *y, win, 4, 1), n=10)
     ws = cd._lib.lib().cd_cross_regression_grad_workspace_size(B, H, W, 4, 1)
-    out["regression"] = {"forward_ms": round(rf, 4), "backward_ms": round(rb, 4), "backward_workspace_bytes": int(ws)}
+    # the training pair: a forward that keeps its state, a backward that reuses it
+    _, kept = ops.cross_regression_keep(*y, win, 4, 1)
+    rfk = timed(lambda: ops.cross_regression_keep(*y, win, 4, 1), n=10)
+    rbk = timed(lambda: ops.cross_regression_grad_kept(*gu, *y, win, 4, 1, kept), n=10)
+    out["regression"] = {"forward_ms": round(rf, 4), "backward_ms": round(rb, 4), "backward_workspace_bytes": int(ws),
+                         "forward_keep_ms": round(rfk, 4), "backward_kept_ms": round(rbk, 4)}
     return out
 
 

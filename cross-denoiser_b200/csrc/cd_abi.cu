@@ -194,6 +194,50 @@ cd_status cd_cross_regression_grad(const float *imga, const float *imgb, const f
                        "cross_regression_grad");
 }
 
+cd_status cd_cross_regression_keep(const float *imga, const float *imgb, const float *albedo, const float *normal,
+                                   float *outa, float *outb, float *vara, float *varb, int B, int H, int W,
+                                   int win_size, int sparsity, int recon_scale, void *grad_workspace,
+                                   size_t grad_workspace_bytes, cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!imga || !imgb || !albedo || !normal || !outa || !outb || !vara || !varb)
+        return fail(CD_EINVAL, "cross_regression_keep: null tensor pointer");
+    cd_status s = check_regression("cross_regression_keep", B, H, W, win_size, sparsity, recon_scale);
+    if (s != CD_OK) return s;
+    const size_t need = cd_cross_regression_grad_workspace_size(B, H, W, sparsity, recon_scale);
+    if (grad_workspace_bytes < need || !grad_workspace)
+        return fail(CD_ENOMEM, "cross_regression_keep: workspace of %zu bytes needed, %zu given", need,
+                    grad_workspace_bytes);
+    return cuda_status(cd::launch_regression_keep(imga, imgb, albedo, normal, outa, outb, vara, varb, B, H, W,
+                                                  win_size, sparsity, recon_scale,
+                                                  static_cast<float *>(grad_workspace), stream),
+                       "cross_regression_keep");
+}
+
+cd_status cd_cross_regression_grad_kept(const float *imga, const float *imgb, const float *albedo,
+                                        const float *normal, const float *grad_outa, const float *grad_outb,
+                                        const float *grad_vara, const float *grad_varb, float *grad_imga,
+                                        float *grad_imgb, float *grad_albedo, float *grad_normal, int B, int H,
+                                        int W, int win_size, int sparsity, int recon_scale, void *grad_workspace,
+                                        size_t grad_workspace_bytes, cudaStream_t stream)
+{
+    g_err[0] = 0;
+    if (!imga || !imgb || !albedo || !normal || !grad_outa || !grad_outb || !grad_imga || !grad_imgb ||
+        !grad_albedo || !grad_normal)
+        return fail(CD_EINVAL, "cross_regression_grad_kept: null tensor pointer");
+    cd_status s = check_regression("cross_regression_grad_kept", B, H, W, win_size, sparsity, recon_scale);
+    if (s != CD_OK) return s;
+    const size_t need = cd_cross_regression_grad_workspace_size(B, H, W, sparsity, recon_scale);
+    if (grad_workspace_bytes < need || !grad_workspace)
+        return fail(CD_ENOMEM, "cross_regression_grad_kept: workspace of %zu bytes needed, %zu given", need,
+                    grad_workspace_bytes);
+    return cuda_status(cd::launch_regression_grad(imga, imgb, albedo, normal, grad_outa, grad_outb, grad_vara,
+                                                  grad_varb, grad_imga, grad_imgb, grad_albedo, grad_normal, B, H,
+                                                  W, win_size, sparsity, recon_scale,
+                                                  static_cast<float *>(grad_workspace), stream, true),
+                       "cross_regression_grad_kept");
+}
+
 cd_status cd_spatial_filter(const float *imga, const float *imgb, const float *albedo,
                             const float *normal, const float *band, float *out_acca,
                             float *out_accb, float *out_wgtsuma, float *out_wgtsumb, int B, int H,

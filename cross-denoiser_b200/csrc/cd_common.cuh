@@ -54,12 +54,18 @@ size_t regression_smem_bytes(int win, int sparsity);
 // CrossRegression backward (regression_grad.cu); ws holds
 // regression_grad_workspace_floats() floats.
 size_t regression_grad_workspace_floats(int B, int H, int W, int sparsity, int recon_scale);
+// kept: the workspace already holds the forward's quantities, written by
+// launch_regression_keep (the forward's outputs plus those quantities).
 cudaError_t launch_regression_grad(const float *imga, const float *imgb, const float *albedo,
                                    const float *normal, const float *g_outa, const float *g_outb,
                                    const float *g_vara, const float *g_varb, float *g_imga,
                                    float *g_imgb, float *g_albedo, float *g_normal, int B, int H,
                                    int W, int win, int sparsity, int recon_scale, float *ws,
-                                   cudaStream_t st);
+                                   cudaStream_t st, bool kept = false);
+cudaError_t launch_regression_keep(const float *imga, const float *imgb, const float *albedo,
+                                   const float *normal, float *outa, float *outb, float *vara,
+                                   float *varb, int B, int H, int W, int win, int sparsity,
+                                   int recon_scale, float *ws, cudaStream_t st);
 size_t recon_smem_bytes(int win, int sparsity, int recon_scale);
 
 size_t spatial_filter_smem_bytes(int win);

@@ -845,11 +845,33 @@ size_t regression_grad_workspace_floats(int B, int H, int W, int sp, int rs)
     return 2 * (13 * P + 117 * C + 4 * R) + 6 * P;
 }
 
+// The workspace begins with the forward's quantities, in this order:
+// variance and standard deviation of A, then of B (P floats each), the
+// coefficients [buf][C][18] and the Cholesky factors [buf][C][63].
+cudaError_t launch_regression_keep(const float *imga, const float *imgb, const float *albedo, const float *normal,
+                                   float *outa, float *outb, float *vara, float *varb, int B, int H, int W, int win,
+                                   int sp, int rs, float *ws, cudaStream_t st)
+{
+    const size_t P = (size_t)B * H * W, C = (size_t)B * (H / sp) * (W / sp);
+    float *v0 = ws, *s0 = ws + P, *v1 = ws + 2 * P, *s1 = ws + 3 * P;
+    float *beta = ws + 4 * P, *L = beta + 2 * C * kBeta;
+    cudaError_t e;
+    if ((e = launch_variance(imga, imgb, v0, v1, s0, s1, B, H, W, st)) != cudaSuccess) return e;
+    if ((e = launch_regression(imga, imgb, albedo, normal, v0, v1, s0, s1, beta, B, H, W, win, sp, st, L)) !=
+        cudaSuccess)
+        return e;
+    if ((e = launch_recon(imga, imgb, albedo, normal, v0, v1, s0, s1, beta, outa, outb, B, H, W, win, sp, rs, st)) !=
+        cudaSuccess)
+        return e;
+    if ((e = cudaMemcpyAsync(vara, v0, P * sizeof(float), cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+    return cudaMemcpyAsync(varb, v1, P * sizeof(float), cudaMemcpyDeviceToDevice, st);
+}
+
 cudaError_t launch_regression_grad(const float *imga, const float *imgb, const float *albedo, const float *normal,
                                    const float *g_outa, const float *g_outb, const float *g_vara,
                                    const float *g_varb, float *g_imga, float *g_imgb, float *g_albedo,
                                    float *g_normal, int B, int H, int W, int win, int sp, int rs, float *ws,
-                                   cudaStream_t st)
+                                   cudaStream_t st, bool kept)
 {
     const size_t P = (size_t)B * H * W, R = (size_t)B * (H / rs) * (W / rs), C = (size_t)B * (H / sp) * (W / sp);
     GArgs A{};
@@ -911,11 +933,14 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
     cudaError_t e = cudaMemsetAsync(zero_begin, 0, (size_t)(cur - zero_begin) * sizeof(float), st);
     if (e != cudaSuccess) return e;
 
-    // pass 1: forward quantities (variance, std, coefficients, Cholesky factors)
-    if ((e = launch_variance(imga, imgb, var[0], var[1], sd[0], sd[1], B, H, W, st)) != cudaSuccess) return e;
-    if ((e = launch_regression(imga, imgb, albedo, normal, var[0], var[1], sd[0], sd[1], beta, B, H, W, win, sp,
-                               st, L)) != cudaSuccess)
-        return e;
+    // pass 1: forward quantities (variance, std, coefficients, Cholesky
+    // factors), unless launch_regression_keep left them in the workspace
+    if (!kept) {
+        if ((e = launch_variance(imga, imgb, var[0], var[1], sd[0], sd[1], B, H, W, st)) != cudaSuccess) return e;
+        if ((e = launch_regression(imga, imgb, albedo, normal, var[0], var[1], sd[0], sd[1], beta, B, H, W, win,
+                                   sp, st, L)) != cudaSuccess)
+            return e;
+    }
     dim3 blk(32, 8);
     dim3 g_out((A.Wr + 31) / 32, (A.Hr + 7) / 8, B), g_cen((A.Ws + 31) / 32, (A.Hs + 7) / 8, B);
     dim3 g_px((W + 31) / 32, (H + 7) / 8, B);

@@ -106,13 +106,14 @@ def _cross_regression_raw(imga, imgb, albedo, normal, win_size, sparsity, recon_
 
 
 def cross_regression_grad(grad_outa, grad_outb, grad_vara, grad_varb, imga, imgb, albedo, normal,
-                          win_size: int, sparsity: int, recon_scale: int = 1):
+                          win_size: int, sparsity: int, recon_scale: int = 1, _kept=None):
     """(grad_imga, grad_imgb, grad_albedo, grad_normal) of CrossRegression.
 
     No counterpart in the reference, which registers a gradient only for
     SpatialFilter (scripts/ops.py:23-32).  The analytic derivative of the
     forward above; grad_vara / grad_varb may be None.  The forward is
-    recomputed, so only its inputs are needed.
+    recomputed, so only its inputs are needed (cross_regression_grad_kept
+    reuses a kept forward instead).
     """
     imga, imgb, albedo, normal, rs = _regression_args(imga, imgb, albedo, normal, win_size, sparsity,
                                                       recon_scale)
@@ -132,24 +133,62 @@ def cross_regression_grad(grad_outa, grad_outb, grad_vara, grad_varb, imga, imgb
     L = _lib.lib()
     outs = [torch.empty_like(imga) for _ in range(4)]
     nbytes = L.cd_cross_regression_grad_workspace_size(B, H, W, int(sparsity), rs)
-    ws = torch.empty((max(nbytes, 1),), dtype=torch.uint8, device=imga.device)
-    _lib.check(L.cd_cross_regression_grad(
+    if _kept is None:
+        ws, fn, name = torch.empty((max(nbytes, 1),), dtype=torch.uint8, device=imga.device), \
+            L.cd_cross_regression_grad, "cross_regression_grad"
+    else:
+        if _kept.dtype != torch.uint8 or _kept.numel() < nbytes or _kept.device != imga.device:
+            raise ValueError(f"workspace must be a uint8 tensor of >= {nbytes} bytes on {imga.device}")
+        ws, fn, name = _kept, L.cd_cross_regression_grad_kept, "cross_regression_grad_kept"
+    _lib.check(fn(
         _ptr(imga), _ptr(imgb), _ptr(albedo), _ptr(normal), _ptr(grad_outa), _ptr(grad_outb),
         None if gv[0] is None else _ptr(gv[0]), None if gv[1] is None else _ptr(gv[1]),
-        *[_ptr(o) for o in outs], B, H, W, int(win_size), int(sparsity), rs, _ptr(ws), nbytes,
-        _stream()), "cross_regression_grad")
+        *[_ptr(o) for o in outs], B, H, W, int(win_size), int(sparsity), rs, _ptr(ws), ws.numel(),
+        _stream()), name)
     return tuple(outs)
 
 
+def cross_regression_keep(imga, imgb, albedo, normal, win_size: int, sparsity: int, recon_scale: int = 1):
+    """cross_regression's four outputs (bit-identical) and a workspace that
+    keeps the forward's variances, coefficients and Cholesky factors for
+    cross_regression_grad_kept (cd_cross_regression_keep).  No counterpart in
+    the reference.  Returns ((outa, outb, out_vara, out_varb), workspace)."""
+    imga, imgb, albedo, normal, rs = _regression_args(imga, imgb, albedo, normal, win_size, sparsity,
+                                                      recon_scale)
+    B, H, W, _ = imga.shape
+    outa = imga.new_empty((B, H // rs, W // rs, 3))
+    outb = imga.new_empty((B, H // rs, W // rs, 3))
+    vara = imga.new_empty((B, H, W, 1))
+    varb = imga.new_empty((B, H, W, 1))
+    L = _lib.lib()
+    nbytes = L.cd_cross_regression_grad_workspace_size(B, H, W, int(sparsity), rs)
+    ws = torch.empty((max(nbytes, 1),), dtype=torch.uint8, device=imga.device)
+    _lib.check(L.cd_cross_regression_keep(_ptr(imga), _ptr(imgb), _ptr(albedo), _ptr(normal), _ptr(outa),
+                                          _ptr(outb), _ptr(vara), _ptr(varb), B, H, W, int(win_size),
+                                          int(sparsity), rs, _ptr(ws), nbytes, _stream()),
+               "cross_regression_keep")
+    return (outa, outb, vara, varb), ws
+
+
+def cross_regression_grad_kept(grad_outa, grad_outb, grad_vara, grad_varb, imga, imgb, albedo, normal,
+                               win_size: int, sparsity: int, recon_scale: int, workspace: torch.Tensor):
+    """cross_regression_grad's result (bit-identical) from the workspace of
+    cross_regression_keep on the same inputs, without recomputing the
+    forward (cd_cross_regression_grad_kept)."""
+    return cross_regression_grad(grad_outa, grad_outb, grad_vara, grad_varb, imga, imgb, albedo, normal,
+                                 win_size, sparsity, recon_scale, _kept=workspace)
+
+
 class _CrossRegressionFn(torch.autograd.Function):
-    """Autograd wrapper: forward cd_cross_regression, backward
-    cd_cross_regression_grad."""
+    """Autograd wrapper: forward cd_cross_regression_keep, backward
+    cd_cross_regression_grad_kept on the kept workspace."""
 
     @staticmethod
     def forward(ctx, imga, imgb, albedo, normal, win_size, sparsity, recon_scale):
-        outs = _cross_regression_raw(imga, imgb, albedo, normal, win_size, sparsity, recon_scale)
+        outs, ws = cross_regression_keep(imga, imgb, albedo, normal, win_size, sparsity, recon_scale)
         ctx.save_for_backward(imga, imgb, albedo, normal)
         ctx.attrs = (int(win_size), int(sparsity), int(recon_scale))
+        ctx.ws = ws
         return outs
 
     @staticmethod
@@ -161,8 +200,9 @@ class _CrossRegressionFn(torch.autograd.Function):
             g_outa = imga.new_zeros((B, H // rs, W // rs, 3))
         if g_outb is None:
             g_outb = imga.new_zeros((B, H // rs, W // rs, 3))
-        grads = cross_regression_grad(g_outa, g_outb, g_vara, g_varb, imga, imgb, albedo, normal,
-                                      *ctx.attrs)
+        grads = cross_regression_grad_kept(g_outa, g_outb, g_vara, g_varb, imga, imgb, albedo, normal,
+                                           *ctx.attrs, ctx.ws)
+        ctx.ws = None
         return (*grads, None, None, None)
 
 

@@ -130,6 +130,36 @@ CD_API cd_status cd_cross_regression_grad(const float *imga, const float *imgb,
                                           cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* Forward and backward of CrossRegression without the backward's recompute */
+/* (no counterpart in the reference).  cd_cross_regression_keep computes    */
+/* cd_cross_regression's four outputs (bit-identical) and leaves the        */
+/* variances, standard deviations, coefficients and Cholesky factors in a   */
+/* workspace of cd_cross_regression_grad_workspace_size() bytes;            */
+/* cd_cross_regression_grad_kept then computes cd_cross_regression_grad's   */
+/* result (bit-identical) from that workspace without recomputing the       */
+/* forward.  Pass the same inputs, attributes and workspace to both, and    */
+/* nothing else may write the workspace in between.                         */
+/* ------------------------------------------------------------------------ */
+CD_API cd_status cd_cross_regression_keep(const float *imga, const float *imgb,
+                                          const float *albedo, const float *normal,
+                                          float *outa, float *outb, float *vara, float *varb,
+                                          int B, int H, int W,
+                                          int win_size, int sparsity, int recon_scale,
+                                          void *grad_workspace, size_t grad_workspace_bytes,
+                                          cudaStream_t stream);
+
+CD_API cd_status cd_cross_regression_grad_kept(const float *imga, const float *imgb,
+                                               const float *albedo, const float *normal,
+                                               const float *grad_outa, const float *grad_outb,
+                                               const float *grad_vara, const float *grad_varb,
+                                               float *grad_imga, float *grad_imgb,
+                                               float *grad_albedo, float *grad_normal,
+                                               int B, int H, int W,
+                                               int win_size, int sparsity, int recon_scale,
+                                               void *grad_workspace, size_t grad_workspace_bytes,
+                                               cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
 /* CrossRegression without a workspace (no counterpart in the reference).    */
 /* For callers that cannot allocate device memory when the op runs: a       */
 /* renderer's or engine's frame loop that owns all device memory through its */

@@ -107,6 +107,31 @@ def test_autograd_function(cd, cuda):
     np.testing.assert_array_equal(N(o[0]), N(outa.detach()))
 
 
+@pytest.mark.parametrize("sp,rs", [(4, 1), (2, 2)])
+def test_keep_and_kept_are_bit_identical(cd, cuda, sp, rs):
+    """cross_regression_keep gives cross_regression's outputs and
+    cross_regression_grad_kept cross_regression_grad's, bit for bit (the
+    same kernels on the same inputs, the backward without its recompute);
+    the autograd path uses the pair."""
+    B, H, W, win = 2, 48, 56, 9
+    ins = [T(a) for a in inputs(cd, H, W, seed=91, B=B)]
+    ups = [None if u is None else T(u) for u in upstream(B, H, W, rs, seed=92)]
+    plain = cd.ops.cross_regression(*ins, win_size=win, sparsity=sp, recon_scale=rs)
+    kept_outs, ws = cd.ops.cross_regression_keep(*ins, win, sp, rs)
+    for a, b in zip(plain, kept_outs):
+        assert torch.equal(a, b)
+    g_re = cd.ops.cross_regression_grad(*ups, *ins, win, sp, rs)
+    g_kept = cd.ops.cross_regression_grad_kept(*ups, *ins, win, sp, rs, ws)
+    for a, b, nm in zip(g_re, g_kept, NAMES):
+        assert torch.equal(a, b), nm
+    x = [t.clone().requires_grad_(True) for t in ins]
+    outs = cd.ops.cross_regression(*x, win_size=win, sparsity=sp, recon_scale=rs)
+    loss = sum((o * u).sum() for o, u in zip(outs, ups) if u is not None)
+    loss.backward()
+    for t, b, nm in zip(x, g_re, NAMES):
+        assert torch.equal(t.grad, b), f"autograd {nm}"
+
+
 def test_argument_errors(cd, cuda):
     ins = [T(a) for a in inputs(cd, 16, 20, seed=1)]
     g = torch.zeros((1, 16, 20, 3), device="cuda:0")
