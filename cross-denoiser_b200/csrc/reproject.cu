@@ -187,6 +187,175 @@ __global__ void __launch_bounds__(256) reproject_kernel(
     }
 }
 
+// Two-kernel form of the 3-tensor, 3-channel list (the per-frame step's):
+// the same decisions and arithmetic as reproject_kernel<3, 3>, split so that
+// each kernel has two dependent load rounds and few live registers.
+// reproject_decide_kernel reads the pixel's own inputs and its taps and
+// leaves its decision in the success byte: 0 none, 0x10 | vmask bilinear
+// (bit s = tap s valid), 0x20 the 3x3 box.  reproject_gather_kernel
+// re-derives the taps and weights from the motion vector, re-tests the box
+// (its rare case), gathers the history tensors, writes every output once
+// and the final success byte.
+constexpr uint8_t kModeBilinear = 0x10, kModeBox = 0x20;
+
+CD_DEV void reproject_taps(float mx, float my, int cx, int cy, int W, int H, int &ipx, int &ipy, float &ppx,
+                           float &ppy)
+{
+    const float fW = (float)W, fH = (float)H, fx = (float)cx, fy = (float)cy;
+    ipx = __float2int_rz(__fadd_rn(__fmaf_rn(mx, fW, fx), 0.5f));
+    ipy = __float2int_rz(__fadd_rn(__fmaf_rn(my, fH, fy), 0.5f));
+    ppx = __fmaf_rn(mx, fW, floorf(fx));
+    ppy = __fmaf_rn(my, fH, floorf(fy));
+}
+
+// bilinear weights of the four taps and their sum over vmask
+CD_DEV float bilinear(float ppx, float ppy, unsigned vmask, float w[4])
+{
+    const float x = __fsub_rn(ppx, floorf(ppx)), y = __fsub_rn(ppy, floorf(ppy));
+    const float a0 = __fsub_rn(1.f, x), b0 = __fsub_rn(1.f, y);
+    const float fa[4] = {a0, x, a0, x}, fb[4] = {b0, b0, y, y};
+    float sumw = 0.f;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        w[s] = __fmul_rn(fa[s], fb[s]);
+        if (vmask & (1u << s)) sumw = __fadd_rn(sumw, w[s]);
+    }
+    return sumw;
+}
+
+__global__ void __launch_bounds__(256) reproject_decide_kernel(
+    const float *__restrict__ mvec, const float *__restrict__ linz, const float *__restrict__ plinz,
+    const float *__restrict__ nrm, const float *__restrict__ pnrm, const float *__restrict__ pnfw,
+    const float *__restrict__ opac, const float *__restrict__ popac, uint8_t *__restrict__ success, int H, int W)
+{
+    const int cx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (cx >= W || cy >= H) return;
+    const size_t base = (size_t)blockIdx.z * H * W;
+    const size_t c = base + (size_t)cy * W + cx;
+    uint8_t code = 0;
+    const float op = __ldg(opac + c), mx = __ldg(mvec + 3 * c), my = __ldg(mvec + 3 * c + 1);
+    const float fwN = __ldg(pnfw + 3 * c + 1);
+    const float Z = __ldg(linz + 3 * c), fwZ = __ldg(linz + 3 * c + 1);
+    const float3 n = ld3(nrm, c);
+    if (op != 0.f) {
+        int ipx, ipy;
+        float ppx, ppy;
+        reproject_taps(mx, my, cx, cy, W, H, ipx, ipy, ppx, ppy);
+        const int lx = __float2int_rz(ppx), ly = __float2int_rz(ppy);
+        const bool border_ok = !(ipx < 1 || ipy < 1 || ipx > W - 1 || ipy > H - 1);
+        unsigned vmask = 0u;
+        if (border_ok) {
+            float po[4], zp[4];
+            float3 np[4];
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const int qx = lx + (s & 1), qy = ly + (s >> 1);
+                po[s] = 0.f;
+                if (qx >= W || qx < 0 || qy >= H || qy < 0) continue;
+                const size_t q = base + (size_t)qy * W + qx;
+                po[s] = __ldg(popac + q);
+                zp[s] = __ldg(plinz + 3 * q);
+                np[s] = ld3(pnrm, q);
+            }
+#pragma unroll
+            for (int s = 0; s < 4; ++s)
+                if (po[s] != 0.f && depth_normal_ok(Z, zp[s], fwZ, n, np[s], fwN)) vmask |= 1u << s;
+        }
+        float w[4];
+        if (vmask && bilinear(ppx, ppy, vmask, w) >= 0.01f) {
+            code = (uint8_t)(kModeBilinear | vmask);
+        } else if (border_ok) {
+#pragma unroll
+            for (int k = 0; k < 9 && code == 0; ++k) {
+                const int qx = ipx + (k % 3) - 1, qy = ipy + (k / 3) - 1;
+                if (qx >= W || qx < 0 || qy >= H || qy < 0) continue;
+                // the reference reads prev_opacity here without the batch
+                // offset (ops/reproject.cu.cc:191)
+                if (__ldg(popac + (size_t)qy * W + qx) == 0.f) continue;
+                const size_t q = base + (size_t)qy * W + qx;
+                if (depth_normal_ok(Z, __ldg(plinz + 3 * q), fwZ, n, ld3(pnrm, q), fwN)) code = kModeBox;
+            }
+        }
+    }
+    success[c] = code;
+}
+
+__global__ void __launch_bounds__(256) reproject_gather_kernel(
+    const float *__restrict__ mvec, ReprojectList list, const float *__restrict__ linz,
+    const float *__restrict__ plinz, const float *__restrict__ nrm, const float *__restrict__ pnrm,
+    const float *__restrict__ pnfw, const float *__restrict__ popac, uint8_t *__restrict__ success, int H, int W)
+{
+    const int cx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (cx >= W || cy >= H) return;
+    const size_t base = (size_t)blockIdx.z * H * W;
+    const size_t c = base + (size_t)cy * W + cx;
+    const uint8_t code = success[c];
+    float acc[3][3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) acc[d][0] = acc[d][1] = acc[d][2] = 0.f;
+    float norm = 1.f;
+    if (code) {
+        const float mx = __ldg(mvec + 3 * c), my = __ldg(mvec + 3 * c + 1);
+        int ipx, ipy;
+        float ppx, ppy;
+        reproject_taps(mx, my, cx, cy, W, H, ipx, ipy, ppx, ppy);
+        if (code & kModeBilinear) {
+            const unsigned vmask = code & 0xFu;
+            float w[4];
+            norm = bilinear(ppx, ppy, vmask, w);
+            const int lx = __float2int_rz(ppx), ly = __float2int_rz(ppy);
+            float3 g[3][4];
+#pragma unroll
+            for (int s = 0; s < 4; ++s)
+                if (vmask & (1u << s)) {
+                    const size_t q = base + (size_t)(ly + (s >> 1)) * W + (lx + (s & 1));
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) g[d][s] = ld3(list.in[d], q);
+                }
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+#pragma unroll
+                for (int s = 0; s < 4; ++s)
+                    if (vmask & (1u << s)) {
+                        acc[d][0] = __fmaf_rn(w[s], g[d][s].x, acc[d][0]);
+                        acc[d][1] = __fmaf_rn(w[s], g[d][s].y, acc[d][1]);
+                        acc[d][2] = __fmaf_rn(w[s], g[d][s].z, acc[d][2]);
+                    }
+        } else {
+            // the 3x3 box, re-tested (the decision kernel keeps one bit)
+            const float fwN = __ldg(pnfw + 3 * c + 1);
+            const float Z = __ldg(linz + 3 * c), fwZ = __ldg(linz + 3 * c + 1);
+            const float3 n = ld3(nrm, c);
+            int cnt = 0;
+            for (int k = 0; k < 9; ++k) {
+                const int qx = ipx + (k % 3) - 1, qy = ipy + (k / 3) - 1;
+                if (qx >= W || qx < 0 || qy >= H || qy < 0) continue;
+                if (__ldg(popac + (size_t)qy * W + qx) == 0.f) continue;
+                const size_t q = base + (size_t)qy * W + qx;
+                if (!depth_normal_ok(Z, __ldg(plinz + 3 * q), fwZ, n, ld3(pnrm, q), fwN)) continue;
+                ++cnt;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const float3 v = ld3(list.in[d], q);
+                    acc[d][0] = __fadd_rn(acc[d][0], v.x);
+                    acc[d][1] = __fadd_rn(acc[d][1], v.y);
+                    acc[d][2] = __fadd_rn(acc[d][2], v.z);
+                }
+            }
+            norm = (float)cnt;
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        float *out = list.out[d] + c * 3;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) out[k] = code ? __fdiv_rn(acc[d][k], norm) : 0.f;
+    }
+    success[c] = code != 0;
+}
+
 }  // namespace
 
 cudaError_t launch_reproject(const float *mvec, const ReprojectList &list, const float *linz,
@@ -198,9 +367,12 @@ cudaError_t launch_reproject(const float *mvec, const ReprojectList &list, const
     dim3 grid((W + 31) / 32, (H + 7) / 8, B);
     bool fast = list.n == 3;
     for (int d = 0; d < list.n; ++d) fast = fast && list.ch[d] == 3;
-    if (fast)
-        reproject_kernel<3, 3><<<grid, block, 0, st>>>(mvec, list, linz, plinz, nrm, pnrm, pnfw,
-                                                       opac, popac, success, H, W);
+    if (fast) {
+        reproject_decide_kernel<<<grid, block, 0, st>>>(mvec, linz, plinz, nrm, pnrm, pnfw, opac, popac, success,
+                                                        H, W);
+        reproject_gather_kernel<<<grid, block, 0, st>>>(mvec, list, linz, plinz, nrm, pnrm, pnfw, popac, success, H,
+                                                        W);
+    }
     else
         reproject_kernel<0, 0><<<grid, block, 0, st>>>(mvec, list, linz, plinz, nrm, pnrm, pnfw,
                                                        opac, popac, success, H, W);
