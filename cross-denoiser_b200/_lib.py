@@ -68,7 +68,7 @@ SIGNATURES = {
 KERNELS_PER_CALL = {
     "cd_cross_regression": 3, "cd_cross_regression_fp64_fallback": 3, "cd_cross_regression_grad": 8,
     "cd_cross_regression_keep": 3, "cd_cross_regression_grad_kept": 6, "cd_spatial_filter": 1, "cd_spatial_filter_grad": 1, "cd_spatial_filter_stored": 1, "cd_spatial_filter_grad_stored": 1,
-    "cd_reproject": 1,
+    "cd_reproject": 1,   # 2 for the three 3-channel tensors of the step (ops.reproject passes the count)
     "cd_erode3x3": 1, "cd_temporal_screening": 1, "cd_erode_temporal_screening": 1,
     "cd_prepare_input": 1, "cd_aggregation_loss": 2, "cd_filter_aggregate": 2,
     "cd_unet_forward": 22, "cd_unet_backward": 42, "cd_adam_update": 2, "cd_unet_conv3x3": 2,
@@ -104,10 +104,11 @@ def lib() -> ctypes.CDLL:
     return _lib
 
 
-def check(status: int, op: str) -> None:
-    """Raise the Python analogue of a non-zero cd_status; count launches."""
+def check(status: int, op: str, kernels: int | None = None) -> None:
+    """Raise the Python analogue of a non-zero cd_status; count launches
+    (`kernels` when the entry point's count depends on its arguments)."""
     if status == CD_OK:
-        LAUNCHES["count"] += KERNELS_PER_CALL.get("cd_" + op, 0)
+        LAUNCHES["count"] += KERNELS_PER_CALL.get("cd_" + op, 0) if kernels is None else kernels
         return
     msg = lib().cd_get_last_error().decode(errors="replace")
     if status == CD_EINVAL:

@@ -382,7 +382,8 @@ def reproject(mvec, input_list: Sequence[torch.Tensor], linear_z, prev_linear_z,
     _lib.check(_lib.lib().cd_reproject(_ptr(mvec), n, in_arr, ch_arr, out_arr, _ptr(linear_z),
                                        _ptr(prev_linear_z), _ptr(normal), _ptr(prev_normal),
                                        _ptr(pn_fwidth), _ptr(opacity), _ptr(prev_opacity),
-                                       _ptr(success), B, H, W, _stream()), "reproject")
+                                       _ptr(success), B, H, W, _stream()), "reproject",
+               kernels=2 if n == 3 and all(int(t.shape[3]) == 3 for t in inputs) else 1)
     return success, outputs
 
 
