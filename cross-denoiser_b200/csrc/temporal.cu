@@ -351,13 +351,17 @@ __global__ void __launch_bounds__(kTX * kTY, 2) temporal_tma_kernel(
     int it = 0;
     for (int t = blockIdx.x; t < ntiles; t += G0, ++it) {
         const int s = it & 1;
+        // this barrier also marks every thread done with the previous tile:
+        // its stage (and the row planes) may be reused from here on
         const bool landed = __syncthreads_and(tc::mbar_wait(&bar[s], (uint32_t)(it >> 1) & 1u, kWaitPolls)) != 0;
+        if (landed && it >= 1 && tid == 0 && t + G0 < ntiles) issue(t + G0, s ^ 1);
         if (!landed) {
-            // give the other stage's copy, if one was issued, a bounded wait
-            // before leaving, and report the time-out
+            // the other stage has a copy in flight only on the first tile
+            // (the prologue's second copy; later ones are issued after a
+            // landed wait): give it a bounded wait, and report the time-out
             if (tid == 0) {
                 atomicOr(&g_image_kernel_error, 1);
-                if (t + G0 < ntiles) tc::mbar_wait(&bar[s ^ 1], (uint32_t)((it + 1) >> 1) & 1u, kWaitPolls);
+                if (it == 0 && t + G0 < ntiles) tc::mbar_wait(&bar[1], 0u, kWaitPolls);
             }
             return;
         }
@@ -463,8 +467,6 @@ __global__ void __launch_bounds__(kTX * kTY, 2) temporal_tma_kernel(
                 succ[p] = ok[2] ? 1.f : 0.f;
             }
         }
-        __syncthreads();   // every read of stage s and of the row planes is done
-        if (tid == 0 && t + 2 * G0 < ntiles) issue(t + 2 * G0, s);
     }
 }
 
