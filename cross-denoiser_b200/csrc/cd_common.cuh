@@ -49,7 +49,7 @@ cudaError_t launch_recon(const float *imga, const float *imgb, const float *albe
                          const float *normal, const float *vara, const float *varb,
                          const float *sda, const float *sdb, const float *beta, float *outa,
                          float *outb, int B, int H, int W, int win, int sparsity, int recon_scale,
-                         cudaStream_t st);
+                         cudaStream_t st, float *state = nullptr);
 size_t regression_smem_bytes(int win, int sparsity);
 // CrossRegression backward (regression_grad.cu); ws holds
 // regression_grad_workspace_floats() floats.

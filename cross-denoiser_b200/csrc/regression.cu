@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
 #include "f32x2.cuh"
+#include "window_rows.cuh"
 
 namespace cd {
 namespace {
@@ -381,32 +382,12 @@ CD_DEV void solve_channel(const Normal &n, int k, float *beta, float *Lo, float 
 // and warp 1 buffer B, one thread per (centre, buffer), so every centre sums
 // its window taps in the reference's order (rows, then columns) with the
 // reference's per-tap arithmetic.  The window rows stream through two
-// shared-memory row slots (cp.async, double buffered): row r + 1 is copied
-// while row r is consumed.  A row slot stores, per pixel of the row segment
-// the 32 windows cover, four float4 groups
-//   g0 = (imga.xyz, varA)  g1 = (imgb.xyz, varB)
-//   g2 = (albedo.xyz, sdA) g3 = (normal.xyz, sdB)
-// and positions are de-interleaved by the sparsity (position p at
-// (p % s) * q + p / s), so the 32 lanes, whose centres are s pixels apart,
-// read 32 consecutive float4s: four conflict-free LDS.128 per tap.
+// shared-memory row slots (cp.async, double buffered; layout in
+// window_rows.cuh): row r + 1 is copied while row r is consumed, and a tap
+// is four conflict-free LDS.128.
 // ---------------------------------------------------------------------------
-constexpr int kCX = 32;       // centres per CTA
+constexpr int kCX = kRowCentres;   // centres per CTA
 constexpr int kThreads = 64;
-
-struct RowGeom {
-    int rw;      // row segment width in pixels
-    int q;       // de-interleave stride
-    int npos;    // positions per group (q * sparsity)
-};
-
-__host__ __device__ inline RowGeom row_geom(int hw, int sp)
-{
-    RowGeom g;
-    g.rw = (kCX - 1) * sp + 2 * hw + 1;
-    g.q = (g.rw + sp - 1) / sp;
-    g.npos = g.q * sp;
-    return g;
-}
 
 // two row slots of 4 float4 groups, then the per-position tables
 __host__ __device__ inline size_t regression_smem(int hw, int sp)
@@ -414,16 +395,6 @@ __host__ __device__ inline size_t regression_smem(int hw, int sp)
     const RowGeom g = row_geom(hw, sp);
     return (size_t)2 * 4 * g.npos * sizeof(float4) + (size_t)2 * g.rw * sizeof(int);
 }
-
-CD_DEV void cp_async4(float *dst, const float *src)
-{
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
-}
-CD_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N> CD_DEV void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-CD_DEV int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
 
 // exp(x) = 2^(x log2 e) on the ex2.approx.ftz instruction (subnormal results
 // flushed to zero).
@@ -468,29 +439,13 @@ __global__ void __launch_bounds__(kThreads, 7) regression_kernel(
     const int lane = threadIdx.x & 31;
     const int R = 2 * hw + 1;
 
-    // Column of every row position (reflect-101; positions past the reflect
-    // range feed no valid centre and are clamped only to stay in bounds) and
-    // its de-interleaved slot index.
-    for (int p = threadIdx.x; p < g.rw; p += kThreads) {
-        pos_gx[p] = clampi(mirror(x0 + p, W), 0, W - 1);
-        pos_dst[p] = (p % sp) * g.q + p / sp;
-    }
+    row_positions(pos_gx, pos_dst, g, x0, W, sp, threadIdx.x, kThreads);
     __syncthreads();
 
     auto stage = [&](int r, int s) {
-        float *base = reinterpret_cast<float *>(sm4 + s * slot);
-        const int gy = clampi(mirror(cy - hw + r, H), 0, H - 1);
-        const size_t row = (size_t)gy * W;
-        for (int p = threadIdx.x; p < g.rw; p += kThreads) {
-            const size_t q = row + pos_gx[p];
-            float *d = base + 4 * pos_dst[p];
-            const float *a = imga + 3 * q, *c = imgb + 3 * q, *l = albedo + 3 * q, *n = normal + 3 * q;
-            float *d0 = d, *d1 = d + 4 * g.npos, *d2 = d + 8 * g.npos, *d3 = d + 12 * g.npos;
-            cp_async4(d0, a); cp_async4(d0 + 1, a + 1); cp_async4(d0 + 2, a + 2); cp_async4(d0 + 3, vara + q);
-            cp_async4(d1, c); cp_async4(d1 + 1, c + 1); cp_async4(d1 + 2, c + 2); cp_async4(d1 + 3, varb + q);
-            cp_async4(d2, l); cp_async4(d2 + 1, l + 1); cp_async4(d2 + 2, l + 2); cp_async4(d2 + 3, sda + q);
-            cp_async4(d3, n); cp_async4(d3 + 1, n + 1); cp_async4(d3 + 2, n + 2); cp_async4(d3 + 3, sdb + q);
-        }
+        stage_window_row(reinterpret_cast<float *>(sm4 + s * slot), g, pos_gx, pos_dst,
+                         clampi(mirror(cy - hw + r, H), 0, H - 1), W, imga, imgb, albedo, normal, vara, varb, sda,
+                         sdb, threadIdx.x, kThreads);
     };
 
     stage(0, 0);
@@ -583,7 +538,7 @@ __global__ void __launch_bounds__(kRX * kRY) recon_kernel(
     const float *__restrict__ vara, const float *__restrict__ varb,
     const float *__restrict__ sda, const float *__restrict__ sdb,
     const float *__restrict__ beta, float *__restrict__ outa, float *__restrict__ outb,
-    int H, int W, int hw, int sp, int rs)
+    float *__restrict__ state, int H, int W, int hw, int sp, int rs)
 {
     using namespace x2;
     extern __shared__ float4 rec[];
@@ -694,8 +649,17 @@ __global__ void __launch_bounds__(kRX * kRY) recon_kernel(
     }
     const float dA = fmaxf(lo(sw), 1e-7f), dB = fmaxf(hi(sw), 1e-7f);
     const size_t o = (size_t)b * Hr * Wr + (size_t)cy * Wr + cx;
-    st3(outa, o, make_float3(fmaxf(0.f, lo(o0) / dA), fmaxf(0.f, lo(o1) / dA), fmaxf(0.f, lo(o2) / dA)));
-    st3(outb, o, make_float3(fmaxf(0.f, hi(o0) / dB), fmaxf(0.f, hi(o1) / dB), fmaxf(0.f, hi(o2) / dB)));
+    const float3 qa = make_float3(fmaxf(0.f, lo(o0) / dA), fmaxf(0.f, lo(o1) / dA), fmaxf(0.f, lo(o2) / dA));
+    const float3 qb = make_float3(fmaxf(0.f, hi(o0) / dB), fmaxf(0.f, hi(o1) / dB), fmaxf(0.f, hi(o2) / dB));
+    if (outa) {
+        st3(outa, o, qa);
+        st3(outb, o, qb);
+    }
+    if (state) {   // for the backward: the outputs and the weight sums D, [buffer][pixel]
+        float4 *S = reinterpret_cast<float4 *>(state);
+        S[o] = make_float4(qa.x, qa.y, qa.z, lo(sw));
+        S[(size_t)gridDim.z * Hr * Wr + o] = make_float4(qb.x, qb.y, qb.z, hi(sw));
+    }
 }
 
 }  // namespace
@@ -739,7 +703,7 @@ cudaError_t launch_regression(const float *imga, const float *imgb, const float 
 cudaError_t launch_recon(const float *imga, const float *imgb, const float *albedo,
                          const float *normal, const float *vara, const float *varb, const float *sda,
                          const float *sdb, const float *beta, float *outa, float *outb, int B, int H,
-                         int W, int win, int sp, int rs, cudaStream_t st)
+                         int W, int win, int sp, int rs, cudaStream_t st, float *state)
 {
     const int hw = win / 2;
     const size_t smem = recon_smem(hw, sp, rs);
@@ -750,7 +714,7 @@ cudaError_t launch_recon(const float *imga, const float *imgb, const float *albe
     dim3 block(kRX, kRY);
     dim3 grid((Wr + kRX - 1) / kRX, (Hr + kRY - 1) / kRY, B);
     recon_kernel<<<grid, block, smem, st>>>(imga, imgb, albedo, normal, vara, varb, sda, sdb, beta, outa,
-                                            outb, H, W, hw, sp, rs);
+                                            outb, state, H, W, hw, sp, rs);
     return cudaGetLastError();
 }
 

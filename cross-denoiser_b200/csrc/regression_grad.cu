@@ -21,16 +21,21 @@
 //
 // Passes (each pixel or centre is written by exactly one thread per pass;
 // passes are stream ordered, so no atomics):
-//   1. variance + std, forward regression keeping each centre's Cholesky factor
-//   2. recon backward, pixel side (dL/dN, dL/dD stored per output pixel)
-//   3. recon backward, centre side (dL/dbeta)
-//   4. solve backward (u) and the regression's centre-side terms
+//   1. variance + std, forward regression keeping each centre's Cholesky factor,
+//      reconstruction keeping each output pixel's outputs and weight sum D
+//   2. recon backward, pixel side (dL/dN, dL/dD from the kept outputs and D,
+//      stored per output pixel)
+//   3. recon backward, centre side (dL/dbeta), one warp per centre
+//   4. solve backward (u) and the regression's centre-side terms, one warp
+//      per centre
 //   5. the regression's tap-side terms, gathered per pixel over every
 //      (centre, window position) whose reflect-101 image is that pixel
 //   6. sqrt / variance chain and assembly of dL/dimga, dL/dimgb, dL/dalbedo,
 //      dL/dnormal.
 #include <cuda_runtime.h>
 #include "cd_common.cuh"
+#include "f32x2.cuh"
+#include "window_rows.cuh"
 
 namespace cd {
 namespace {
@@ -45,6 +50,7 @@ struct GBuf {
 
 struct GArgs {
     GBuf bf[2];
+    const float4 *state;        // forward recon: (out[3], D) per [buffer][output pixel]
     const float *alb, *nrm;
     float *galb, *gn;
     float *out_a, *out_b, *out_alb, *out_n;   // final gradients
@@ -117,6 +123,29 @@ CD_DEV void recon_pair(float3 fp, float3 fc, float sp_, float sc, float vp, floa
     g.gdn = make_float3(gdn[0], gdn[1], gdn[2]);
 }
 
+// dL/dN and dL/dD of one output pixel, from the forward's outputs and weight
+// sum (out_k = max(0, N_k / max(D, 1e-7))): dL/dN_k = dL/dout_k / max(D, 1e-7)
+// where out_k > 0, else 0; dL/dD = -sum_k dL/dN_k out_k, 0 where D <= 1e-7.
+CD_DEV void recon_upstream(float4 S, float3 G, float gN[3], float &gD)
+{
+    const float Dt = fmaxf(S.w, 1e-7f);
+    const float ov[3] = {S.x, S.y, S.z}, Gv[3] = {G.x, G.y, G.z};
+    gD = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        gN[k] = ov[k] > 0.f ? Gv[k] / Dt : 0.f;
+        gD -= gN[k] * ov[k];
+    }
+    if (!(S.w > 1e-7f)) gD = 0.f;
+}
+
+CD_DEV float warp_sum(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 CD_DEV void centre_range(int pos, int n, int hw, int sp, int &lo, int &hi)
 {
     lo = max(0, idivup(pos - hw, sp));
@@ -143,33 +172,9 @@ __global__ void __launch_bounds__(256) recon_grad_pixel_kernel(GArgs A)
         const GBuf &B_ = A.bf[X];
         const float3 fp = f3(B_.f, p);
         const float vp = __ldg(B_.v + p), sp_ = __ldg(B_.s + p);
-        float N[3] = {0.f, 0.f, 0.f}, D = 0.f;
-        const float zero[3] = {0.f, 0.f, 0.f};
         PairGrad g;
-        for (int iy = sy; iy <= ey; ++iy)
-            for (int ix = sx; ix <= ex; ++ix) {
-                const size_t c = b * P + (size_t)(iy * A.sp) * A.W + ix * A.sp;
-                const float3 fc = f3(B_.f, c), ac = f3(A.alb, c), nc = f3(A.nrm, c);
-                const float3 da = make_float3(ap.x - ac.x, ap.y - ac.y, ap.z - ac.z);
-                const float3 dn = make_float3(np_.x - nc.x, np_.y - nc.y, np_.z - nc.z);
-                recon_pair<false>(fp, fc, sp_, __ldg(B_.s + c), vp, __ldg(B_.v + c), da, dn,
-                                  B_.beta + (b * C + (size_t)iy * A.Ws + ix) * kBeta, zero, 0.f, g);
-                N[0] += g.w * g.pred[0];
-                N[1] += g.w * g.pred[1];
-                N[2] += g.w * g.pred[2];
-                D += g.w;
-            }
-        const float Dt = fmaxf(D, 1e-7f);
-        const float3 G = f3(B_.gout, o);
-        const float Gv[3] = {G.x, G.y, G.z};
-        float gN[3], gD = 0.f;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const float ok = N[k] / Dt;
-            gN[k] = ok > 0.f ? Gv[k] / Dt : 0.f;
-            gD -= gN[k] * ok;
-        }
-        if (!(D > 1e-7f)) gD = 0.f;
+        float gN[3], gD;
+        recon_upstream(A.state[X * (size_t)gridDim.z * R + o], f3(B_.gout, o), gN, gD);
         B_.gN[3 * o] = gN[0];
         B_.gN[3 * o + 1] = gN[1];
         B_.gN[3 * o + 2] = gN[2];
@@ -204,26 +209,55 @@ __global__ void __launch_bounds__(256) recon_grad_pixel_kernel(GArgs A)
     add3(A.gn, p, gnn);
 }
 
-// Pass 2 with the tile's centres staged in shared memory: a CTA of 32 x 8
-// output pixels first copies, for every centre any of its pixels reaches
-// (the forward recon kernel's superset), both buffers' features, standard
-// deviation, variance and coefficients and the shared albedo and normal into
-// one record of kRecG floats; the per-pixel loops then read records instead
-// of global memory.  Same pairs, same order, same arithmetic as
-// recon_grad_pixel_kernel, so the same results.
-constexpr int kRecG = 52;   // fA[3] sA vA betaA[18] | fB[3] sB vB betaB[18] | alb[3] nrm[3]
+// Pass 2 with the tile's centres staged in shared memory and both buffers
+// of a pair evaluated as packed FP32x2 lanes (low A, high B).  A CTA of
+// 32 x 8 output pixels first copies, for every centre any of its pixels
+// reaches (the forward recon kernel's superset), one record of kRecG2
+// float4s (pairs (A, B) unless noted):
+//   0  f.x f.y   1  f.z s   2  v | alb.x alb.y (scalars)   3  alb.z nrm.xyz (scalars)
+//   4 + 3k + m   coefficients of channel k, rows 2m and 2m + 1
+// A warp covers 4 x 8 pixels of the tile, so its lanes step through the
+// same or neighbouring records (shared-memory broadcast).
+constexpr int kRecG2 = 13;
 
 __host__ __device__ inline int floordiv_g(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
 __host__ __device__ inline size_t recon_grad_smem(int hw, int sp, int rs)
 {
     const int ncx = (31 * rs + 2 * hw) / sp + 2, ncy = (7 * rs + 2 * hw) / sp + 2;
-    return (size_t)ncx * ncy * kRecG * sizeof(float);
+    return (size_t)ncx * ncy * kRecG2 * sizeof(float4);
 }
 
-__global__ void __launch_bounds__(256) recon_grad_pixel_smem_kernel(GArgs A)
+CD_DEV x2::f2 neg2(x2::f2 v) { return v ^ 0x8000000080000000ull; }
+CD_DEV x2::f2 dup2(float v) { return x2::pack(v, v); }
+CD_DEV x2::f2 rcp2(x2::f2 v) { return x2::pack(__fdividef(1.f, x2::lo(v)), __fdividef(1.f, x2::hi(v))); }
+CD_DEV x2::f2 expneg2(x2::f2 v) { return x2::pack(__expf(-x2::lo(v)), __expf(-x2::hi(v))); }
+
+// stage the coefficients (or u) of one channel k of centre ci as three
+// float4s of (A, B) pairs, rows 2m and 2m + 1
+CD_DEV void stage_rows(float4 *d, const float *pa, const float *pb, size_t ci, int k)
 {
-    extern __shared__ float recs[];
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+        d[m] = make_float4(__ldg(pa + ci * kBeta + 6 * m + k), __ldg(pb + ci * kBeta + 6 * m + k),
+                           __ldg(pa + ci * kBeta + 6 * m + 3 + k), __ldg(pb + ci * kBeta + 6 * m + 3 + k));
+}
+
+// the per-centre head of a record: features, sd, variance of both buffers,
+// albedo and normal
+CD_DEV void stage_head(float4 *r, const GArgs &A, size_t c)
+{
+    const float3 fa = f3(A.bf[0].f, c), fb = f3(A.bf[1].f, c), al = f3(A.alb, c), nr = f3(A.nrm, c);
+    r[0] = make_float4(fa.x, fb.x, fa.y, fb.y);
+    r[1] = make_float4(fa.z, fb.z, __ldg(A.bf[0].s + c), __ldg(A.bf[1].s + c));
+    r[2] = make_float4(__ldg(A.bf[0].v + c), __ldg(A.bf[1].v + c), al.x, al.y);
+    r[3] = make_float4(al.z, nr.x, nr.y, nr.z);
+}
+
+__global__ void __launch_bounds__(256) recon_grad_pixel_x2_kernel(GArgs A)
+{
+    using namespace x2;
+    extern __shared__ float4 rec4[];
     const int b = blockIdx.z;
     const size_t P = (size_t)A.H * A.W, R = (size_t)A.Hr * A.Wr, C = (size_t)A.Hs * A.Ws;
     const int ox0 = blockIdx.x * 32, oy0 = blockIdx.y * 8;
@@ -231,43 +265,22 @@ __global__ void __launch_bounds__(256) recon_grad_pixel_smem_kernel(GArgs A)
     const int cx_lo = max(0, floordiv_g(ox0 * A.rs - A.hw, A.sp)), cx_hi = min(A.Ws - 1, (ox1 * A.rs + A.hw) / A.sp);
     const int cy_lo = max(0, floordiv_g(oy0 * A.rs - A.hw, A.sp)), cy_hi = min(A.Hs - 1, (oy1 * A.rs + A.hw) / A.sp);
     const int ncx = cx_hi - cx_lo + 1, ncy = cy_hi - cy_lo + 1;
-    const int tid = threadIdx.y * 32 + threadIdx.x;
-    // one thread per (centre, field group)
+    const int tid = threadIdx.x;
     for (int e = tid; e < ncx * ncy * 4; e += 256) {
         const int n = e >> 2, part = e & 3;
         const int iy = cy_lo + n / ncx, ix = cx_lo + n % ncx;
         const size_t c = b * P + (size_t)(iy * A.sp) * A.W + ix * A.sp;
         const size_t ci = b * C + (size_t)iy * A.Ws + ix;
-        float *r = recs + (size_t)n * kRecG;
-        if (part < 2) {
-            const GBuf &B_ = A.bf[part];
-            float *q = r + 23 * part;
-            const float3 f = f3(B_.f, c);
-            q[0] = f.x;
-            q[1] = f.y;
-            q[2] = f.z;
-            q[3] = __ldg(B_.s + c);
-            q[4] = __ldg(B_.v + c);
-#pragma unroll
-            for (int k = 0; k < 9; ++k) q[5 + k] = __ldg(B_.beta + ci * kBeta + k);
-        } else if (part == 2) {
-#pragma unroll
-            for (int X = 0; X < 2; ++X)
-#pragma unroll
-                for (int k = 9; k < kBeta; ++k) r[23 * X + 5 + k] = __ldg(A.bf[X].beta + ci * kBeta + k);
-        } else {
-            const float3 al = f3(A.alb, c), nr = f3(A.nrm, c);
-            r[46] = al.x;
-            r[47] = al.y;
-            r[48] = al.z;
-            r[49] = nr.x;
-            r[50] = nr.y;
-            r[51] = nr.z;
-        }
+        float4 *r = rec4 + (size_t)n * kRecG2;
+        if (part == 0)
+            stage_head(r, A, c);
+        else
+            stage_rows(r + 4 + 3 * (part - 1), A.bf[0].beta, A.bf[1].beta, ci, part - 1);
     }
     __syncthreads();
 
-    const int ox = ox0 + threadIdx.x, oy = oy0 + threadIdx.y;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int ox = ox0 + 4 * warp + (lane & 3), oy = oy0 + (lane >> 2);
     if (ox >= A.Wr || oy >= A.Hr) return;
     const int px = ox * A.rs, py = oy * A.rs;
     const size_t p = b * P + (size_t)py * A.W + px, o = b * R + (size_t)oy * A.Wr + ox;
@@ -275,69 +288,84 @@ __global__ void __launch_bounds__(256) recon_grad_pixel_smem_kernel(GArgs A)
     centre_range(px, A.W, A.hw, A.sp, sx, ex);
     centre_range(py, A.H, A.hw, A.sp, sy, ey);
     const float3 ap = f3(A.alb, p), np_ = f3(A.nrm, p);
-    float3 galb = make_float3(0.f, 0.f, 0.f), gnn = galb;
+    const float3 fpa = f3(A.bf[0].f, p), fpb = f3(A.bf[1].f, p);
+    const f2 fp0 = pack(fpa.x, fpb.x), fp1 = pack(fpa.y, fpb.y), fp2 = pack(fpa.z, fpb.z);
+    const f2 spp = pack(__ldg(A.bf[0].s + p), __ldg(A.bf[1].s + p));
+    const f2 vpp = pack(__ldg(A.bf[0].v + p), __ldg(A.bf[1].v + p));
+    // dL/dN and dL/dD of the pixel, both buffers
+    f2 gN0, gN1, gN2, gD;
+    {
+        float na[3], nb[3], da, db;
+        const size_t RB = (size_t)gridDim.z * R;
+        recon_upstream(A.state[o], f3(A.bf[0].gout, o), na, da);
+        recon_upstream(A.state[RB + o], f3(A.bf[1].gout, o), nb, db);
+        for (int X = 0; X < 2; ++X) {
+            const float *g = X ? nb : na;
+            A.bf[X].gN[3 * o] = g[0];
+            A.bf[X].gN[3 * o + 1] = g[1];
+            A.bf[X].gN[3 * o + 2] = g[2];
+            A.bf[X].gD[o] = X ? db : da;
+        }
+        gN0 = pack(na[0], nb[0]);
+        gN1 = pack(na[1], nb[1]);
+        gN2 = pack(na[2], nb[2]);
+        gD = pack(da, db);
+    }
+    const f2 k1e2 = pack(1e-2f, 1e-2f), k1e4 = pack(1e-4f, 1e-4f), k1e7 = pack(1e-7f, 1e-7f);
+    const f2 two = pack(2.f, 2.f);
+    f2 gf0 = 0ull, gf1 = 0ull, gf2 = 0ull, gs = 0ull, gv = 0ull;
+    f2 ga0 = 0ull, ga1 = 0ull, ga2 = 0ull, gn0 = 0ull, gn1 = 0ull, gn2 = 0ull;
+    for (int iy = sy; iy <= ey; ++iy)
+        for (int ix = sx; ix <= ex; ++ix) {
+            const float4 *R4 = rec4 + (size_t)((iy - cy_lo) * ncx + (ix - cx_lo)) * kRecG2;
+            const ulonglong2 *RR = reinterpret_cast<const ulonglong2 *>(R4);
+            const ulonglong2 h0 = RR[0], h1 = RR[1];
+            const float4 q2 = R4[2], q3 = R4[3];
+            const f2 df0 = sub2(fp0, h0.x), df1 = sub2(fp1, h0.y), df2 = sub2(fp2, h1.x);
+            const f2 rden = rcp2(add2(add2(spp, h1.y), k1e2));
+            const f2 rV = rcp2(add2(add2(vpp, pack(q2.x, q2.y)), k1e4));
+            const f2 dist = mul2(sqnorm2(df0, df1, df2), rV);
+            const f2 e = expneg2(dist);
+            const f2 w = add2(e, k1e7);
+            const f2 da[3] = {dup2(ap.x - q2.z), dup2(ap.y - q2.w), dup2(ap.z - q3.x)};
+            const f2 dn0 = dup2(np_.x - q3.y), dn1 = dup2(np_.y - q3.z), dn2 = dup2(np_.z - q3.w);
+            const f2 df[3] = {df0, df1, df2}, gN[3] = {gN0, gN1, gN2};
+            f2 gw = gD, gsum = 0ull;
+            f2 gd1[3], d1[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const ulonglong2 b01 = RR[4 + 3 * k], b23 = RR[5 + 3 * k], b45 = RR[6 + 3 * k];
+                d1[k] = mul2(df[k], rden);
+                const f2 pr = fma2(b45.y, dn2, fma2(b45.x, dn1, fma2(b23.y, dn0,
+                                   fma2(b23.x, da[k], fma2(b01.y, d1[k], b01.x)))));
+                gw = fma2(gN[k], pr, gw);
+                const f2 gp = mul2(gN[k], w);
+                gd1[k] = mul2(gp, b01.y);
+                gsum = fma2(gd1[k], d1[k], gsum);
+                if (k == 0) ga0 = fma2(gp, b23.x, ga0);
+                if (k == 1) ga1 = fma2(gp, b23.x, ga1);
+                if (k == 2) ga2 = fma2(gp, b23.x, ga2);
+                gn0 = fma2(gp, b23.y, gn0);
+                gn1 = fma2(gp, b45.x, gn1);
+                gn2 = fma2(gp, b45.y, gn2);
+            }
+            const f2 gdist = neg2(mul2(gw, e));
+            const f2 t = mul2(mul2(two, gdist), rV);
+            gf0 = add2(gf0, fma2(t, df0, mul2(gd1[0], rden)));
+            gf1 = add2(gf1, fma2(t, df1, mul2(gd1[1], rden)));
+            gf2 = add2(gf2, fma2(t, df2, mul2(gd1[2], rden)));
+            gs = sub2(gs, mul2(gsum, rden));
+            gv = sub2(gv, mul2(mul2(gdist, dist), rV));
+        }
     for (int X = 0; X < 2; ++X) {
         const GBuf &B_ = A.bf[X];
-        const float3 fp = f3(B_.f, p);
-        const float vp = __ldg(B_.v + p), sp_ = __ldg(B_.s + p);
-        float N[3] = {0.f, 0.f, 0.f}, D = 0.f;
-        const float zero[3] = {0.f, 0.f, 0.f};
-        PairGrad g;
-        for (int iy = sy; iy <= ey; ++iy)
-            for (int ix = sx; ix <= ex; ++ix) {
-                const float *r = recs + (size_t)((iy - cy_lo) * ncx + (ix - cx_lo)) * kRecG;
-                const float *q = r + 23 * X;
-                const float3 da = make_float3(ap.x - r[46], ap.y - r[47], ap.z - r[48]);
-                const float3 dn = make_float3(np_.x - r[49], np_.y - r[50], np_.z - r[51]);
-                recon_pair<false>(fp, make_float3(q[0], q[1], q[2]), sp_, q[3], vp, q[4], da, dn, q + 5, zero, 0.f,
-                                  g);
-                N[0] += g.w * g.pred[0];
-                N[1] += g.w * g.pred[1];
-                N[2] += g.w * g.pred[2];
-                D += g.w;
-            }
-        const float Dt = fmaxf(D, 1e-7f);
-        const float3 G = f3(B_.gout, o);
-        const float Gv[3] = {G.x, G.y, G.z};
-        float gN[3], gD = 0.f;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const float ok = N[k] / Dt;
-            gN[k] = ok > 0.f ? Gv[k] / Dt : 0.f;
-            gD -= gN[k] * ok;
-        }
-        if (!(D > 1e-7f)) gD = 0.f;
-        B_.gN[3 * o] = gN[0];
-        B_.gN[3 * o + 1] = gN[1];
-        B_.gN[3 * o + 2] = gN[2];
-        B_.gD[o] = gD;
-        float3 gf = make_float3(0.f, 0.f, 0.f);
-        float gs = 0.f, gv = 0.f;
-        for (int iy = sy; iy <= ey; ++iy)
-            for (int ix = sx; ix <= ex; ++ix) {
-                const float *r = recs + (size_t)((iy - cy_lo) * ncx + (ix - cx_lo)) * kRecG;
-                const float *q = r + 23 * X;
-                const float3 da = make_float3(ap.x - r[46], ap.y - r[47], ap.z - r[48]);
-                const float3 dn = make_float3(np_.x - r[49], np_.y - r[50], np_.z - r[51]);
-                recon_pair<false>(fp, make_float3(q[0], q[1], q[2]), sp_, q[3], vp, q[4], da, dn, q + 5, gN, gD, g);
-                gf.x += g.gdf.x;
-                gf.y += g.gdf.y;
-                gf.z += g.gdf.z;
-                gs += g.gden;
-                gv += g.gV;
-                galb.x += g.gda.x;
-                galb.y += g.gda.y;
-                galb.z += g.gda.z;
-                gnn.x += g.gdn.x;
-                gnn.y += g.gdn.y;
-                gnn.z += g.gdn.z;
-            }
-        add3(B_.gf, p, gf);
-        B_.gs[p] += gs;
-        B_.gv[p] += gv;
+        const float x0 = X ? hi(gf0) : lo(gf0), x1 = X ? hi(gf1) : lo(gf1), x2_ = X ? hi(gf2) : lo(gf2);
+        add3(B_.gf, p, make_float3(x0, x1, x2_));
+        B_.gs[p] += X ? hi(gs) : lo(gs);
+        B_.gv[p] += X ? hi(gv) : lo(gv);
     }
-    add3(A.galb, p, galb);
-    add3(A.gn, p, gnn);
+    add3(A.galb, p, make_float3(lo(ga0) + hi(ga0), lo(ga1) + hi(ga1), lo(ga2) + hi(ga2)));
+    add3(A.gn, p, make_float3(lo(gn0) + hi(gn0), lo(gn1) + hi(gn1), lo(gn2) + hi(gn2)));
 }
 
 // ---------------------------------------------------------------------------
@@ -437,6 +465,129 @@ __global__ void __launch_bounds__(256) recon_grad_centre_kernel(GArgs A)
     add3(A.gn, c, gnn);
 }
 
+// Pass 3, one warp per centre: the output pixels whose centre range holds
+// the centre are listed per axis (tested by the forward's range rule on the
+// candidate box, one candidate per lane), the warp's lanes take the
+// (pixel row, pixel column) pairs of the two lists in turn, and the lanes'
+// partial sums are reduced by a fixed butterfly (deterministic).  Needs at
+// most kCand candidates per axis; recon_grad_centre_kernel serves the rest.
+constexpr int kCand = 64, kCW = 8;   // candidates per axis, warps (centres) per CTA
+
+__host__ __device__ inline bool recon_grad_centre_warp_ok(int hw, int sp, int rs)
+{
+    return (2 * (hw + sp)) / rs + 2 <= kCand;
+}
+
+__global__ void __launch_bounds__(32 * kCW) recon_grad_centre_warp_kernel(GArgs A)
+{
+    __shared__ short cand[kCW][2][kCand];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n = blockIdx.x * kCW + warp, b = blockIdx.y;
+    if (n >= A.Hs * A.Ws) return;   // the whole warp
+    const int j = n / A.Ws, i = n - j * A.Ws;
+    const size_t P = (size_t)A.H * A.W, R = (size_t)A.Hr * A.Wr, C = (size_t)A.Hs * A.Ws;
+    const size_t c = b * P + (size_t)(j * A.sp) * A.W + i * A.sp;
+    const size_t ci = b * C + n;
+    const int ox0 = max(0, (i * A.sp - A.hw - A.sp) / A.rs), ox1 = min(A.Wr - 1, (i * A.sp + A.hw + A.sp) / A.rs);
+    const int oy0 = max(0, (j * A.sp - A.hw - A.sp) / A.rs), oy1 = min(A.Hr - 1, (j * A.sp + A.hw + A.sp) / A.rs);
+    short *lx = cand[warp][0], *ly = cand[warp][1];
+    const unsigned below = (1u << lane) - 1u;
+    int nx = 0, ny = 0;
+    for (int base = ox0; base <= ox1; base += 32) {
+        const int ox = base + lane;
+        bool in = false;
+        if (ox <= ox1) {
+            int sx, ex;
+            centre_range(ox * A.rs, A.W, A.hw, A.sp, sx, ex);
+            in = i >= sx && i <= ex;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, in);
+        if (in) lx[nx + __popc(m & below)] = (short)ox;
+        nx += __popc(m);
+    }
+    for (int base = oy0; base <= oy1; base += 32) {
+        const int oy = base + lane;
+        bool in = false;
+        if (oy <= oy1) {
+            int sy, ey;
+            centre_range(oy * A.rs, A.H, A.hw, A.sp, sy, ey);
+            in = j >= sy && j <= ey;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, in);
+        if (in) ly[ny + __popc(m & below)] = (short)oy;
+        ny += __popc(m);
+    }
+    __syncwarp();
+    const int npair = nx * ny;
+    const int kx0 = nx ? lane % nx : 0, ky0 = nx ? lane / nx : 0;
+    const int stx = nx ? 32 % nx : 0, sty = nx ? 32 / nx : 0;
+    const float3 ac = f3(A.alb, c), nc = f3(A.nrm, c);
+    float3 galb = make_float3(0.f, 0.f, 0.f), gnn = galb;
+    for (int X = 0; X < 2; ++X) {
+        const GBuf &B_ = A.bf[X];
+        const float3 fc = f3(B_.f, c);
+        const float vc = __ldg(B_.v + c), sc = __ldg(B_.s + c);
+        float beta[kBeta], gb[kBeta];
+#pragma unroll
+        for (int k = 0; k < kBeta; ++k) {
+            beta[k] = __ldg(B_.beta + ci * kBeta + k);
+            gb[k] = 0.f;
+        }
+        float3 gf = make_float3(0.f, 0.f, 0.f);
+        float gs = 0.f, gv = 0.f;
+        PairGrad g;
+        int kx = kx0, ky = ky0;
+        for (int k = lane; k < npair; k += 32) {
+            const int ox = lx[kx], oy = ly[ky];
+            kx += stx;
+            ky += sty;
+            if (kx >= nx) {
+                kx -= nx;
+                ++ky;
+            }
+            const size_t p = b * P + (size_t)(oy * A.rs) * A.W + ox * A.rs;
+            const size_t o = b * R + (size_t)oy * A.Wr + ox;
+            const float3 ap = f3(A.alb, p), np_ = f3(A.nrm, p);
+            const float3 da = make_float3(ap.x - ac.x, ap.y - ac.y, ap.z - ac.z);
+            const float3 dn = make_float3(np_.x - nc.x, np_.y - nc.y, np_.z - nc.z);
+            const float gN[3] = {__ldg(B_.gN + 3 * o), __ldg(B_.gN + 3 * o + 1), __ldg(B_.gN + 3 * o + 2)};
+            recon_pair<true>(f3(B_.f, p), fc, __ldg(B_.s + p), sc, __ldg(B_.v + p), vc, da, dn, beta, gN,
+                             __ldg(B_.gD + o), g);
+#pragma unroll
+            for (int q = 0; q < kBeta; ++q) gb[q] += g.gbeta[q];
+            gf.x -= g.gdf.x;
+            gf.y -= g.gdf.y;
+            gf.z -= g.gdf.z;
+            gs += g.gden;
+            gv += g.gV;
+            galb.x -= g.gda.x;
+            galb.y -= g.gda.y;
+            galb.z -= g.gda.z;
+            gnn.x -= g.gdn.x;
+            gnn.y -= g.gdn.y;
+            gnn.z -= g.gdn.z;
+        }
+#pragma unroll
+        for (int q = 0; q < kBeta; ++q) gb[q] = warp_sum(gb[q]);
+        gf = make_float3(warp_sum(gf.x), warp_sum(gf.y), warp_sum(gf.z));
+        gs = warp_sum(gs);
+        gv = warp_sum(gv);
+        if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < kBeta; ++q) B_.gbeta[ci * kBeta + q] = gb[q];
+            add3(B_.gf, c, gf);
+            B_.gs[c] += gs;
+            B_.gv[c] += gv;
+        }
+    }
+    galb = make_float3(warp_sum(galb.x), warp_sum(galb.y), warp_sum(galb.z));
+    gnn = make_float3(warp_sum(gnn.x), warp_sum(gnn.y), warp_sum(gnn.z));
+    if (lane == 0) {
+        add3(A.galb, c, galb);
+        add3(A.gn, c, gnn);
+    }
+}
+
 // One regression tap of one buffer: the forward quantities and the
 // derivatives of dL with respect to the tap's inputs, given u and beta.
 struct TapGrad {
@@ -489,78 +640,152 @@ CD_DEV void regression_tap(float3 ft, float3 fc, float3 yt, float st, float sc, 
 
 // ---------------------------------------------------------------------------
 // Pass 4: u = A^-1 dL/dbeta with the stored Cholesky factor, then the
-// centre-side terms of every window tap.
+// centre-side terms of every window tap.  Built like the forward regression
+// kernel: a CTA owns 32 consecutive centres of one centre row, warp 0 takes
+// buffer A and warp 1 buffer B, one thread per (centre, buffer), and the
+// window rows stream through two shared-memory row slots (window_rows.cuh;
+// cp.async, double buffered), a tap being four conflict-free LDS.128.  The
+// albedo and normal terms of a centre's two buffers are summed by warp 0
+// (buffer A's terms first) through shared memory.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) regression_grad_centre_kernel(GArgs A)
+__host__ __device__ inline size_t grad_centre_smem(int hw, int sp)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= A.Ws || j >= A.Hs) return;
+    const RowGeom g = row_geom(hw, sp);
+    return (size_t)2 * 4 * g.npos * sizeof(float4) + (size_t)2 * g.rw * sizeof(int) +
+           (size_t)kRowCentres * 6 * sizeof(float);
+}
+
+__global__ void __launch_bounds__(64, 8) regression_grad_centre_kernel(GArgs A)
+{
+    extern __shared__ float4 sm4[];
+    const RowGeom g = row_geom(A.hw, A.sp);
+    const int slot = 4 * g.npos;   // float4s per slot
+    int *pos_gx = reinterpret_cast<int *>(sm4 + 2 * slot);
+    int *pos_dst = pos_gx + g.rw;
+    float *other = reinterpret_cast<float *>(pos_dst + g.rw);   // buffer B's albedo / normal terms
     const int b = blockIdx.z;
     const size_t P = (size_t)A.H * A.W, C = (size_t)A.Hs * A.Ws;
-    const int cx = i * A.sp, cy = j * A.sp;
-    const size_t c = b * P + (size_t)cy * A.W + cx;
-    const size_t ci = b * C + (size_t)j * A.Ws + i;
-    const float3 ac = f3(A.alb, c), nc = f3(A.nrm, c);
-    float3 galb = make_float3(0.f, 0.f, 0.f), gnn = galb;
-    for (int X = 0; X < 2; ++X) {
-        const GBuf &B_ = A.bf[X];
-        float u[kBeta], beta[kBeta];
+    const int i0 = blockIdx.x * kRowCentres, cy = blockIdx.y * A.sp;
+    const int X = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int Rw = 2 * A.hw + 1;
+    const float *imga = A.bf[0].f + 3 * P * b, *imgb = A.bf[1].f + 3 * P * b;
+    const float *alb = A.alb + 3 * P * b, *nrm = A.nrm + 3 * P * b;
+    const float *vara = A.bf[0].v + P * b, *varb = A.bf[1].v + P * b;
+    const float *sda = A.bf[0].s + P * b, *sdb = A.bf[1].s + P * b;
+
+    row_positions(pos_gx, pos_dst, g, i0 * A.sp - A.hw, A.W, A.sp, threadIdx.x, 64);
+    __syncthreads();
+    auto stage = [&](int r, int s) {
+        stage_window_row(reinterpret_cast<float *>(sm4 + s * slot), g, pos_gx, pos_dst,
+                         clampi(mirror(cy - A.hw + r, A.H), 0, A.H - 1), A.W, imga, imgb, alb, nrm, vara, varb, sda,
+                         sdb, threadIdx.x, 64);
+    };
+    stage(0, 0);
+    cp_async_commit();
+
+    // the thread's centre (clamped for lanes past the last centre) and u
+    const int i = min(i0 + lane, A.Ws - 1);
+    const size_t c = (size_t)cy * A.W + (size_t)i * A.sp;   // within the image
+    const size_t ci = b * C + (size_t)blockIdx.y * A.Ws + i;
+    const float *Lc = (X ? A.bf[1].L : A.bf[0].L) + ci * kL;
+    const float *gbeta = (X ? A.bf[1].gbeta : A.bf[0].gbeta) + ci * kBeta;
+    const float *betap = (X ? A.bf[1].beta : A.bf[0].beta) + ci * kBeta;
+    float u[kBeta], beta[kBeta];
 #pragma unroll
-        for (int k = 0; k < kBeta; ++k) beta[k] = __ldg(B_.beta + ci * kBeta + k);
-        // per channel: L z = g, L^T u = z (L lower triangular, row-major packed)
+    for (int k = 0; k < kBeta; ++k) beta[k] = __ldg(betap + k);
+    // per channel: L z = g, L^T u = z (L lower triangular, row-major packed)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const float *Lk = B_.L + ci * kL + 21 * k;
-            float z[kP];
+    for (int k = 0; k < 3; ++k) {
+        const float *Lk = Lc + 21 * k;
+        float z[kP];
 #pragma unroll
-            for (int r = 0; r < kP; ++r) {
-                float s = B_.gbeta[ci * kBeta + r * 3 + k];
+        for (int r = 0; r < kP; ++r) {
+            float s = gbeta[r * 3 + k];
 #pragma unroll
-                for (int q = 0; q < r; ++q) s -= __ldg(Lk + r * (r + 1) / 2 + q) * z[q];
-                z[r] = s / __ldg(Lk + r * (r + 1) / 2 + r);
-            }
-#pragma unroll
-            for (int r = kP - 1; r >= 0; --r) {
-                float s = z[r];
-#pragma unroll
-                for (int q = r + 1; q < kP; ++q) s -= __ldg(Lk + q * (q + 1) / 2 + r) * u[q * 3 + k];
-                u[r * 3 + k] = s / __ldg(Lk + r * (r + 1) / 2 + r);
-            }
+            for (int q = 0; q < r; ++q) s -= __ldg(Lk + r * (r + 1) / 2 + q) * z[q];
+            z[r] = s / __ldg(Lk + r * (r + 1) / 2 + r);
         }
 #pragma unroll
-        for (int k = 0; k < kBeta; ++k) B_.u[ci * kBeta + k] = u[k];
-        const float3 fc = f3(B_.f, c);
-        const float vc = __ldg(B_.v + c), sc = __ldg(B_.s + c);
-        float3 gf = make_float3(0.f, 0.f, 0.f);
-        float gs = 0.f, gv = 0.f;
-        TapGrad g;
-        for (int dy = -A.hw; dy <= A.hw; ++dy) {
-            const int ty = mirror(cy + dy, A.H);
-            for (int dx = -A.hw; dx <= A.hw; ++dx) {
-                const size_t t = b * P + (size_t)ty * A.W + mirror(cx + dx, A.W);
-                const float3 at = f3(A.alb, t), nt = f3(A.nrm, t);
-                regression_tap(f3(B_.f, t), fc, f3(B_.y, t), __ldg(B_.s + t), sc, __ldg(B_.v + t), vc,
-                               make_float3(at.x - ac.x, at.y - ac.y, at.z - ac.z),
-                               make_float3(nt.x - nc.x, nt.y - nc.y, nt.z - nc.z), u, beta, g);
-                gf.x -= g.gdf.x;
-                gf.y -= g.gdf.y;
-                gf.z -= g.gdf.z;
-                gs += g.gden;
-                gv += g.gV;
-                galb.x -= g.gda.x;
-                galb.y -= g.gda.y;
-                galb.z -= g.gda.z;
-                gnn.x -= g.gdn.x;
-                gnn.y -= g.gdn.y;
-                gnn.z -= g.gdn.z;
-            }
+        for (int r = kP - 1; r >= 0; --r) {
+            float s = z[r];
+#pragma unroll
+            for (int q = r + 1; q < kP; ++q) s -= __ldg(Lk + q * (q + 1) / 2 + r) * u[q * 3 + k];
+            u[r * 3 + k] = s / __ldg(Lk + r * (r + 1) / 2 + r);
         }
-        add3(B_.gf, c, gf);
-        B_.gs[c] += gs;
-        B_.gv[c] += gv;
     }
-    add3(A.galb, c, galb);
-    add3(A.gn, c, gnn);
+    const bool valid = i0 + lane < A.Ws;
+    if (valid) {
+        float *ug = (X ? A.bf[1].u : A.bf[0].u) + ci * kBeta;
+#pragma unroll
+        for (int k = 0; k < kBeta; ++k) ug[k] = u[k];
+    }
+    const float3 fc = ld3(X ? imgb : imga, c), ac = ld3(alb, c), nc = ld3(nrm, c);
+    const float vc = __ldg((X ? varb : vara) + c), sc = __ldg((X ? sdb : sda) + c);
+    const int gfi = X ? 1 : 0, gyi = X ? 0 : 1;   // own features + variance, target
+
+    float3 gf = make_float3(0.f, 0.f, 0.f), galb = gf, gnn = gf;
+    float gs = 0.f, gv = 0.f;
+    TapGrad tg;
+    for (int r = 0; r < Rw; ++r) {
+        if (r + 1 < Rw) {
+            stage(r + 1, (r + 1) & 1);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const float4 *Pp = sm4 + (r & 1) * slot;
+        const float4 *Gf = Pp + gfi * g.npos, *Gy = Pp + gyi * g.npos;
+        const float4 *Ga = Pp + 2 * g.npos, *Gn = Pp + 3 * g.npos;
+        int tm = 0, td = 0;
+        for (int t = 0; t < Rw; ++t) {
+            const int o = tm * g.q + td + lane;
+            const float4 f4 = Gf[o], y4 = Gy[o], a4 = Ga[o], n4 = Gn[o];
+            const float st = X ? n4.w : a4.w;   // sdA rides in g2.w, sdB in g3.w
+            regression_tap(make_float3(f4.x, f4.y, f4.z), fc, make_float3(y4.x, y4.y, y4.z), st, sc, f4.w, vc,
+                           make_float3(a4.x - ac.x, a4.y - ac.y, a4.z - ac.z),
+                           make_float3(n4.x - nc.x, n4.y - nc.y, n4.z - nc.z), u, beta, tg);
+            gf.x -= tg.gdf.x;
+            gf.y -= tg.gdf.y;
+            gf.z -= tg.gdf.z;
+            gs += tg.gden;
+            gv += tg.gV;
+            galb.x -= tg.gda.x;
+            galb.y -= tg.gda.y;
+            galb.z -= tg.gda.z;
+            gnn.x -= tg.gdn.x;
+            gnn.y -= tg.gdn.y;
+            gnn.z -= tg.gdn.z;
+            if (++tm == A.sp) {
+                tm = 0;
+                ++td;
+            }
+        }
+        __syncthreads();
+    }
+    const size_t cp = b * P + c;
+    if (valid) {
+        const GBuf &B_ = X ? A.bf[1] : A.bf[0];
+        add3(B_.gf, cp, gf);
+        B_.gs[cp] += gs;
+        B_.gv[cp] += gv;
+    }
+    if (X == 1) {
+        other[6 * lane] = galb.x;
+        other[6 * lane + 1] = galb.y;
+        other[6 * lane + 2] = galb.z;
+        other[6 * lane + 3] = gnn.x;
+        other[6 * lane + 4] = gnn.y;
+        other[6 * lane + 5] = gnn.z;
+    }
+    __syncthreads();
+    if (X == 0 && valid) {
+        add3(A.galb, cp, make_float3(galb.x + other[6 * lane], galb.y + other[6 * lane + 1],
+                                     galb.z + other[6 * lane + 2]));
+        add3(A.gn, cp, make_float3(gnn.x + other[6 * lane + 3], gnn.y + other[6 * lane + 4],
+                                   gnn.z + other[6 * lane + 5]));
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -634,7 +859,7 @@ __global__ void __launch_bounds__(256) regression_grad_tap_kernel(GArgs A)
             }
         }
         add3(B_.gf, q, gf);
-        add3(B_.gy, q, gy);
+        st3(B_.gy, q, gy);   // the only writer of gy
         B_.gs[q] += gs;
         B_.gv[q] += gv;
     }
@@ -642,25 +867,30 @@ __global__ void __launch_bounds__(256) regression_grad_tap_kernel(GArgs A)
     add3(A.gn, q, gnn);
 }
 
-// Pass 5 with the tile's centres staged in shared memory.  Along each axis
-// the centres any pixel of a 32 x 8 tile reaches (directly, or through the
-// reflect-101 images -q near the low edge and 2n-2-q near the high edge,
-// which only occur when the direct range already reaches centre 0 or the
-// last centre) form one range [lo, hi]; a record per centre holds both
-// buffers' features, standard deviation, variance, u and coefficients and
-// the shared albedo and normal.  Same pairs, order and arithmetic as
-// regression_grad_tap_kernel.
-constexpr int kRecT = 88;   // per buffer X at 41 X: f[3] s v u[18] beta[18]; alb[3] at 82, nrm[3] at 85
+// Pass 5 with the tile's centres staged in shared memory and both buffers
+// as packed FP32x2 lanes.  Along each axis the centres any pixel of a
+// 32 x 8 tile reaches (directly, or through the reflect-101 images -q near
+// the low edge and 2n-2-q near the high edge, which only occur when the
+// direct range already reaches centre 0 or the last centre) form one range
+// [lo, hi]; a record of kRecT2 float4s per centre holds (pairs (A, B)
+// unless noted):
+//   0  f.x f.y   1  f.z s   2  v | alb.x alb.y (scalars)   3  alb.z nrm.xyz (scalars)
+//   4 + 3k + m   u of channel k, rows 2m and 2m + 1
+//   13 + 3k + m  coefficients of channel k, rows 2m and 2m + 1
+// A warp covers 4 x 8 pixels of the tile (shared-memory broadcast, as in
+// pass 2).  Same pairs and order as regression_grad_tap_kernel.
+constexpr int kRecT2 = 22;
 
 __host__ __device__ inline size_t tap_grad_smem(int hw, int sp)
 {
     const int ncx = (31 + 2 * hw) / sp + 2, ncy = (7 + 2 * hw) / sp + 2;
-    return (size_t)ncx * ncy * kRecT * sizeof(float);
+    return (size_t)ncx * ncy * kRecT2 * sizeof(float4);
 }
 
-__global__ void __launch_bounds__(256) regression_grad_tap_smem_kernel(GArgs A)
+__global__ void __launch_bounds__(256, 2) regression_grad_tap_x2_kernel(GArgs A)
 {
-    extern __shared__ float recs[];
+    using namespace x2;
+    extern __shared__ float4 rec4[];
     const int b = blockIdx.z;
     const size_t P = (size_t)A.H * A.W, C = (size_t)A.Hs * A.Ws;
     const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
@@ -669,98 +899,113 @@ __global__ void __launch_bounds__(256) regression_grad_tap_smem_kernel(GArgs A)
     const int cy_lo = y0 - A.hw > 0 ? (y0 - A.hw + A.sp - 1) / A.sp : 0;
     const int cx_hi = min(A.Ws - 1, (x1 + A.hw) / A.sp), cy_hi = min(A.Hs - 1, (y1 + A.hw) / A.sp);
     const int ncx = cx_hi - cx_lo + 1, ncy = cy_hi - cy_lo + 1;
-    const int tid = threadIdx.y * 32 + threadIdx.x;
-    for (int e = tid; e < ncx * ncy * 5; e += 256) {
-        const int n = e / 5, part = e - 5 * n;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < ncx * ncy * 7; e += 256) {
+        const int n = e / 7, part = e - 7 * n;
         const int iy = cy_lo + n / ncx, ix = cx_lo + n % ncx;
         const size_t c = b * P + (size_t)(iy * A.sp) * A.W + ix * A.sp;
         const size_t ci = b * C + (size_t)iy * A.Ws + ix;
-        float *r = recs + (size_t)n * kRecT;
-        if (part < 2) {                       // features, sd, var, u of buffer `part`
-            const GBuf &B_ = A.bf[part];
-            float *q = r + 41 * part;
-            const float3 f = f3(B_.f, c);
-            q[0] = f.x;
-            q[1] = f.y;
-            q[2] = f.z;
-            q[3] = __ldg(B_.s + c);
-            q[4] = __ldg(B_.v + c);
-#pragma unroll
-            for (int k = 0; k < kBeta; ++k) q[5 + k] = B_.u[ci * kBeta + k];
-        } else if (part < 4) {                // coefficients of buffer part - 2
-            const GBuf &B_ = A.bf[part - 2];
-            float *q = r + 41 * (part - 2) + 23;
-#pragma unroll
-            for (int k = 0; k < kBeta; ++k) q[k] = __ldg(B_.beta + ci * kBeta + k);
-        } else {
-            const float3 al = f3(A.alb, c), nr = f3(A.nrm, c);
-            r[82] = al.x;
-            r[83] = al.y;
-            r[84] = al.z;
-            r[85] = nr.x;
-            r[86] = nr.y;
-            r[87] = nr.z;
-        }
+        float4 *r = rec4 + (size_t)n * kRecT2;
+        if (part == 0)
+            stage_head(r, A, c);
+        else if (part <= 3)
+            stage_rows(r + 4 + 3 * (part - 1), A.bf[0].u, A.bf[1].u, ci, part - 1);
+        else
+            stage_rows(r + 13 + 3 * (part - 4), A.bf[0].beta, A.bf[1].beta, ci, part - 4);
     }
     __syncthreads();
 
-    const int qx = x0 + threadIdx.x, qy = y0 + threadIdx.y;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int qx = x0 + 4 * warp + (lane & 3), qy = y0 + (lane >> 2);
     if (qx >= A.W || qy >= A.H) return;
     const size_t q = b * P + (size_t)qy * A.W + qx;
     int txs[3], tys[3];
     const int ntx = tap_positions(qx, A.W, A.hw, (A.Ws - 1) * A.sp, txs);
     const int nty = tap_positions(qy, A.H, A.hw, (A.Hs - 1) * A.sp, tys);
     const float3 at = f3(A.alb, q), nt = f3(A.nrm, q);
-    float3 galb = make_float3(0.f, 0.f, 0.f), gnn = galb;
-    for (int X = 0; X < 2; ++X) {
-        const GBuf &B_ = A.bf[X];
-        const float3 ft = f3(B_.f, q), yt = f3(B_.y, q);
-        const float vt = __ldg(B_.v + q), st = __ldg(B_.s + q);
-        float3 gf = make_float3(0.f, 0.f, 0.f), gy = gf;
-        float gs = 0.f, gv = 0.f;
-        TapGrad g;
-        for (int a = 0; a < nty; ++a) {
-            const int ty = tys[a];
-            const int j0 = max(0, (ty - A.hw + A.sp - 1) >= 0 ? (ty - A.hw + A.sp - 1) / A.sp : 0);
-            const int j1 = min(A.Hs - 1, (ty + A.hw) >= 0 ? (ty + A.hw) / A.sp : -1);
-            for (int j = j0; j <= j1; ++j) {
-                if (abs(j * A.sp - ty) > A.hw) continue;
-                for (int bb = 0; bb < ntx; ++bb) {
-                    const int tx = txs[bb];
-                    const int i0 = max(0, (tx - A.hw + A.sp - 1) >= 0 ? (tx - A.hw + A.sp - 1) / A.sp : 0);
-                    const int i1 = min(A.Ws - 1, (tx + A.hw) >= 0 ? (tx + A.hw) / A.sp : -1);
-                    for (int i = i0; i <= i1; ++i) {
-                        if (abs(i * A.sp - tx) > A.hw) continue;
-                        const float *r = recs + (size_t)((j - cy_lo) * ncx + (i - cx_lo)) * kRecT;
-                        const float *rq = r + 41 * X;
-                        regression_tap(ft, make_float3(rq[0], rq[1], rq[2]), yt, st, rq[3], vt, rq[4],
-                                       make_float3(at.x - r[82], at.y - r[83], at.z - r[84]),
-                                       make_float3(nt.x - r[85], nt.y - r[86], nt.z - r[87]), rq + 5, rq + 23, g);
-                        gf.x += g.gdf.x;
-                        gf.y += g.gdf.y;
-                        gf.z += g.gdf.z;
-                        gy.x += g.gy.x;
-                        gy.y += g.gy.y;
-                        gy.z += g.gy.z;
-                        gs += g.gden;
-                        gv += g.gV;
-                        galb.x += g.gda.x;
-                        galb.y += g.gda.y;
-                        galb.z += g.gda.z;
-                        gnn.x += g.gdn.x;
-                        gnn.y += g.gdn.y;
-                        gnn.z += g.gdn.z;
+    const float3 fqa = f3(A.bf[0].f, q), fqb = f3(A.bf[1].f, q);
+    const f2 ft[3] = {pack(fqa.x, fqb.x), pack(fqa.y, fqb.y), pack(fqa.z, fqb.z)};
+    const f2 yt[3] = {pack(fqb.x, fqa.x), pack(fqb.y, fqa.y), pack(fqb.z, fqa.z)};   // y of A is imgb
+    const f2 stt = pack(__ldg(A.bf[0].s + q), __ldg(A.bf[1].s + q));
+    const f2 vtt = pack(__ldg(A.bf[0].v + q), __ldg(A.bf[1].v + q));
+    const f2 k1e2 = pack(1e-2f, 1e-2f), k1e4 = pack(1e-4f, 1e-4f), k1e7 = pack(1e-7f, 1e-7f);
+    const f2 two = pack(2.f, 2.f);
+    f2 gf[3] = {0ull, 0ull, 0ull}, gy[3] = {0ull, 0ull, 0ull}, ga[3] = {0ull, 0ull, 0ull};
+    f2 gn0 = 0ull, gn1 = 0ull, gn2 = 0ull, gs = 0ull, gv = 0ull;
+    for (int a_ = 0; a_ < nty; ++a_) {
+        const int ty = tys[a_];
+        const int j0 = max(0, (ty - A.hw + A.sp - 1) >= 0 ? (ty - A.hw + A.sp - 1) / A.sp : 0);
+        const int j1 = min(A.Hs - 1, (ty + A.hw) >= 0 ? (ty + A.hw) / A.sp : -1);
+        for (int j = j0; j <= j1; ++j) {
+            if (abs(j * A.sp - ty) > A.hw) continue;
+            for (int bb = 0; bb < ntx; ++bb) {
+                const int tx = txs[bb];
+                const int i0 = max(0, (tx - A.hw + A.sp - 1) >= 0 ? (tx - A.hw + A.sp - 1) / A.sp : 0);
+                const int i1 = min(A.Ws - 1, (tx + A.hw) >= 0 ? (tx + A.hw) / A.sp : -1);
+                for (int i = i0; i <= i1; ++i) {
+                    if (abs(i * A.sp - tx) > A.hw) continue;
+                    const float4 *R4 = rec4 + (size_t)((j - cy_lo) * ncx + (i - cx_lo)) * kRecT2;
+                    const ulonglong2 *RR = reinterpret_cast<const ulonglong2 *>(R4);
+                    const ulonglong2 h0 = RR[0], h1 = RR[1];
+                    const float4 q2 = R4[2], q3 = R4[3];
+                    const f2 df[3] = {sub2(ft[0], h0.x), sub2(ft[1], h0.y), sub2(ft[2], h1.x)};
+                    const f2 rden = rcp2(add2(add2(h1.y, stt), k1e2));
+                    const f2 rV = rcp2(add2(add2(pack(q2.x, q2.y), vtt), k1e4));
+                    const f2 dist = mul2(sqnorm2(df[0], df[1], df[2]), rV);
+                    const f2 e = expneg2(dist);
+                    const f2 w = add2(e, k1e7);
+                    const f2 da[3] = {dup2(at.x - q2.z), dup2(at.y - q2.w), dup2(at.z - q3.x)};
+                    const f2 dn0 = dup2(nt.x - q3.y), dn1 = dup2(nt.y - q3.z), dn2 = dup2(nt.z - q3.w);
+                    f2 gw = 0ull, gsum = 0ull, t1[3], t2[3], d1[3];
+                    f2 tn0 = 0ull, tn1 = 0ull, tn2 = 0ull;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const ulonglong2 u01 = RR[4 + 3 * k], u23 = RR[5 + 3 * k], u45 = RR[6 + 3 * k];
+                        const ulonglong2 b01 = RR[13 + 3 * k], b23 = RR[14 + 3 * k], b45 = RR[15 + 3 * k];
+                        d1[k] = mul2(df[k], rden);
+                        const f2 a = fma2(u45.y, dn2, fma2(u45.x, dn1, fma2(u23.y, dn0,
+                                         fma2(u23.x, da[k], fma2(u01.y, d1[k], u01.x)))));
+                        const f2 c = fma2(b45.y, dn2, fma2(b45.x, dn1, fma2(b23.y, dn0,
+                                         fma2(b23.x, da[k], fma2(b01.y, d1[k], b01.x)))));
+                        const f2 res = sub2(yt[k], c);
+                        gw = fma2(a, res, gw);
+                        gy[k] = fma2(w, a, gy[k]);
+                        const f2 na = neg2(a);
+                        // dL/ddelta_r / w = u_r res - a beta_r
+                        t1[k] = fma2(na, b01.y, mul2(u01.y, res));
+                        t2[k] = fma2(na, b23.x, mul2(u23.x, res));
+                        tn0 = fma2(na, b23.y, fma2(u23.y, res, tn0));
+                        tn1 = fma2(na, b45.x, fma2(u45.x, res, tn1));
+                        tn2 = fma2(na, b45.y, fma2(u45.y, res, tn2));
                     }
+                    const f2 gdist = neg2(mul2(gw, e));
+                    const f2 t = mul2(mul2(two, gdist), rV);
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const f2 g1 = mul2(w, t1[k]);
+                        gf[k] = add2(gf[k], fma2(t, df[k], mul2(g1, rden)));
+                        gsum = fma2(g1, d1[k], gsum);
+                        ga[k] = fma2(w, t2[k], ga[k]);
+                    }
+                    gn0 = fma2(w, tn0, gn0);
+                    gn1 = fma2(w, tn1, gn1);
+                    gn2 = fma2(w, tn2, gn2);
+                    gs = sub2(gs, mul2(gsum, rden));
+                    gv = sub2(gv, mul2(mul2(gdist, dist), rV));
                 }
             }
         }
-        add3(B_.gf, q, gf);
-        add3(B_.gy, q, gy);
-        B_.gs[q] += gs;
-        B_.gv[q] += gv;
     }
-    add3(A.galb, q, galb);
-    add3(A.gn, q, gnn);
+    for (int X = 0; X < 2; ++X) {
+        const GBuf &B_ = A.bf[X];
+        auto pick = [X](f2 v) { return X ? hi(v) : lo(v); };
+        add3(B_.gf, q, make_float3(pick(gf[0]), pick(gf[1]), pick(gf[2])));
+        st3(B_.gy, q, make_float3(pick(gy[0]), pick(gy[1]), pick(gy[2])));   // the only writer of gy
+        B_.gs[q] += pick(gs);
+        B_.gv[q] += pick(gv);
+    }
+    add3(A.galb, q, make_float3(lo(ga[0]) + hi(ga[0]), lo(ga[1]) + hi(ga[1]), lo(ga[2]) + hi(ga[2])));
+    add3(A.gn, q, make_float3(lo(gn0) + hi(gn0), lo(gn1) + hi(gn1), lo(gn2) + hi(gn2)));
 }
 
 // ---------------------------------------------------------------------------
@@ -835,33 +1080,75 @@ __global__ void __launch_bounds__(256) assemble_grad_kernel(GArgs A)
     st3(A.out_n, p, f3(A.gn, p));
 }
 
+// Workspace layout, offsets in floats, every region 16-byte aligned.  It
+// begins with the forward's quantities (kept by launch_regression_keep):
+// variance and standard deviation of A, then of B (P floats each), the
+// coefficients [buf][C][18], the Cholesky factors [buf][C][63] and the
+// reconstruction's (out[3], D) [buf][R] as float4; then the backward's own
+// planes, those that are accumulated last and zeroed before the passes.
+struct GradLayout {
+    size_t var[2], sd[2], beta, L, state, u[2], gbeta[2], gN[2], gD[2], gy[2], hn[2];
+    size_t zero_begin, gf[2], gs[2], gv[2], galb, gn, total;
+};
+
+GradLayout grad_layout(int B, int H, int W, int sp, int rs)
+{
+    const size_t P = (size_t)B * H * W, R = (size_t)B * (H / rs) * (W / rs), C = (size_t)B * (H / sp) * (W / sp);
+    GradLayout g{};
+    size_t cur = 0;
+    auto take = [&](size_t n) {
+        const size_t at = cur;
+        cur += (n + 3) & ~(size_t)3;
+        return at;
+    };
+    for (int X = 0; X < 2; ++X) {
+        g.var[X] = take(P);
+        g.sd[X] = take(P);
+    }
+    g.beta = take(2 * C * kBeta);   // [buf][C][18], the layout the forward kernels use
+    g.L = take(2 * C * kL);
+    g.state = take(2 * R * 4);
+    for (int X = 0; X < 2; ++X) {
+        g.u[X] = take(C * kBeta);
+        g.gbeta[X] = take(C * kBeta);
+        g.gN[X] = take(3 * R);
+        g.gD[X] = take(R);
+        g.gy[X] = take(3 * P);
+        g.hn[X] = take(3 * P);
+    }
+    g.zero_begin = cur;
+    for (int X = 0; X < 2; ++X) {
+        g.gf[X] = take(3 * P);
+        g.gs[X] = take(P);
+        g.gv[X] = take(P);
+    }
+    g.galb = take(3 * P);
+    g.gn = take(3 * P);
+    g.total = cur;
+    return g;
+}
+
 }  // namespace
 
 size_t regression_grad_workspace_floats(int B, int H, int W, int sp, int rs)
 {
-    const size_t P = (size_t)B * H * W, R = (size_t)B * (H / rs) * (W / rs), C = (size_t)B * (H / sp) * (W / sp);
-    // per buffer: v, s, gf(3), gy(3), gs, gv, hn(3) = 13 P; beta, L, u, gbeta = 117 C; gN(3), gD = 4 R
-    // shared: galb(3), gn(3) = 6 P
-    return 2 * (13 * P + 117 * C + 4 * R) + 6 * P;
+    return grad_layout(B, H, W, sp, rs).total;
 }
 
-// The workspace begins with the forward's quantities, in this order:
-// variance and standard deviation of A, then of B (P floats each), the
-// coefficients [buf][C][18] and the Cholesky factors [buf][C][63].
 cudaError_t launch_regression_keep(const float *imga, const float *imgb, const float *albedo, const float *normal,
                                    float *outa, float *outb, float *vara, float *varb, int B, int H, int W, int win,
                                    int sp, int rs, float *ws, cudaStream_t st)
 {
-    const size_t P = (size_t)B * H * W, C = (size_t)B * (H / sp) * (W / sp);
-    float *v0 = ws, *s0 = ws + P, *v1 = ws + 2 * P, *s1 = ws + 3 * P;
-    float *beta = ws + 4 * P, *L = beta + 2 * C * kBeta;
+    const GradLayout g = grad_layout(B, H, W, sp, rs);
+    const size_t P = (size_t)B * H * W;
+    float *v0 = ws + g.var[0], *s0 = ws + g.sd[0], *v1 = ws + g.var[1], *s1 = ws + g.sd[1];
     cudaError_t e;
     if ((e = launch_variance(imga, imgb, v0, v1, s0, s1, B, H, W, st)) != cudaSuccess) return e;
-    if ((e = launch_regression(imga, imgb, albedo, normal, v0, v1, s0, s1, beta, B, H, W, win, sp, st, L)) !=
-        cudaSuccess)
+    if ((e = launch_regression(imga, imgb, albedo, normal, v0, v1, s0, s1, ws + g.beta, B, H, W, win, sp, st,
+                               ws + g.L)) != cudaSuccess)
         return e;
-    if ((e = launch_recon(imga, imgb, albedo, normal, v0, v1, s0, s1, beta, outa, outb, B, H, W, win, sp, rs, st)) !=
-        cudaSuccess)
+    if ((e = launch_recon(imga, imgb, albedo, normal, v0, v1, s0, s1, ws + g.beta, outa, outb, B, H, W, win, sp, rs,
+                          st, ws + g.state)) != cudaSuccess)
         return e;
     if ((e = cudaMemcpyAsync(vara, v0, P * sizeof(float), cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
     return cudaMemcpyAsync(varb, v1, P * sizeof(float), cudaMemcpyDeviceToDevice, st);
@@ -873,7 +1160,7 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
                                    float *g_normal, int B, int H, int W, int win, int sp, int rs, float *ws,
                                    cudaStream_t st, bool kept)
 {
-    const size_t P = (size_t)B * H * W, R = (size_t)B * (H / rs) * (W / rs), C = (size_t)B * (H / sp) * (W / sp);
+    const GradLayout L = grad_layout(B, H, W, sp, rs);
     GArgs A{};
     A.H = H;
     A.W = W;
@@ -884,83 +1171,80 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
     A.Ws = W / sp;
     A.Hr = H / rs;
     A.Wr = W / rs;
-    float *cur = ws;
-    auto take = [&](size_t n) {
-        float *p = cur;
-        cur += n;
-        return p;
-    };
-    float *var[2], *sd[2], *beta, *L, *u[2], *gbeta[2];
-    for (int X = 0; X < 2; ++X) {
-        var[X] = take(P);
-        sd[X] = take(P);
-    }
-    beta = take(2 * C * kBeta);   // [buf][C][18], the layout the forward kernels use
-    L = take(2 * C * kL);
-    for (int X = 0; X < 2; ++X) {
-        u[X] = take(C * kBeta);
-        gbeta[X] = take(C * kBeta);
-    }
-    float *zero_begin = cur;      // everything below is accumulated and starts at zero
+    const size_t C = (size_t)B * A.Hs * A.Ws;
     for (int X = 0; X < 2; ++X) {
         GBuf &g = A.bf[X];
         g.f = X ? imgb : imga;
         g.y = X ? imga : imgb;
-        g.v = var[X];
-        g.s = sd[X];
-        g.beta = beta + X * C * kBeta;
-        g.L = L + X * C * kL;
-        g.u = u[X];
-        g.gbeta = gbeta[X];
-        g.gN = take(3 * R);
-        g.gD = take(R);
-        g.gf = take(3 * P);
-        g.gy = take(3 * P);
-        g.gs = take(P);
-        g.gv = take(P);
-        g.hn = take(3 * P);
+        g.v = ws + L.var[X];
+        g.s = ws + L.sd[X];
+        g.beta = ws + L.beta + X * C * kBeta;
+        g.L = ws + L.L + X * C * kL;
+        g.u = ws + L.u[X];
+        g.gbeta = ws + L.gbeta[X];
+        g.gN = ws + L.gN[X];
+        g.gD = ws + L.gD[X];
+        g.gf = ws + L.gf[X];
+        g.gy = ws + L.gy[X];
+        g.gs = ws + L.gs[X];
+        g.gv = ws + L.gv[X];
+        g.hn = ws + L.hn[X];
         g.gout = X ? g_outb : g_outa;
         g.gvar = X ? g_varb : g_vara;
     }
+    A.state = reinterpret_cast<const float4 *>(ws + L.state);
     A.alb = albedo;
     A.nrm = normal;
-    A.galb = take(3 * P);
-    A.gn = take(3 * P);
+    A.galb = ws + L.galb;
+    A.gn = ws + L.gn;
     A.out_a = g_imga;
     A.out_b = g_imgb;
     A.out_alb = g_albedo;
     A.out_n = g_normal;
-    cudaError_t e = cudaMemsetAsync(zero_begin, 0, (size_t)(cur - zero_begin) * sizeof(float), st);
+    cudaError_t e = cudaMemsetAsync(ws + L.zero_begin, 0, (L.total - L.zero_begin) * sizeof(float), st);
     if (e != cudaSuccess) return e;
 
     // pass 1: forward quantities (variance, std, coefficients, Cholesky
-    // factors), unless launch_regression_keep left them in the workspace
+    // factors, the reconstruction's outputs and weight sums), unless
+    // launch_regression_keep left them in the workspace
     if (!kept) {
-        if ((e = launch_variance(imga, imgb, var[0], var[1], sd[0], sd[1], B, H, W, st)) != cudaSuccess) return e;
-        if ((e = launch_regression(imga, imgb, albedo, normal, var[0], var[1], sd[0], sd[1], beta, B, H, W, win,
-                                   sp, st, L)) != cudaSuccess)
+        float *v0 = ws + L.var[0], *v1 = ws + L.var[1], *s0 = ws + L.sd[0], *s1 = ws + L.sd[1];
+        if ((e = launch_variance(imga, imgb, v0, v1, s0, s1, B, H, W, st)) != cudaSuccess) return e;
+        if ((e = launch_regression(imga, imgb, albedo, normal, v0, v1, s0, s1, ws + L.beta, B, H, W, win, sp, st,
+                                   ws + L.L)) != cudaSuccess)
+            return e;
+        if ((e = launch_recon(imga, imgb, albedo, normal, v0, v1, s0, s1, ws + L.beta, nullptr, nullptr, B, H, W,
+                              win, sp, rs, st, ws + L.state)) != cudaSuccess)
             return e;
     }
     dim3 blk(32, 8);
     dim3 g_out((A.Wr + 31) / 32, (A.Hr + 7) / 8, B), g_cen((A.Ws + 31) / 32, (A.Hs + 7) / 8, B);
     dim3 g_px((W + 31) / 32, (H + 7) / 8, B);
+    dim3 g_warp((A.Hs * A.Ws + kCW - 1) / kCW, B);
     const size_t rg_smem = recon_grad_smem(A.hw, A.sp, A.rs);
     if (rg_smem <= 200 * 1024) {
-        if ((e = cudaFuncSetAttribute(recon_grad_pixel_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if ((e = cudaFuncSetAttribute(recon_grad_pixel_x2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)rg_smem)) != cudaSuccess)
             return e;
-        recon_grad_pixel_smem_kernel<<<g_out, blk, rg_smem, st>>>(A);
+        recon_grad_pixel_x2_kernel<<<g_out, 256, rg_smem, st>>>(A);
     } else {
         recon_grad_pixel_kernel<<<g_out, blk, 0, st>>>(A);
     }
-    recon_grad_centre_kernel<<<g_cen, blk, 0, st>>>(A);
-    regression_grad_centre_kernel<<<dim3((A.Ws + 15) / 16, (A.Hs + 7) / 8, B), dim3(16, 8), 0, st>>>(A);
+    if (recon_grad_centre_warp_ok(A.hw, A.sp, A.rs))
+        recon_grad_centre_warp_kernel<<<g_warp, 32 * kCW, 0, st>>>(A);
+    else
+        recon_grad_centre_kernel<<<g_cen, blk, 0, st>>>(A);
+    const size_t gc_smem = grad_centre_smem(A.hw, A.sp);
+    if ((e = cudaFuncSetAttribute(regression_grad_centre_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)gc_smem)) != cudaSuccess)
+        return e;
+    regression_grad_centre_kernel<<<dim3((A.Ws + kRowCentres - 1) / kRowCentres, A.Hs, B), 64, gc_smem, st>>>(A);
     const size_t tg_smem = tap_grad_smem(A.hw, A.sp);
     if (tg_smem <= 200 * 1024) {
-        if ((e = cudaFuncSetAttribute(regression_grad_tap_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if ((e = cudaFuncSetAttribute(regression_grad_tap_x2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)tg_smem)) != cudaSuccess)
             return e;
-        regression_grad_tap_smem_kernel<<<g_px, blk, tg_smem, st>>>(A);
+        regression_grad_tap_x2_kernel<<<g_px, 256, tg_smem, st>>>(A);
     } else {
         regression_grad_tap_kernel<<<g_px, blk, 0, st>>>(A);
     }
