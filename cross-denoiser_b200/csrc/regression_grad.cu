@@ -25,9 +25,10 @@
 //      reconstruction keeping each output pixel's outputs and weight sum D
 //   2. recon backward, pixel side (dL/dN, dL/dD from the kept outputs and D,
 //      stored per output pixel)
-//   3. recon backward, centre side (dL/dbeta), one warp per centre
-//   4. solve backward (u) and the regression's centre-side terms, one warp
-//      per centre
+//   3. recon backward, centre side (dL/dbeta), one thread per (centre,
+//      buffer), the output rows streamed through shared memory
+//   4. solve backward (u) and the regression's centre-side terms, one thread
+//      per (centre, buffer), the window rows streamed through shared memory
 //   5. the regression's tap-side terms, gathered per pixel over every
 //      (centre, window position) whose reflect-101 image is that pixel
 //   6. sqrt / variance chain and assembly of dL/dimga, dL/dimgb, dL/dalbedo,
@@ -137,13 +138,6 @@ CD_DEV void recon_upstream(float4 S, float3 G, float gN[3], float &gD)
         gD -= gN[k] * ov[k];
     }
     if (!(S.w > 1e-7f)) gD = 0.f;
-}
-
-CD_DEV float warp_sum(float v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
 }
 
 CD_DEV void centre_range(int pos, int n, int hw, int sp, int &lo, int &hi)
@@ -465,129 +459,6 @@ __global__ void __launch_bounds__(256) recon_grad_centre_kernel(GArgs A)
     add3(A.gn, c, gnn);
 }
 
-// Pass 3, one warp per centre: the output pixels whose centre range holds
-// the centre are listed per axis (tested by the forward's range rule on the
-// candidate box, one candidate per lane), the warp's lanes take the
-// (pixel row, pixel column) pairs of the two lists in turn, and the lanes'
-// partial sums are reduced by a fixed butterfly (deterministic).  Needs at
-// most kCand candidates per axis; recon_grad_centre_kernel serves the rest.
-constexpr int kCand = 64, kCW = 8;   // candidates per axis, warps (centres) per CTA
-
-__host__ __device__ inline bool recon_grad_centre_warp_ok(int hw, int sp, int rs)
-{
-    return (2 * (hw + sp)) / rs + 2 <= kCand;
-}
-
-__global__ void __launch_bounds__(32 * kCW) recon_grad_centre_warp_kernel(GArgs A)
-{
-    __shared__ short cand[kCW][2][kCand];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n = blockIdx.x * kCW + warp, b = blockIdx.y;
-    if (n >= A.Hs * A.Ws) return;   // the whole warp
-    const int j = n / A.Ws, i = n - j * A.Ws;
-    const size_t P = (size_t)A.H * A.W, R = (size_t)A.Hr * A.Wr, C = (size_t)A.Hs * A.Ws;
-    const size_t c = b * P + (size_t)(j * A.sp) * A.W + i * A.sp;
-    const size_t ci = b * C + n;
-    const int ox0 = max(0, (i * A.sp - A.hw - A.sp) / A.rs), ox1 = min(A.Wr - 1, (i * A.sp + A.hw + A.sp) / A.rs);
-    const int oy0 = max(0, (j * A.sp - A.hw - A.sp) / A.rs), oy1 = min(A.Hr - 1, (j * A.sp + A.hw + A.sp) / A.rs);
-    short *lx = cand[warp][0], *ly = cand[warp][1];
-    const unsigned below = (1u << lane) - 1u;
-    int nx = 0, ny = 0;
-    for (int base = ox0; base <= ox1; base += 32) {
-        const int ox = base + lane;
-        bool in = false;
-        if (ox <= ox1) {
-            int sx, ex;
-            centre_range(ox * A.rs, A.W, A.hw, A.sp, sx, ex);
-            in = i >= sx && i <= ex;
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, in);
-        if (in) lx[nx + __popc(m & below)] = (short)ox;
-        nx += __popc(m);
-    }
-    for (int base = oy0; base <= oy1; base += 32) {
-        const int oy = base + lane;
-        bool in = false;
-        if (oy <= oy1) {
-            int sy, ey;
-            centre_range(oy * A.rs, A.H, A.hw, A.sp, sy, ey);
-            in = j >= sy && j <= ey;
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, in);
-        if (in) ly[ny + __popc(m & below)] = (short)oy;
-        ny += __popc(m);
-    }
-    __syncwarp();
-    const int npair = nx * ny;
-    const int kx0 = nx ? lane % nx : 0, ky0 = nx ? lane / nx : 0;
-    const int stx = nx ? 32 % nx : 0, sty = nx ? 32 / nx : 0;
-    const float3 ac = f3(A.alb, c), nc = f3(A.nrm, c);
-    float3 galb = make_float3(0.f, 0.f, 0.f), gnn = galb;
-    for (int X = 0; X < 2; ++X) {
-        const GBuf &B_ = A.bf[X];
-        const float3 fc = f3(B_.f, c);
-        const float vc = __ldg(B_.v + c), sc = __ldg(B_.s + c);
-        float beta[kBeta], gb[kBeta];
-#pragma unroll
-        for (int k = 0; k < kBeta; ++k) {
-            beta[k] = __ldg(B_.beta + ci * kBeta + k);
-            gb[k] = 0.f;
-        }
-        float3 gf = make_float3(0.f, 0.f, 0.f);
-        float gs = 0.f, gv = 0.f;
-        PairGrad g;
-        int kx = kx0, ky = ky0;
-        for (int k = lane; k < npair; k += 32) {
-            const int ox = lx[kx], oy = ly[ky];
-            kx += stx;
-            ky += sty;
-            if (kx >= nx) {
-                kx -= nx;
-                ++ky;
-            }
-            const size_t p = b * P + (size_t)(oy * A.rs) * A.W + ox * A.rs;
-            const size_t o = b * R + (size_t)oy * A.Wr + ox;
-            const float3 ap = f3(A.alb, p), np_ = f3(A.nrm, p);
-            const float3 da = make_float3(ap.x - ac.x, ap.y - ac.y, ap.z - ac.z);
-            const float3 dn = make_float3(np_.x - nc.x, np_.y - nc.y, np_.z - nc.z);
-            const float gN[3] = {__ldg(B_.gN + 3 * o), __ldg(B_.gN + 3 * o + 1), __ldg(B_.gN + 3 * o + 2)};
-            recon_pair<true>(f3(B_.f, p), fc, __ldg(B_.s + p), sc, __ldg(B_.v + p), vc, da, dn, beta, gN,
-                             __ldg(B_.gD + o), g);
-#pragma unroll
-            for (int q = 0; q < kBeta; ++q) gb[q] += g.gbeta[q];
-            gf.x -= g.gdf.x;
-            gf.y -= g.gdf.y;
-            gf.z -= g.gdf.z;
-            gs += g.gden;
-            gv += g.gV;
-            galb.x -= g.gda.x;
-            galb.y -= g.gda.y;
-            galb.z -= g.gda.z;
-            gnn.x -= g.gdn.x;
-            gnn.y -= g.gdn.y;
-            gnn.z -= g.gdn.z;
-        }
-#pragma unroll
-        for (int q = 0; q < kBeta; ++q) gb[q] = warp_sum(gb[q]);
-        gf = make_float3(warp_sum(gf.x), warp_sum(gf.y), warp_sum(gf.z));
-        gs = warp_sum(gs);
-        gv = warp_sum(gv);
-        if (lane == 0) {
-#pragma unroll
-            for (int q = 0; q < kBeta; ++q) B_.gbeta[ci * kBeta + q] = gb[q];
-            add3(B_.gf, c, gf);
-            B_.gs[c] += gs;
-            B_.gv[c] += gv;
-        }
-    }
-    galb = make_float3(warp_sum(galb.x), warp_sum(galb.y), warp_sum(galb.z));
-    gnn = make_float3(warp_sum(gnn.x), warp_sum(gnn.y), warp_sum(gnn.z));
-    if (lane == 0) {
-        add3(A.galb, c, galb);
-        add3(A.gn, c, gnn);
-    }
-}
-
 // One regression tap of one buffer: the forward quantities and the
 // derivatives of dL with respect to the tap's inputs, given u and beta.
 struct TapGrad {
@@ -636,6 +507,222 @@ CD_DEV void regression_tap(float3 ft, float3 fc, float3 yt, float st, float sc, 
     g.gy = make_float3(gyv[0], gyv[1], gyv[2]);
     g.gda = make_float3(gda[0], gda[1], gda[2]);
     g.gdn = make_float3(gdn[0], gdn[1], gdn[2]);
+}
+
+// ---------------------------------------------------------------------------
+// Pass 3: reconstruction backward, centre side (dL/dbeta and the centre's
+// own features).  Built like pass 4: a CTA owns 32 consecutive centres of one
+// centre row, warp 0 takes buffer A and warp 1 buffer B, one thread per
+// (centre, buffer).  The output rows whose centre range holds the centre row
+// stream through two shared-memory row slots (cp.async, double buffered); a
+// slot stores, per output pixel of the row segment the 32 centres' candidate
+// columns cover, six float4 groups: g0..g3 as the regression's window rows
+// (window_rows.cuh), g4 = (dL/dN_A.xyz, dL/dD_A), g5 = (dL/dN_B.xyz, dL/dD_B),
+// positions de-interleaved by the centre spacing sp / rs when rs divides sp
+// (32 lanes then read 32 consecutive float4s).  Each thread tests the
+// forward's range rule once per candidate column (bits; the rule's lower
+// end follows the reference's iDivUp, which is not monotone near the image's
+// top and left edges, so the set need not be an interval), and the CTA steps
+// through the span of its lanes' columns.
+// ---------------------------------------------------------------------------
+struct RconGeom {
+    int nc;     // candidate columns (and rows) per centre
+    int st;     // de-interleave stride: sp / rs when rs divides sp, else 1
+    int rw;     // row segment width in output pixels
+    int q;      // positions per de-interleaved run
+    int npos;   // positions per group (q * st)
+};
+
+__host__ __device__ inline RconGeom rcon_geom(int hw, int sp, int rs)
+{
+    RconGeom g;
+    g.nc = (2 * (hw + sp)) / rs + 2;
+    g.st = sp % rs == 0 ? sp / rs : 1;
+    g.rw = ((kRowCentres - 1) * sp) / rs + g.nc + 1;
+    g.q = (g.rw + g.st - 1) / g.st;
+    g.npos = g.q * g.st;
+    return g;
+}
+
+__host__ __device__ inline size_t recon_centre_smem(int hw, int sp, int rs)
+{
+    const RconGeom g = rcon_geom(hw, sp, rs);
+    return (size_t)2 * 6 * g.npos * sizeof(float4) + (size_t)2 * g.rw * sizeof(int) + 64 * sizeof(int) +
+           (size_t)kRowCentres * 6 * sizeof(float);
+}
+
+__host__ __device__ inline bool recon_centre_rows_ok(int hw, int sp, int rs)
+{
+    return rcon_geom(hw, sp, rs).nc <= 64 && recon_centre_smem(hw, sp, rs) <= 200 * 1024;
+}
+
+__global__ void __launch_bounds__(64, 7) recon_grad_centre_rows_kernel(GArgs A)
+{
+    extern __shared__ float4 sm4[];
+    const RconGeom g = rcon_geom(A.hw, A.sp, A.rs);
+    const int slot = 6 * g.npos;   // float4s per slot
+    int *pos_ox = reinterpret_cast<int *>(sm4 + 2 * slot);
+    int *pos_dst = pos_ox + g.rw;
+    int *rows = pos_dst + g.rw;
+    float *other = reinterpret_cast<float *>(rows + 64);   // buffer B's albedo / normal terms
+    __shared__ int nrows_s;
+    const int b = blockIdx.z;
+    const size_t P = (size_t)A.H * A.W, R = (size_t)A.Hr * A.Wr, C = (size_t)A.Hs * A.Ws;
+    const int i0 = blockIdx.x * kRowCentres, j = blockIdx.y;
+    const int X = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int seg = floordiv_g(i0 * A.sp - A.hw - A.sp, A.rs);   // output column of position 0
+
+    for (int p = threadIdx.x; p < g.rw; p += 64) {
+        pos_ox[p] = clampi(seg + p, 0, A.Wr - 1);
+        pos_dst[p] = (p % g.st) * g.q + p / g.st;
+    }
+    if (threadIdx.x == 0) {
+        // output rows whose centre range holds centre row j, in order
+        const int oy0 = floordiv_g(j * A.sp - A.hw - A.sp, A.rs);
+        int n = 0;
+        for (int t = 0; t < g.nc; ++t) {
+            const int oy = oy0 + t;
+            if (oy < 0 || oy >= A.Hr) continue;
+            int sy, ey;
+            centre_range(oy * A.rs, A.H, A.hw, A.sp, sy, ey);
+            if (j >= sy && j <= ey) rows[n++] = oy;
+        }
+        nrows_s = n;
+    }
+    __syncthreads();
+    const int nrows = nrows_s;
+
+    const float *imga = A.bf[0].f + 3 * P * b, *imgb = A.bf[1].f + 3 * P * b;
+    const float *alb = A.alb + 3 * P * b, *nrm = A.nrm + 3 * P * b;
+    const float *vara = A.bf[0].v + P * b, *varb = A.bf[1].v + P * b;
+    const float *sda = A.bf[0].s + P * b, *sdb = A.bf[1].s + P * b;
+    const float *gNa = A.bf[0].gN + 3 * R * b, *gNb = A.bf[1].gN + 3 * R * b;
+    const float *gDa = A.bf[0].gD + R * b, *gDb = A.bf[1].gD + R * b;
+    auto stage = [&](int k, int s) {
+        const int oy = rows[k];
+        float *base = reinterpret_cast<float *>(sm4 + s * slot);
+        const size_t prow = (size_t)(oy * A.rs) * A.W, orow = (size_t)oy * A.Wr;
+        for (int p = threadIdx.x; p < g.rw; p += 64) {
+            const int ox = pos_ox[p];
+            const size_t q = prow + (size_t)ox * A.rs, o = orow + ox;
+            float *d0 = base + 4 * pos_dst[p];
+            float *d1 = d0 + 4 * g.npos, *d2 = d0 + 8 * g.npos, *d3 = d0 + 12 * g.npos;
+            float *d4 = d0 + 16 * g.npos, *d5 = d0 + 20 * g.npos;
+            const float *a = imga + 3 * q, *c = imgb + 3 * q, *l = alb + 3 * q, *n = nrm + 3 * q;
+            cp_async4(d0, a); cp_async4(d0 + 1, a + 1); cp_async4(d0 + 2, a + 2); cp_async4(d0 + 3, vara + q);
+            cp_async4(d1, c); cp_async4(d1 + 1, c + 1); cp_async4(d1 + 2, c + 2); cp_async4(d1 + 3, varb + q);
+            cp_async4(d2, l); cp_async4(d2 + 1, l + 1); cp_async4(d2 + 2, l + 2); cp_async4(d2 + 3, sda + q);
+            cp_async4(d3, n); cp_async4(d3 + 1, n + 1); cp_async4(d3 + 2, n + 2); cp_async4(d3 + 3, sdb + q);
+            cp_async4(d4, gNa + 3 * o); cp_async4(d4 + 1, gNa + 3 * o + 1); cp_async4(d4 + 2, gNa + 3 * o + 2);
+            cp_async4(d4 + 3, gDa + o);
+            cp_async4(d5, gNb + 3 * o); cp_async4(d5 + 1, gNb + 3 * o + 1); cp_async4(d5 + 2, gNb + 3 * o + 2);
+            cp_async4(d5 + 3, gDb + o);
+        }
+    };
+    if (nrows > 0) stage(0, 0);
+    cp_async_commit();
+
+    // the thread's centre (clamped for lanes past the last centre), its
+    // candidate columns [cs, cs + nc) and which of them have it in range
+    const int i = min(i0 + lane, A.Ws - 1);
+    const size_t c = (size_t)(j * A.sp) * A.W + (size_t)i * A.sp;   // within the image
+    const size_t ci = b * C + (size_t)j * A.Ws + i;
+    const int cs = floordiv_g(i * A.sp - A.hw - A.sp, A.rs);
+    unsigned long long xb = 0ull;
+    for (int t = 0; t < g.nc; ++t) {
+        const int ox = cs + t;
+        if (ox < 0 || ox >= A.Wr) continue;
+        int sx, ex;
+        centre_range(ox * A.rs, A.W, A.hw, A.sp, sx, ex);
+        if (i >= sx && i <= ex) xb |= 1ull << t;
+    }
+    const bool valid = i0 + lane < A.Ws;
+    if (!valid) xb = 0ull;
+    const unsigned lo_any = __reduce_or_sync(0xffffffffu, (unsigned)xb);
+    const unsigned hi_any = __reduce_or_sync(0xffffffffu, (unsigned)(xb >> 32));
+    const unsigned long long any = ((unsigned long long)hi_any << 32) | lo_any;
+    const int t_lo = any ? __ffsll((long long)any) - 1 : 0, t_hi = any ? 63 - __clzll((long long)any) : -1;
+    const int loff = A.sp % A.rs == 0 ? lane : cs - seg;   // the lane's position offset, as de-interleaved
+
+    const float *betap = (X ? A.bf[1].beta : A.bf[0].beta) + ci * kBeta;
+    float beta[kBeta], gb[kBeta];
+#pragma unroll
+    for (int k = 0; k < kBeta; ++k) {
+        beta[k] = __ldg(betap + k);
+        gb[k] = 0.f;
+    }
+    const float3 fc = ld3(X ? imgb : imga, c), ac = ld3(alb, c), nc = ld3(nrm, c);
+    const float vc = __ldg((X ? varb : vara) + c), sc = __ldg((X ? sdb : sda) + c);
+    float3 gf = make_float3(0.f, 0.f, 0.f), galb = gf, gnn = gf;
+    float gs = 0.f, gv = 0.f;
+    PairGrad pg;
+    for (int k = 0; k < nrows; ++k) {
+        if (k + 1 < nrows) {
+            stage(k + 1, (k + 1) & 1);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const float4 *Pp = sm4 + (k & 1) * slot;
+        const float4 *Gf = Pp + X * g.npos, *Ga = Pp + 2 * g.npos, *Gn = Pp + 3 * g.npos;
+        const float4 *Gg = Pp + (4 + X) * g.npos;
+        int tm = t_lo % g.st, td = t_lo / g.st;
+        for (int t = t_lo; t <= t_hi; ++t) {
+            if ((xb >> t) & 1ull) {
+                const int o = tm * g.q + td + loff;
+                const float4 f4 = Gf[o], a4 = Ga[o], n4 = Gn[o], g4 = Gg[o];
+                const float spx = X ? n4.w : a4.w;   // sdA rides in g2.w, sdB in g3.w
+                const float gN[3] = {g4.x, g4.y, g4.z};
+                recon_pair<true>(make_float3(f4.x, f4.y, f4.z), fc, spx, sc, f4.w, vc,
+                                 make_float3(a4.x - ac.x, a4.y - ac.y, a4.z - ac.z),
+                                 make_float3(n4.x - nc.x, n4.y - nc.y, n4.z - nc.z), beta, gN, g4.w, pg);
+#pragma unroll
+                for (int q = 0; q < kBeta; ++q) gb[q] += pg.gbeta[q];
+                gf.x -= pg.gdf.x;
+                gf.y -= pg.gdf.y;
+                gf.z -= pg.gdf.z;
+                gs += pg.gden;
+                gv += pg.gV;
+                galb.x -= pg.gda.x;
+                galb.y -= pg.gda.y;
+                galb.z -= pg.gda.z;
+                gnn.x -= pg.gdn.x;
+                gnn.y -= pg.gdn.y;
+                gnn.z -= pg.gdn.z;
+            }
+            if (++tm == g.st) {
+                tm = 0;
+                ++td;
+            }
+        }
+        __syncthreads();
+    }
+    const size_t cp = b * P + c;
+    if (valid) {
+        const GBuf &B_ = X ? A.bf[1] : A.bf[0];
+#pragma unroll
+        for (int q = 0; q < kBeta; ++q) B_.gbeta[ci * kBeta + q] = gb[q];
+        add3(B_.gf, cp, gf);
+        B_.gs[cp] += gs;
+        B_.gv[cp] += gv;
+    }
+    if (X == 1) {
+        other[6 * lane] = galb.x;
+        other[6 * lane + 1] = galb.y;
+        other[6 * lane + 2] = galb.z;
+        other[6 * lane + 3] = gnn.x;
+        other[6 * lane + 4] = gnn.y;
+        other[6 * lane + 5] = gnn.z;
+    }
+    __syncthreads();
+    if (X == 0 && valid) {
+        add3(A.galb, cp, make_float3(galb.x + other[6 * lane], galb.y + other[6 * lane + 1],
+                                     galb.z + other[6 * lane + 2]));
+        add3(A.gn, cp, make_float3(gnn.x + other[6 * lane + 3], gnn.y + other[6 * lane + 4],
+                                   gnn.z + other[6 * lane + 5]));
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1220,7 +1307,6 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
     dim3 blk(32, 8);
     dim3 g_out((A.Wr + 31) / 32, (A.Hr + 7) / 8, B), g_cen((A.Ws + 31) / 32, (A.Hs + 7) / 8, B);
     dim3 g_px((W + 31) / 32, (H + 7) / 8, B);
-    dim3 g_warp((A.Hs * A.Ws + kCW - 1) / kCW, B);
     const size_t rg_smem = recon_grad_smem(A.hw, A.sp, A.rs);
     if (rg_smem <= 200 * 1024) {
         if ((e = cudaFuncSetAttribute(recon_grad_pixel_x2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1230,10 +1316,16 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
     } else {
         recon_grad_pixel_kernel<<<g_out, blk, 0, st>>>(A);
     }
-    if (recon_grad_centre_warp_ok(A.hw, A.sp, A.rs))
-        recon_grad_centre_warp_kernel<<<g_warp, 32 * kCW, 0, st>>>(A);
-    else
+    if (recon_centre_rows_ok(A.hw, A.sp, A.rs)) {
+        const size_t rc_smem = recon_centre_smem(A.hw, A.sp, A.rs);
+        if ((e = cudaFuncSetAttribute(recon_grad_centre_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)rc_smem)) != cudaSuccess)
+            return e;
+        recon_grad_centre_rows_kernel<<<dim3((A.Ws + kRowCentres - 1) / kRowCentres, A.Hs, B), 64, rc_smem, st>>>(
+            A);
+    } else {
         recon_grad_centre_kernel<<<g_cen, blk, 0, st>>>(A);
+    }
     const size_t gc_smem = grad_centre_smem(A.hw, A.sp);
     if ((e = cudaFuncSetAttribute(regression_grad_centre_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)gc_smem)) != cudaSuccess)
