@@ -45,17 +45,20 @@ constexpr int kP = 6, kBeta = 18, kL = 63;
 
 struct GBuf {
     const float *f, *y, *v, *s, *beta, *L;
-    float *u, *gbeta, *gN, *gD, *gf, *gy, *gs, *gv, *hn;
+    float *u, *gbeta, *gN, *gD, *gf, *gs, *gv, *hn;
+    float *gt, *gvs;   // the tap side's own planes: dL/d(image X), and its variance term
     const float *gout, *gvar;   // upstream dL/dout [R,3], dL/dvar [P] (nullable)
 };
 
 struct GArgs {
     GBuf bf[2];
     const float4 *state;        // forward recon: (out[3], D) per [buffer][output pixel]
+    float4 *crec;               // per centre: head and coefficient pairs, kRecG2 float4s
+    float4 *upair;              // per centre: u pairs by channel, 9 float4s
     const float *alb, *nrm;
-    float *galb, *gn;
+    float *galb, *gn, *galb_t, *gn_t;
     float *out_a, *out_b, *out_alb, *out_n;   // final gradients
-    int H, W, hw, sp, rs, Hs, Ws, Hr, Wr;
+    int B, H, W, hw, sp, rs, Hs, Ws, Hr, Wr;
 };
 
 CD_DEV float3 f3(const float *p, size_t i) { return ld3(p, i); }
@@ -227,72 +230,133 @@ CD_DEV x2::f2 dup2(float v) { return x2::pack(v, v); }
 CD_DEV x2::f2 rcp2(x2::f2 v) { return x2::pack(__fdividef(1.f, x2::lo(v)), __fdividef(1.f, x2::hi(v))); }
 CD_DEV x2::f2 expneg2(x2::f2 v) { return x2::pack(__expf(-x2::lo(v)), __expf(-x2::hi(v))); }
 
-// stage the coefficients (or u) of one channel k of centre ci as three
-// float4s of (A, B) pairs, rows 2m and 2m + 1
-CD_DEV void stage_rows(float4 *d, const float *pa, const float *pb, size_t ci, int k)
+// A tile's centres [cx_lo, cx_lo + ncx) x [cy_lo, cy_lo + ncy) of image b.
+struct CentreTile {
+    int b, x0, y0, cx_lo, cy_lo, ncx, ncy;
+};
+
+CD_DEV void cp_async16(void *dst, const void *src)
 {
-#pragma unroll
-    for (int m = 0; m < 3; ++m)
-        d[m] = make_float4(__ldg(pa + ci * kBeta + 6 * m + k), __ldg(pb + ci * kBeta + 6 * m + k),
-                           __ldg(pa + ci * kBeta + 6 * m + 3 + k), __ldg(pb + ci * kBeta + 6 * m + 3 + k));
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
 }
 
-// the per-centre head of a record: features, sd, variance of both buffers,
-// albedo and normal
-CD_DEV void stage_head(float4 *r, const GArgs &A, size_t c)
+// The centre records of the pixel- and tap-side passes, built once per
+// backward in their shared-memory layout (kRecG2 float4s per centre: the
+// head, then the coefficient pairs of channel k, rows 2m and 2m + 1, at
+// 4 + 3k + m), so that a tile stages them with 16-byte copies.
+__global__ void __launch_bounds__(256) centre_records_kernel(GArgs A)
 {
-    const float3 fa = f3(A.bf[0].f, c), fb = f3(A.bf[1].f, c), al = f3(A.alb, c), nr = f3(A.nrm, c);
-    r[0] = make_float4(fa.x, fb.x, fa.y, fb.y);
-    r[1] = make_float4(fa.z, fb.z, __ldg(A.bf[0].s + c), __ldg(A.bf[1].s + c));
-    r[2] = make_float4(__ldg(A.bf[0].v + c), __ldg(A.bf[1].v + c), al.x, al.y);
-    r[3] = make_float4(al.z, nr.x, nr.y, nr.z);
+    const size_t C = (size_t)A.B * A.Hs * A.Ws, P = (size_t)A.H * A.W;
+    const size_t idx = (size_t)blockIdx.x * 256 + threadIdx.x;
+    if (idx >= C * kRecG2) return;
+    const size_t ci = idx / kRecG2;
+    const int j = (int)(idx - ci * kRecG2);
+    const int per = A.Hs * A.Ws, b = (int)(ci / per), r = (int)(ci - (size_t)b * per);
+    const int iy = r / A.Ws, ix = r - iy * A.Ws;
+    const size_t c = b * P + (size_t)(iy * A.sp) * A.W + ix * A.sp;
+    float4 v;
+    if (j == 0) {
+        v = make_float4(__ldg(A.bf[0].f + 3 * c), __ldg(A.bf[1].f + 3 * c), __ldg(A.bf[0].f + 3 * c + 1),
+                        __ldg(A.bf[1].f + 3 * c + 1));
+    } else if (j == 1) {
+        v = make_float4(__ldg(A.bf[0].f + 3 * c + 2), __ldg(A.bf[1].f + 3 * c + 2), __ldg(A.bf[0].s + c),
+                        __ldg(A.bf[1].s + c));
+    } else if (j == 2) {
+        v = make_float4(__ldg(A.bf[0].v + c), __ldg(A.bf[1].v + c), __ldg(A.alb + 3 * c), __ldg(A.alb + 3 * c + 1));
+    } else if (j == 3) {
+        v = make_float4(__ldg(A.alb + 3 * c + 2), __ldg(A.nrm + 3 * c), __ldg(A.nrm + 3 * c + 1),
+                        __ldg(A.nrm + 3 * c + 2));
+    } else {
+        const int k = (j - 4) / 3, m = (j - 4) - 3 * k;
+        const float *pa = A.bf[0].beta + ci * kBeta, *pb = A.bf[1].beta + ci * kBeta;
+        v = make_float4(__ldg(pa + 6 * m + k), __ldg(pb + 6 * m + k), __ldg(pa + 6 * m + 3 + k),
+                        __ldg(pb + 6 * m + 3 + k));
+    }
+    A.crec[idx] = v;
 }
 
-__global__ void __launch_bounds__(256) recon_grad_pixel_x2_kernel(GArgs A)
+// Copy (cp.async, 16 bytes each) the NQ float4s per centre of src for a
+// tile's centres into rec, record n at rec + n * stride + off.
+template <int NQ>
+CD_DEV void stage_records(float4 *rec, int stride, int off, const float4 *src, const GArgs &A, const CentreTile &T,
+                          int tid)
+{
+    const size_t C = (size_t)A.Hs * A.Ws;
+    const int nrec = T.ncx * T.ncy;
+    const float rncx = 1.f / (float)T.ncx;
+    for (int e = tid; e < nrec * NQ; e += 256) {
+        const int n = e / NQ, j = e - n * NQ;
+        const int ry = (int)(((float)n + 0.5f) * rncx), rx = n - ry * T.ncx;
+        const size_t ci = T.b * C + (size_t)(T.cy_lo + ry) * A.Ws + T.cx_lo + rx;
+        cp_async16(rec + (size_t)n * stride + off + j, src + ci * NQ + j);
+    }
+}
+
+CD_DEV CentreTile pixel_tile(const GArgs &A, int t, int tx, int ty)
+{
+    CentreTile T;
+    T.b = t / (tx * ty);
+    const int r = t - T.b * tx * ty, by = r / tx, bx = r - by * tx;
+    T.x0 = bx * 32;
+    T.y0 = by * 8;
+    const int ox1 = min(T.x0 + 31, A.Wr - 1), oy1 = min(T.y0 + 7, A.Hr - 1);
+    T.cx_lo = max(0, floordiv_g(T.x0 * A.rs - A.hw, A.sp));
+    T.cy_lo = max(0, floordiv_g(T.y0 * A.rs - A.hw, A.sp));
+    T.ncx = min(A.Ws - 1, (ox1 * A.rs + A.hw) / A.sp) - T.cx_lo + 1;
+    T.ncy = min(A.Hs - 1, (oy1 * A.rs + A.hw) / A.sp) - T.cy_lo + 1;
+    return T;
+}
+
+// The per-pixel inputs of the pixel side, loaded one tile ahead.
+struct PixIn2 {
+    float3 ap, np, fa, fb, goa, gob;
+    float sa, sb, va, vb;
+    float4 sta, stb;
+};
+
+CD_DEV void load_pixel_x2(const GArgs &A, const CentreTile &T, int warp, int lane, PixIn2 &I)
+{
+    const size_t P = (size_t)A.H * A.W, R = (size_t)A.Hr * A.Wr;
+    const int ox = T.x0 + 4 * warp + (lane & 3), oy = T.y0 + (lane >> 2);
+    if (ox >= A.Wr || oy >= A.Hr) return;
+    const size_t p = T.b * P + (size_t)(oy * A.rs) * A.W + ox * A.rs, o = T.b * R + (size_t)oy * A.Wr + ox;
+    I.ap = f3(A.alb, p);
+    I.np = f3(A.nrm, p);
+    I.fa = f3(A.bf[0].f, p);
+    I.fb = f3(A.bf[1].f, p);
+    I.sa = __ldg(A.bf[0].s + p);
+    I.sb = __ldg(A.bf[1].s + p);
+    I.va = __ldg(A.bf[0].v + p);
+    I.vb = __ldg(A.bf[1].v + p);
+    I.sta = A.state[o];
+    I.stb = A.state[(size_t)A.B * R + o];
+    I.goa = f3(A.bf[0].gout, o);
+    I.gob = f3(A.bf[1].gout, o);
+}
+
+// the pixel side of one output pixel of tile T (warp covers 4 x 8 pixels)
+CD_DEV void recon_grad_pixel_x2(const GArgs &A, const CentreTile &T, const float4 *rec4, int warp, int lane,
+                                const PixIn2 &I)
 {
     using namespace x2;
-    extern __shared__ float4 rec4[];
-    const int b = blockIdx.z;
-    const size_t P = (size_t)A.H * A.W, R = (size_t)A.Hr * A.Wr, C = (size_t)A.Hs * A.Ws;
-    const int ox0 = blockIdx.x * 32, oy0 = blockIdx.y * 8;
-    const int ox1 = min(ox0 + 31, A.Wr - 1), oy1 = min(oy0 + 7, A.Hr - 1);
-    const int cx_lo = max(0, floordiv_g(ox0 * A.rs - A.hw, A.sp)), cx_hi = min(A.Ws - 1, (ox1 * A.rs + A.hw) / A.sp);
-    const int cy_lo = max(0, floordiv_g(oy0 * A.rs - A.hw, A.sp)), cy_hi = min(A.Hs - 1, (oy1 * A.rs + A.hw) / A.sp);
-    const int ncx = cx_hi - cx_lo + 1, ncy = cy_hi - cy_lo + 1;
-    const int tid = threadIdx.x;
-    for (int e = tid; e < ncx * ncy * 4; e += 256) {
-        const int n = e >> 2, part = e & 3;
-        const int iy = cy_lo + n / ncx, ix = cx_lo + n % ncx;
-        const size_t c = b * P + (size_t)(iy * A.sp) * A.W + ix * A.sp;
-        const size_t ci = b * C + (size_t)iy * A.Ws + ix;
-        float4 *r = rec4 + (size_t)n * kRecG2;
-        if (part == 0)
-            stage_head(r, A, c);
-        else
-            stage_rows(r + 4 + 3 * (part - 1), A.bf[0].beta, A.bf[1].beta, ci, part - 1);
-    }
-    __syncthreads();
-
-    const int warp = tid >> 5, lane = tid & 31;
-    const int ox = ox0 + 4 * warp + (lane & 3), oy = oy0 + (lane >> 2);
+    const size_t P = (size_t)A.H * A.W, R = (size_t)A.Hr * A.Wr;
+    const int ox = T.x0 + 4 * warp + (lane & 3), oy = T.y0 + (lane >> 2);
     if (ox >= A.Wr || oy >= A.Hr) return;
     const int px = ox * A.rs, py = oy * A.rs;
-    const size_t p = b * P + (size_t)py * A.W + px, o = b * R + (size_t)oy * A.Wr + ox;
+    const size_t p = T.b * P + (size_t)py * A.W + px, o = T.b * R + (size_t)oy * A.Wr + ox;
     int sx, ex, sy, ey;
     centre_range(px, A.W, A.hw, A.sp, sx, ex);
     centre_range(py, A.H, A.hw, A.sp, sy, ey);
-    const float3 ap = f3(A.alb, p), np_ = f3(A.nrm, p);
-    const float3 fpa = f3(A.bf[0].f, p), fpb = f3(A.bf[1].f, p);
-    const f2 fp0 = pack(fpa.x, fpb.x), fp1 = pack(fpa.y, fpb.y), fp2 = pack(fpa.z, fpb.z);
-    const f2 spp = pack(__ldg(A.bf[0].s + p), __ldg(A.bf[1].s + p));
-    const f2 vpp = pack(__ldg(A.bf[0].v + p), __ldg(A.bf[1].v + p));
+    const float3 ap = I.ap, np_ = I.np;
+    const f2 fp0 = pack(I.fa.x, I.fb.x), fp1 = pack(I.fa.y, I.fb.y), fp2 = pack(I.fa.z, I.fb.z);
+    const f2 spp = pack(I.sa, I.sb), vpp = pack(I.va, I.vb);
     // dL/dN and dL/dD of the pixel, both buffers
     f2 gN0, gN1, gN2, gD;
     {
         float na[3], nb[3], da, db;
-        const size_t RB = (size_t)gridDim.z * R;
-        recon_upstream(A.state[o], f3(A.bf[0].gout, o), na, da);
-        recon_upstream(A.state[RB + o], f3(A.bf[1].gout, o), nb, db);
+        recon_upstream(I.sta, I.goa, na, da);
+        recon_upstream(I.stb, I.gob, nb, db);
         for (int X = 0; X < 2; ++X) {
             const float *g = X ? nb : na;
             A.bf[X].gN[3 * o] = g[0];
@@ -311,7 +375,7 @@ __global__ void __launch_bounds__(256) recon_grad_pixel_x2_kernel(GArgs A)
     f2 ga0 = 0ull, ga1 = 0ull, ga2 = 0ull, gn0 = 0ull, gn1 = 0ull, gn2 = 0ull;
     for (int iy = sy; iy <= ey; ++iy)
         for (int ix = sx; ix <= ex; ++ix) {
-            const float4 *R4 = rec4 + (size_t)((iy - cy_lo) * ncx + (ix - cx_lo)) * kRecG2;
+            const float4 *R4 = rec4 + (size_t)((iy - T.cy_lo) * T.ncx + (ix - T.cx_lo)) * kRecG2;
             const ulonglong2 *RR = reinterpret_cast<const ulonglong2 *>(R4);
             const ulonglong2 h0 = RR[0], h1 = RR[1];
             const float4 q2 = R4[2], q3 = R4[3];
@@ -353,13 +417,44 @@ __global__ void __launch_bounds__(256) recon_grad_pixel_x2_kernel(GArgs A)
         }
     for (int X = 0; X < 2; ++X) {
         const GBuf &B_ = A.bf[X];
+        // the first writer of these planes (zeroed before the passes): a
+        // store, without the read of an accumulate
         const float x0 = X ? hi(gf0) : lo(gf0), x1 = X ? hi(gf1) : lo(gf1), x2_ = X ? hi(gf2) : lo(gf2);
-        add3(B_.gf, p, make_float3(x0, x1, x2_));
-        B_.gs[p] += X ? hi(gs) : lo(gs);
-        B_.gv[p] += X ? hi(gv) : lo(gv);
+        st3(B_.gf, p, make_float3(x0, x1, x2_));
+        B_.gs[p] = X ? hi(gs) : lo(gs);
+        B_.gv[p] = X ? hi(gv) : lo(gv);
     }
-    add3(A.galb, p, make_float3(lo(ga0) + hi(ga0), lo(ga1) + hi(ga1), lo(ga2) + hi(ga2)));
-    add3(A.gn, p, make_float3(lo(gn0) + hi(gn0), lo(gn1) + hi(gn1), lo(gn2) + hi(gn2)));
+    st3(A.galb, p, make_float3(lo(ga0) + hi(ga0), lo(ga1) + hi(ga1), lo(ga2) + hi(ga2)));
+    st3(A.gn, p, make_float3(lo(gn0) + hi(gn0), lo(gn1) + hi(gn1), lo(gn2) + hi(gn2)));
+}
+
+// Persistent: a CTA takes tiles t, t + grid, ...; the next tile's records are
+// copied (cp.async) into the second buffer while the current tile computes.
+__global__ void __launch_bounds__(256, 2) recon_grad_pixel_x2_kernel(GArgs A, int tx, int ty, int ntiles, int cap)
+{
+    extern __shared__ float4 rec4[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, G = gridDim.x;
+    auto stage = [&](int t, int s) {
+        const CentreTile T = pixel_tile(A, t, tx, ty);
+        stage_records<kRecG2>(rec4 + (size_t)s * cap, kRecG2, 0, A.crec, A, T, threadIdx.x);
+    };
+    PixIn2 I;
+    if ((int)blockIdx.x < ntiles) {
+        stage(blockIdx.x, 0);
+        load_pixel_x2(A, pixel_tile(A, blockIdx.x, tx, ty), warp, lane, I);
+    }
+    cp_async_commit();
+    int it = 0;
+    for (int t = blockIdx.x; t < ntiles; t += G, ++it) {
+        if (t + G < ntiles) stage(t + G, (it + 1) & 1);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        recon_grad_pixel_x2(A, pixel_tile(A, t, tx, ty), rec4 + (size_t)(it & 1) * cap, warp, lane, I);
+        // the next tile's pixel inputs, in flight across the barrier and the staging
+        if (t + G < ntiles) load_pixel_x2(A, pixel_tile(A, t + G, tx, ty), warp, lane, I);
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -803,8 +898,14 @@ __global__ void __launch_bounds__(64, 8) regression_grad_centre_kernel(GArgs A)
     const bool valid = i0 + lane < A.Ws;
     if (valid) {
         float *ug = (X ? A.bf[1].u : A.bf[0].u) + ci * kBeta;
+        float *up = reinterpret_cast<float *>(A.upair + ci * 9);   // pairs: channel k, row r at 12k + 4(r/2) + 2(r%2)
 #pragma unroll
-        for (int k = 0; k < kBeta; ++k) ug[k] = u[k];
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int r = 0; r < kP; ++r) {
+                ug[r * 3 + k] = u[r * 3 + k];
+                up[12 * k + 4 * (r >> 1) + 2 * (r & 1) + X] = u[r * 3 + k];
+            }
     }
     const float3 fc = ld3(X ? imgb : imga, c), ac = ld3(alb, c), nc = ld3(nrm, c);
     const float vc = __ldg((X ? varb : vara) + c), sc = __ldg((X ? sdb : sda) + c);
@@ -900,7 +1001,8 @@ __global__ void __launch_bounds__(256) regression_grad_tap_kernel(GArgs A)
     const int ntx = tap_positions(qx, A.W, A.hw, (A.Ws - 1) * A.sp, txs);
     const int nty = tap_positions(qy, A.H, A.hw, (A.Hs - 1) * A.sp, tys);
     const float3 at = f3(A.alb, q), nt = f3(A.nrm, q);
-    float3 galb = make_float3(0.f, 0.f, 0.f), gnn = galb;
+    float3 galb = make_float3(0.f, 0.f, 0.f), gnn = galb, gfX[2], gyX[2];
+    float gvsX[2];
     for (int X = 0; X < 2; ++X) {
         const GBuf &B_ = A.bf[X];
         const float3 ft = f3(B_.f, q), yt = f3(B_.y, q);
@@ -945,13 +1047,17 @@ __global__ void __launch_bounds__(256) regression_grad_tap_kernel(GArgs A)
                 }
             }
         }
-        add3(B_.gf, q, gf);
-        st3(B_.gy, q, gy);   // the only writer of gy
-        B_.gs[q] += gs;
-        B_.gv[q] += gv;
+        gfX[X] = gf;
+        gyX[X] = gy;
+        gvsX[X] = gv + (st > 0.f ? gs / (2.f * st) : 0.f);
     }
-    add3(A.galb, q, galb);
-    add3(A.gn, q, gnn);
+    // the only writer of its planes: stores
+    st3(A.bf[0].gt, q, make_float3(gfX[0].x + gyX[1].x, gfX[0].y + gyX[1].y, gfX[0].z + gyX[1].z));
+    st3(A.bf[1].gt, q, make_float3(gfX[1].x + gyX[0].x, gfX[1].y + gyX[0].y, gfX[1].z + gyX[0].z));
+    A.bf[0].gvs[q] = gvsX[0];
+    A.bf[1].gvs[q] = gvsX[1];
+    st3(A.galb_t, q, galb);
+    st3(A.gn_t, q, gnn);
 }
 
 // Pass 5 with the tile's centres staged in shared memory and both buffers
@@ -962,10 +1068,10 @@ __global__ void __launch_bounds__(256) regression_grad_tap_kernel(GArgs A)
 // [lo, hi]; a record of kRecT2 float4s per centre holds (pairs (A, B)
 // unless noted):
 //   0  f.x f.y   1  f.z s   2  v | alb.x alb.y (scalars)   3  alb.z nrm.xyz (scalars)
-//   4 + 3k + m   u of channel k, rows 2m and 2m + 1
-//   13 + 3k + m  coefficients of channel k, rows 2m and 2m + 1
-// A warp covers 4 x 8 pixels of the tile (shared-memory broadcast, as in
-// pass 2).  Same pairs and order as regression_grad_tap_kernel.
+//   4 + 3k + m   coefficients of channel k, rows 2m and 2m + 1
+//   13 + 3k + m  u of channel k, rows 2m and 2m + 1
+// (the first 13 the pixel side's record).  A warp covers 4 x 8 pixels of the
+// tile (shared-memory broadcast, as in pass 2).  Same pairs and order as regression_grad_tap_kernel.
 constexpr int kRecT2 = 22;
 
 __host__ __device__ inline size_t tap_grad_smem(int hw, int sp)
@@ -974,47 +1080,59 @@ __host__ __device__ inline size_t tap_grad_smem(int hw, int sp)
     return (size_t)ncx * ncy * kRecT2 * sizeof(float4);
 }
 
-__global__ void __launch_bounds__(256, 2) regression_grad_tap_x2_kernel(GArgs A)
+CD_DEV CentreTile tap_tile(const GArgs &A, int t, int tx, int ty)
+{
+    CentreTile T;
+    T.b = t / (tx * ty);
+    const int r = t - T.b * tx * ty, by = r / tx, bx = r - by * tx;
+    T.x0 = bx * 32;
+    T.y0 = by * 8;
+    const int x1 = min(T.x0 + 31, A.W - 1), y1 = min(T.y0 + 7, A.H - 1);
+    T.cx_lo = T.x0 - A.hw > 0 ? (T.x0 - A.hw + A.sp - 1) / A.sp : 0;
+    T.cy_lo = T.y0 - A.hw > 0 ? (T.y0 - A.hw + A.sp - 1) / A.sp : 0;
+    T.ncx = min(A.Ws - 1, (x1 + A.hw) / A.sp) - T.cx_lo + 1;
+    T.ncy = min(A.Hs - 1, (y1 + A.hw) / A.sp) - T.cy_lo + 1;
+    return T;
+}
+
+// The per-pixel inputs of the tap side, loaded one tile ahead.
+struct PixIn5 {
+    float3 at, nt, fa, fb;
+    float sa, sb, va, vb;
+};
+
+CD_DEV void load_pixel_tap(const GArgs &A, const CentreTile &T, int warp, int lane, PixIn5 &I)
+{
+    const size_t P = (size_t)A.H * A.W;
+    const int qx = T.x0 + 4 * warp + (lane & 3), qy = T.y0 + (lane >> 2);
+    if (qx >= A.W || qy >= A.H) return;
+    const size_t q = T.b * P + (size_t)qy * A.W + qx;
+    I.at = f3(A.alb, q);
+    I.nt = f3(A.nrm, q);
+    I.fa = f3(A.bf[0].f, q);
+    I.fb = f3(A.bf[1].f, q);
+    I.sa = __ldg(A.bf[0].s + q);
+    I.sb = __ldg(A.bf[1].s + q);
+    I.va = __ldg(A.bf[0].v + q);
+    I.vb = __ldg(A.bf[1].v + q);
+}
+
+// the tap side of one pixel of tile T (warp covers 4 x 8 pixels)
+CD_DEV void regression_grad_tap_x2(const GArgs &A, const CentreTile &T, const float4 *rec4, int warp, int lane,
+                                   const PixIn5 &I)
 {
     using namespace x2;
-    extern __shared__ float4 rec4[];
-    const int b = blockIdx.z;
-    const size_t P = (size_t)A.H * A.W, C = (size_t)A.Hs * A.Ws;
-    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
-    const int x1 = min(x0 + 31, A.W - 1), y1 = min(y0 + 7, A.H - 1);
-    const int cx_lo = x0 - A.hw > 0 ? (x0 - A.hw + A.sp - 1) / A.sp : 0;
-    const int cy_lo = y0 - A.hw > 0 ? (y0 - A.hw + A.sp - 1) / A.sp : 0;
-    const int cx_hi = min(A.Ws - 1, (x1 + A.hw) / A.sp), cy_hi = min(A.Hs - 1, (y1 + A.hw) / A.sp);
-    const int ncx = cx_hi - cx_lo + 1, ncy = cy_hi - cy_lo + 1;
-    const int tid = threadIdx.x;
-    for (int e = tid; e < ncx * ncy * 7; e += 256) {
-        const int n = e / 7, part = e - 7 * n;
-        const int iy = cy_lo + n / ncx, ix = cx_lo + n % ncx;
-        const size_t c = b * P + (size_t)(iy * A.sp) * A.W + ix * A.sp;
-        const size_t ci = b * C + (size_t)iy * A.Ws + ix;
-        float4 *r = rec4 + (size_t)n * kRecT2;
-        if (part == 0)
-            stage_head(r, A, c);
-        else if (part <= 3)
-            stage_rows(r + 4 + 3 * (part - 1), A.bf[0].u, A.bf[1].u, ci, part - 1);
-        else
-            stage_rows(r + 13 + 3 * (part - 4), A.bf[0].beta, A.bf[1].beta, ci, part - 4);
-    }
-    __syncthreads();
-
-    const int warp = tid >> 5, lane = tid & 31;
-    const int qx = x0 + 4 * warp + (lane & 3), qy = y0 + (lane >> 2);
+    const size_t P = (size_t)A.H * A.W;
+    const int qx = T.x0 + 4 * warp + (lane & 3), qy = T.y0 + (lane >> 2);
     if (qx >= A.W || qy >= A.H) return;
-    const size_t q = b * P + (size_t)qy * A.W + qx;
+    const size_t q = T.b * P + (size_t)qy * A.W + qx;
     int txs[3], tys[3];
     const int ntx = tap_positions(qx, A.W, A.hw, (A.Ws - 1) * A.sp, txs);
     const int nty = tap_positions(qy, A.H, A.hw, (A.Hs - 1) * A.sp, tys);
-    const float3 at = f3(A.alb, q), nt = f3(A.nrm, q);
-    const float3 fqa = f3(A.bf[0].f, q), fqb = f3(A.bf[1].f, q);
+    const float3 at = I.at, nt = I.nt, fqa = I.fa, fqb = I.fb;
     const f2 ft[3] = {pack(fqa.x, fqb.x), pack(fqa.y, fqb.y), pack(fqa.z, fqb.z)};
     const f2 yt[3] = {pack(fqb.x, fqa.x), pack(fqb.y, fqa.y), pack(fqb.z, fqa.z)};   // y of A is imgb
-    const f2 stt = pack(__ldg(A.bf[0].s + q), __ldg(A.bf[1].s + q));
-    const f2 vtt = pack(__ldg(A.bf[0].v + q), __ldg(A.bf[1].v + q));
+    const f2 stt = pack(I.sa, I.sb), vtt = pack(I.va, I.vb);
     const f2 k1e2 = pack(1e-2f, 1e-2f), k1e4 = pack(1e-4f, 1e-4f), k1e7 = pack(1e-7f, 1e-7f);
     const f2 two = pack(2.f, 2.f);
     f2 gf[3] = {0ull, 0ull, 0ull}, gy[3] = {0ull, 0ull, 0ull}, ga[3] = {0ull, 0ull, 0ull};
@@ -1031,7 +1149,7 @@ __global__ void __launch_bounds__(256, 2) regression_grad_tap_x2_kernel(GArgs A)
                 const int i1 = min(A.Ws - 1, (tx + A.hw) >= 0 ? (tx + A.hw) / A.sp : -1);
                 for (int i = i0; i <= i1; ++i) {
                     if (abs(i * A.sp - tx) > A.hw) continue;
-                    const float4 *R4 = rec4 + (size_t)((j - cy_lo) * ncx + (i - cx_lo)) * kRecT2;
+                    const float4 *R4 = rec4 + (size_t)((j - T.cy_lo) * T.ncx + (i - T.cx_lo)) * kRecT2;
                     const ulonglong2 *RR = reinterpret_cast<const ulonglong2 *>(R4);
                     const ulonglong2 h0 = RR[0], h1 = RR[1];
                     const float4 q2 = R4[2], q3 = R4[3];
@@ -1047,8 +1165,8 @@ __global__ void __launch_bounds__(256, 2) regression_grad_tap_x2_kernel(GArgs A)
                     f2 tn0 = 0ull, tn1 = 0ull, tn2 = 0ull;
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
-                        const ulonglong2 u01 = RR[4 + 3 * k], u23 = RR[5 + 3 * k], u45 = RR[6 + 3 * k];
-                        const ulonglong2 b01 = RR[13 + 3 * k], b23 = RR[14 + 3 * k], b45 = RR[15 + 3 * k];
+                        const ulonglong2 b01 = RR[4 + 3 * k], b23 = RR[5 + 3 * k], b45 = RR[6 + 3 * k];
+                        const ulonglong2 u01 = RR[13 + 3 * k], u23 = RR[14 + 3 * k], u45 = RR[15 + 3 * k];
                         d1[k] = mul2(df[k], rden);
                         const f2 a = fma2(u45.y, dn2, fma2(u45.x, dn1, fma2(u23.y, dn0,
                                          fma2(u23.x, da[k], fma2(u01.y, d1[k], u01.x)))));
@@ -1083,16 +1201,43 @@ __global__ void __launch_bounds__(256, 2) regression_grad_tap_x2_kernel(GArgs A)
             }
         }
     }
-    for (int X = 0; X < 2; ++X) {
-        const GBuf &B_ = A.bf[X];
-        auto pick = [X](f2 v) { return X ? hi(v) : lo(v); };
-        add3(B_.gf, q, make_float3(pick(gf[0]), pick(gf[1]), pick(gf[2])));
-        st3(B_.gy, q, make_float3(pick(gy[0]), pick(gy[1]), pick(gy[2])));   // the only writer of gy
-        B_.gs[q] += pick(gs);
-        B_.gv[q] += pick(gv);
+    // the only writer of its planes: stores (image A's features are buffer
+    // A's and buffer B's target, and the other way round)
+    st3(A.bf[0].gt, q, make_float3(lo(gf[0]) + hi(gy[0]), lo(gf[1]) + hi(gy[1]), lo(gf[2]) + hi(gy[2])));
+    st3(A.bf[1].gt, q, make_float3(hi(gf[0]) + lo(gy[0]), hi(gf[1]) + lo(gy[1]), hi(gf[2]) + lo(gy[2])));
+    A.bf[0].gvs[q] = lo(gv) + (I.sa > 0.f ? lo(gs) / (2.f * I.sa) : 0.f);
+    A.bf[1].gvs[q] = hi(gv) + (I.sb > 0.f ? hi(gs) / (2.f * I.sb) : 0.f);
+    st3(A.galb_t, q, make_float3(lo(ga[0]) + hi(ga[0]), lo(ga[1]) + hi(ga[1]), lo(ga[2]) + hi(ga[2])));
+    st3(A.gn_t, q, make_float3(lo(gn0) + hi(gn0), lo(gn1) + hi(gn1), lo(gn2) + hi(gn2)));
+}
+
+// Persistent, the next tile's records copied while the current one computes
+// (as recon_grad_pixel_x2_kernel).
+__global__ void __launch_bounds__(256, 2) regression_grad_tap_x2_kernel(GArgs A, int tx, int ty, int ntiles, int cap)
+{
+    extern __shared__ float4 rec4[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, G = gridDim.x;
+    auto stage = [&](int t, int s) {
+        const CentreTile T = tap_tile(A, t, tx, ty);
+        stage_records<kRecG2>(rec4 + (size_t)s * cap, kRecT2, 0, A.crec, A, T, threadIdx.x);
+        stage_records<9>(rec4 + (size_t)s * cap, kRecT2, kRecG2, A.upair, A, T, threadIdx.x);
+    };
+    PixIn5 I;
+    if ((int)blockIdx.x < ntiles) {
+        stage(blockIdx.x, 0);
+        load_pixel_tap(A, tap_tile(A, blockIdx.x, tx, ty), warp, lane, I);
     }
-    add3(A.galb, q, make_float3(lo(ga[0]) + hi(ga[0]), lo(ga[1]) + hi(ga[1]), lo(ga[2]) + hi(ga[2])));
-    add3(A.gn, q, make_float3(lo(gn0) + hi(gn0), lo(gn1) + hi(gn1), lo(gn2) + hi(gn2)));
+    cp_async_commit();
+    int it = 0;
+    for (int t = blockIdx.x; t < ntiles; t += G, ++it) {
+        if (t + G < ntiles) stage(t + G, (it + 1) & 1);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        regression_grad_tap_x2(A, tap_tile(A, t, tx, ty), rec4 + (size_t)(it & 1) * cap, warp, lane, I);
+        if (t + G < ntiles) load_pixel_tap(A, tap_tile(A, t + G, tx, ty), warp, lane, I);
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1112,7 +1257,7 @@ __global__ void __launch_bounds__(256) variance_grad_kernel(GArgs A)
     for (int X = 0; X < 2; ++X) {
         const GBuf &B_ = A.bf[X];
         const float s = __ldg(B_.s + p);
-        float gv = B_.gv[p] + (s > 0.f ? B_.gs[p] / (2.f * s) : 0.f);
+        float gv = B_.gv[p] + (s > 0.f ? B_.gs[p] / (2.f * s) : 0.f) + B_.gvs[p];
         if (B_.gvar) gv += __ldg(B_.gvar + p);
         const int sx = max(0, x - 1), ex = min(A.W - 1, x + 1), sy = max(0, y - 1), ey = min(A.H - 1, y + 1);
         float m[3] = {0.f, 0.f, 0.f};
@@ -1137,8 +1282,8 @@ __global__ void __launch_bounds__(256) variance_grad_kernel(GArgs A)
     }
 }
 
-// Pass 6b: neighbours' variance terms and the assembly:
-// dL/dimga = gf(A) + gy(B), dL/dimgb = gf(B) + gy(A).
+// Pass 6b: neighbours' variance terms and the assembly with the tap side's
+// planes: dL/dimga = gf(A) + gt(A), dL/dimgb = gf(B) + gt(B).
 __global__ void __launch_bounds__(256) assemble_grad_kernel(GArgs A)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -1160,11 +1305,12 @@ __global__ void __launch_bounds__(256) assemble_grad_kernel(GArgs A)
             }
         g[X] = v;
     }
-    const float3 ya = f3(A.bf[0].gy, p), yb = f3(A.bf[1].gy, p);
-    st3(A.out_a, p, make_float3(g[0].x + yb.x, g[0].y + yb.y, g[0].z + yb.z));
-    st3(A.out_b, p, make_float3(g[1].x + ya.x, g[1].y + ya.y, g[1].z + ya.z));
-    st3(A.out_alb, p, f3(A.galb, p));
-    st3(A.out_n, p, f3(A.gn, p));
+    const float3 ta = f3(A.bf[0].gt, p), tb = f3(A.bf[1].gt, p);
+    const float3 al = f3(A.galb, p), alt = f3(A.galb_t, p), nr = f3(A.gn, p), nrt = f3(A.gn_t, p);
+    st3(A.out_a, p, make_float3(g[0].x + ta.x, g[0].y + ta.y, g[0].z + ta.z));
+    st3(A.out_b, p, make_float3(g[1].x + tb.x, g[1].y + tb.y, g[1].z + tb.z));
+    st3(A.out_alb, p, make_float3(al.x + alt.x, al.y + alt.y, al.z + alt.z));
+    st3(A.out_n, p, make_float3(nr.x + nrt.x, nr.y + nrt.y, nr.z + nrt.z));
 }
 
 // Workspace layout, offsets in floats, every region 16-byte aligned.  It
@@ -1174,7 +1320,8 @@ __global__ void __launch_bounds__(256) assemble_grad_kernel(GArgs A)
 // reconstruction's (out[3], D) [buf][R] as float4; then the backward's own
 // planes, those that are accumulated last and zeroed before the passes.
 struct GradLayout {
-    size_t var[2], sd[2], beta, L, state, u[2], gbeta[2], gN[2], gD[2], gy[2], hn[2];
+    size_t var[2], sd[2], beta, L, state, crec, upair, u[2], gbeta[2], gN[2], gD[2], gt[2], gvs[2], hn[2];
+    size_t galb_t, gn_t;
     size_t zero_begin, gf[2], gs[2], gv[2], galb, gn, total;
 };
 
@@ -1195,14 +1342,19 @@ GradLayout grad_layout(int B, int H, int W, int sp, int rs)
     g.beta = take(2 * C * kBeta);   // [buf][C][18], the layout the forward kernels use
     g.L = take(2 * C * kL);
     g.state = take(2 * R * 4);
+    g.crec = take(C * 4 * kRecG2);
+    g.upair = take(C * 36);
     for (int X = 0; X < 2; ++X) {
         g.u[X] = take(C * kBeta);
         g.gbeta[X] = take(C * kBeta);
         g.gN[X] = take(3 * R);
         g.gD[X] = take(R);
-        g.gy[X] = take(3 * P);
+        g.gt[X] = take(3 * P);
+        g.gvs[X] = take(P);
         g.hn[X] = take(3 * P);
     }
+    g.galb_t = take(3 * P);
+    g.gn_t = take(3 * P);
     g.zero_begin = cur;
     for (int X = 0; X < 2; ++X) {
         g.gf[X] = take(3 * P);
@@ -1249,6 +1401,7 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
 {
     const GradLayout L = grad_layout(B, H, W, sp, rs);
     GArgs A{};
+    A.B = B;
     A.H = H;
     A.W = W;
     A.hw = win / 2;
@@ -1272,7 +1425,8 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
         g.gN = ws + L.gN[X];
         g.gD = ws + L.gD[X];
         g.gf = ws + L.gf[X];
-        g.gy = ws + L.gy[X];
+        g.gt = ws + L.gt[X];
+        g.gvs = ws + L.gvs[X];
         g.gs = ws + L.gs[X];
         g.gv = ws + L.gv[X];
         g.hn = ws + L.hn[X];
@@ -1280,9 +1434,13 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
         g.gvar = X ? g_varb : g_vara;
     }
     A.state = reinterpret_cast<const float4 *>(ws + L.state);
+    A.crec = reinterpret_cast<float4 *>(ws + L.crec);
+    A.upair = reinterpret_cast<float4 *>(ws + L.upair);
     A.alb = albedo;
     A.nrm = normal;
     A.galb = ws + L.galb;
+    A.galb_t = ws + L.galb_t;
+    A.gn_t = ws + L.gn_t;
     A.gn = ws + L.gn;
     A.out_a = g_imga;
     A.out_b = g_imgb;
@@ -1308,11 +1466,19 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
     dim3 g_out((A.Wr + 31) / 32, (A.Hr + 7) / 8, B), g_cen((A.Ws + 31) / 32, (A.Hs + 7) / 8, B);
     dim3 g_px((W + 31) / 32, (H + 7) / 8, B);
     const size_t rg_smem = recon_grad_smem(A.hw, A.sp, A.rs);
-    if (rg_smem <= 200 * 1024) {
+    int dev = 0, nsm = 148;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return e;
+    const size_t nrec4 = C * kRecG2;
+    centre_records_kernel<<<(unsigned)((nrec4 + 255) / 256), 256, 0, st>>>(A);
+    if (2 * rg_smem <= 200 * 1024) {
         if ((e = cudaFuncSetAttribute(recon_grad_pixel_x2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)rg_smem)) != cudaSuccess)
+                                      (int)(2 * rg_smem))) != cudaSuccess)
             return e;
-        recon_grad_pixel_x2_kernel<<<g_out, 256, rg_smem, st>>>(A);
+        const int ntiles = (int)(g_out.x * g_out.y * g_out.z);
+        recon_grad_pixel_x2_kernel<<<min(ntiles, 2 * nsm), 256, 2 * rg_smem, st>>>(A, g_out.x, g_out.y, ntiles,
+                                                                                 (int)(rg_smem / sizeof(float4)));
     } else {
         recon_grad_pixel_kernel<<<g_out, blk, 0, st>>>(A);
     }
@@ -1332,11 +1498,13 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
         return e;
     regression_grad_centre_kernel<<<dim3((A.Ws + kRowCentres - 1) / kRowCentres, A.Hs, B), 64, gc_smem, st>>>(A);
     const size_t tg_smem = tap_grad_smem(A.hw, A.sp);
-    if (tg_smem <= 200 * 1024) {
+    if (2 * tg_smem <= 200 * 1024) {
         if ((e = cudaFuncSetAttribute(regression_grad_tap_x2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)tg_smem)) != cudaSuccess)
+                                      (int)(2 * tg_smem))) != cudaSuccess)
             return e;
-        regression_grad_tap_x2_kernel<<<g_px, 256, tg_smem, st>>>(A);
+        const int ntiles = (int)(g_px.x * g_px.y * g_px.z);
+        regression_grad_tap_x2_kernel<<<min(ntiles, 2 * nsm), 256, 2 * tg_smem, st>>>(A, g_px.x, g_px.y, ntiles,
+                                                                                    (int)(tg_smem / sizeof(float4)));
     } else {
         regression_grad_tap_kernel<<<g_px, blk, 0, st>>>(A);
     }
