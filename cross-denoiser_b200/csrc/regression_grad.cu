@@ -1446,8 +1446,14 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
     A.out_b = g_imgb;
     A.out_alb = g_albedo;
     A.out_n = g_normal;
-    cudaError_t e = cudaMemsetAsync(ws + L.zero_begin, 0, (L.total - L.zero_begin) * sizeof(float), st);
-    if (e != cudaSuccess) return e;
+    // the accumulated planes start at zero, unless the packed pixel side
+    // stores every pixel of them first (recon_scale 1)
+    const size_t rg_smem = recon_grad_smem(A.hw, A.sp, A.rs);
+    const bool pixel_x2 = 2 * rg_smem <= 200 * 1024;
+    cudaError_t e;
+    if (!(pixel_x2 && rs == 1) &&
+        (e = cudaMemsetAsync(ws + L.zero_begin, 0, (L.total - L.zero_begin) * sizeof(float), st)) != cudaSuccess)
+        return e;
 
     // pass 1: forward quantities (variance, std, coefficients, Cholesky
     // factors, the reconstruction's outputs and weight sums), unless
@@ -1465,14 +1471,13 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
     dim3 blk(32, 8);
     dim3 g_out((A.Wr + 31) / 32, (A.Hr + 7) / 8, B), g_cen((A.Ws + 31) / 32, (A.Hs + 7) / 8, B);
     dim3 g_px((W + 31) / 32, (H + 7) / 8, B);
-    const size_t rg_smem = recon_grad_smem(A.hw, A.sp, A.rs);
     int dev = 0, nsm = 148;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
         (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
         return e;
     const size_t nrec4 = C * kRecG2;
     centre_records_kernel<<<(unsigned)((nrec4 + 255) / 256), 256, 0, st>>>(A);
-    if (2 * rg_smem <= 200 * 1024) {
+    if (pixel_x2) {
         if ((e = cudaFuncSetAttribute(recon_grad_pixel_x2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(2 * rg_smem))) != cudaSuccess)
             return e;
