@@ -59,6 +59,7 @@ struct GArgs {
     float *galb, *gn, *galb_t, *gn_t;
     float *out_a, *out_b, *out_alb, *out_n;   // final gradients
     int B, H, W, hw, sp, rs, Hs, Ws, Hr, Wr;
+    bool u_rows;   // pass 4 also writes u as [buffer][centre][18] (for the unstaged tap pass)
 };
 
 CD_DEV float3 f3(const float *p, size_t i) { return ld3(p, i); }
@@ -897,15 +898,16 @@ __global__ void __launch_bounds__(64, 8) regression_grad_centre_kernel(GArgs A)
     }
     const bool valid = i0 + lane < A.Ws;
     if (valid) {
-        float *ug = (X ? A.bf[1].u : A.bf[0].u) + ci * kBeta;
         float *up = reinterpret_cast<float *>(A.upair + ci * 9);   // pairs: channel k, row r at 12k + 4(r/2) + 2(r%2)
 #pragma unroll
         for (int k = 0; k < 3; ++k)
 #pragma unroll
-            for (int r = 0; r < kP; ++r) {
-                ug[r * 3 + k] = u[r * 3 + k];
-                up[12 * k + 4 * (r >> 1) + 2 * (r & 1) + X] = u[r * 3 + k];
-            }
+            for (int r = 0; r < kP; ++r) up[12 * k + 4 * (r >> 1) + 2 * (r & 1) + X] = u[r * 3 + k];
+        if (A.u_rows) {
+            float *ug = (X ? A.bf[1].u : A.bf[0].u) + ci * kBeta;
+#pragma unroll
+            for (int k = 0; k < kBeta; ++k) ug[k] = u[k];
+        }
     }
     const float3 fc = ld3(X ? imgb : imga, c), ac = ld3(alb, c), nc = ld3(nrm, c);
     const float vc = __ldg((X ? varb : vara) + c), sc = __ldg((X ? sdb : sda) + c);
@@ -1448,8 +1450,9 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
     A.out_n = g_normal;
     // the accumulated planes start at zero, unless the packed pixel side
     // stores every pixel of them first (recon_scale 1)
-    const size_t rg_smem = recon_grad_smem(A.hw, A.sp, A.rs);
-    const bool pixel_x2 = 2 * rg_smem <= 200 * 1024;
+    const size_t rg_smem = recon_grad_smem(A.hw, A.sp, A.rs), tg_smem = tap_grad_smem(A.hw, A.sp);
+    const bool pixel_x2 = 2 * rg_smem <= 200 * 1024, tap_x2 = 2 * tg_smem <= 200 * 1024;
+    A.u_rows = !tap_x2;
     cudaError_t e;
     if (!(pixel_x2 && rs == 1) &&
         (e = cudaMemsetAsync(ws + L.zero_begin, 0, (L.total - L.zero_begin) * sizeof(float), st)) != cudaSuccess)
@@ -1502,8 +1505,7 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
                                   (int)gc_smem)) != cudaSuccess)
         return e;
     regression_grad_centre_kernel<<<dim3((A.Ws + kRowCentres - 1) / kRowCentres, A.Hs, B), 64, gc_smem, st>>>(A);
-    const size_t tg_smem = tap_grad_smem(A.hw, A.sp);
-    if (2 * tg_smem <= 200 * 1024) {
+    if (tap_x2) {
         if ((e = cudaFuncSetAttribute(regression_grad_tap_x2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(2 * tg_smem))) != cudaSuccess)
             return e;
