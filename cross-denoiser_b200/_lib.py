@@ -66,8 +66,8 @@ SIGNATURES = {
 
 # kernels each entry point launches (for the launch count of bench.py)
 KERNELS_PER_CALL = {
-    "cd_cross_regression": 3, "cd_cross_regression_fp64_fallback": 3, "cd_cross_regression_grad": 8,
-    "cd_cross_regression_keep": 3, "cd_cross_regression_grad_kept": 6, "cd_spatial_filter": 1, "cd_spatial_filter_grad": 1, "cd_spatial_filter_stored": 1, "cd_spatial_filter_grad_stored": 1,
+    "cd_cross_regression": 3, "cd_cross_regression_fp64_fallback": 3, "cd_cross_regression_grad": 10,
+    "cd_cross_regression_keep": 3, "cd_cross_regression_grad_kept": 7, "cd_spatial_filter": 1, "cd_spatial_filter_grad": 1, "cd_spatial_filter_stored": 1, "cd_spatial_filter_grad_stored": 1,
     "cd_reproject": 1,   # 2 for the three 3-channel tensors of the step (ops.reproject passes the count)
     "cd_erode3x3": 1, "cd_temporal_screening": 1, "cd_erode_temporal_screening": 1,
     "cd_prepare_input": 1, "cd_aggregation_loss": 2, "cd_filter_aggregate": 2,

@@ -108,9 +108,10 @@ CD_API cd_status cd_cross_regression_fp64_fallback(const float *imga, const floa
 /* dL/d(imga, imgb, albedo, normal).  grad_vara / grad_varb may be NULL       */
 /* (no loss on the variances).  It recomputes the forward, so it needs only  */
 /* the forward's inputs.  Same requirements as cd_cross_regression; the      */
-/* workspace holds the recomputed coefficients, their Cholesky factors and   */
-/* the per-pixel partial gradients (with recon_scale 1: 274 floats per      */
-/* pixel at sparsity 1, 55 at sparsity 4).                                    */
+/* workspace holds the recomputed coefficients, their Cholesky factors, the  */
+/* reconstruction's outputs and weight sums, staged centre records and the   */
+/* per-pixel partial gradients (with recon_scale 1: 378 floats per pixel at  */
+/* sparsity 1, 76 at sparsity 4).                                             */
 /*  grad_outa, grad_outb : [B,H/recon_scale,W/recon_scale,3]                  */
 /*  grad_vara, grad_varb : [B,H,W,1] or NULL                                  */
 /*  grad_imga, grad_imgb, grad_albedo, grad_normal : [B,H,W,3]                */
@@ -133,8 +134,9 @@ CD_API cd_status cd_cross_regression_grad(const float *imga, const float *imgb,
 /* Forward and backward of CrossRegression without the backward's recompute */
 /* (no counterpart in the reference).  cd_cross_regression_keep computes    */
 /* cd_cross_regression's four outputs (bit-identical) and leaves the        */
-/* variances, standard deviations, coefficients and Cholesky factors in a   */
-/* workspace of cd_cross_regression_grad_workspace_size() bytes;            */
+/* variances, standard deviations, coefficients, Cholesky factors and the   */
+/* reconstruction's outputs and weight sums in a workspace of               */
+/* cd_cross_regression_grad_workspace_size() bytes;                         */
 /* cd_cross_regression_grad_kept then computes cd_cross_regression_grad's   */
 /* result (bit-identical) from that workspace without recomputing the       */
 /* forward.  Pass the same inputs, attributes and workspace to both, and    */
