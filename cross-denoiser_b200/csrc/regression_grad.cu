@@ -1251,13 +1251,14 @@ __global__ void __launch_bounds__(256, 2) regression_grad_tap_x2_kernel(GArgs A,
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) variance_grad_kernel(GArgs A)
 {
+    // one thread per (pixel, buffer): grid z = image * 2 + buffer
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= A.W || y >= A.H) return;
-    const int b = blockIdx.z;
+    const int b = blockIdx.z >> 1, X = blockIdx.z & 1;
     const size_t P = (size_t)A.H * A.W;
     const size_t p = b * P + (size_t)y * A.W + x;
-    for (int X = 0; X < 2; ++X) {
-        const GBuf &B_ = A.bf[X];
+    {
+        const GBuf &B_ = X ? A.bf[1] : A.bf[0];
         const float s = __ldg(B_.s + p);
         float gv = B_.gv[p] + (s > 0.f ? B_.gs[p] / (2.f * s) : 0.f) + B_.gvs[p];
         if (B_.gvar) gv += __ldg(B_.gvar + p);
@@ -1515,7 +1516,7 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
     } else {
         regression_grad_tap_kernel<<<g_px, blk, 0, st>>>(A);
     }
-    variance_grad_kernel<<<g_px, blk, 0, st>>>(A);
+    variance_grad_kernel<<<dim3(g_px.x, g_px.y, 2 * B), blk, 0, st>>>(A);
     assemble_grad_kernel<<<g_px, blk, 0, st>>>(A);
     return cudaGetLastError();
 }
