@@ -1246,8 +1246,8 @@ __global__ void __launch_bounds__(256, 2) regression_grad_tap_x2_kernel(GArgs A,
 // Pass 6a: dL/dv (through sqrt, the regression, the reconstruction and the
 // variance output) and the variance's own derivative:
 // v_p = |m_p - f_p|^2, m_p = mean of the in-bounds neighbours (without p).
-// h_p = 2 (m_p - f_p) dL/dv_p: f_p gets -h_p, each neighbour h_p / n_p
-// (gathered in pass 6b).
+// h_p = 2 (m_p - f_p) dL/dv_p: f_p gets -h_p = -n_p (h_p / n_p), each
+// neighbour h_p / n_p (both gathered in pass 6b).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) variance_grad_kernel(GArgs A)
 {
@@ -1278,10 +1278,12 @@ __global__ void __launch_bounds__(256) variance_grad_kernel(GArgs A)
         const float inv = n > 0 ? 1.f / (float)n : 0.f;
         const float h[3] = {2.f * (m[0] * inv - fp.x) * gv, 2.f * (m[1] * inv - fp.y) * gv,
                             2.f * (m[2] * inv - fp.z) * gv};
+        // h / n only: the assembly takes f_p's own term as n (h / n), except
+        // for a pixel without neighbours (a 1 x 1 image), whose -h goes here
         B_.hn[3 * p] = h[0] * inv;
         B_.hn[3 * p + 1] = h[1] * inv;
         B_.hn[3 * p + 2] = h[2] * inv;
-        add3(B_.gf, p, make_float3(-h[0], -h[1], -h[2]));
+        if (n == 0) add3(B_.gf, p, make_float3(-h[0], -h[1], -h[2]));
     }
 }
 
@@ -1289,31 +1291,30 @@ __global__ void __launch_bounds__(256) variance_grad_kernel(GArgs A)
 // planes: dL/dimga = gf(A) + gt(A), dL/dimgb = gf(B) + gt(B).
 __global__ void __launch_bounds__(256) assemble_grad_kernel(GArgs A)
 {
+    // one thread per (pixel, image): grid z = batch image * 2 + X; X = 0
+    // writes dL/dimga and dL/dalbedo, X = 1 dL/dimgb and dL/dnormal
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= A.W || y >= A.H) return;
-    const int b = blockIdx.z;
+    const int b = blockIdx.z >> 1, X = blockIdx.z & 1;
     const size_t P = (size_t)A.H * A.W;
     const size_t p = b * P + (size_t)y * A.W + x;
-    float3 g[2];
-    for (int X = 0; X < 2; ++X) {
-        const GBuf &B_ = A.bf[X];
-        float3 v = f3(B_.gf, p);
-        for (int iy = max(0, y - 1); iy <= min(A.H - 1, y + 1); ++iy)
-            for (int ix = max(0, x - 1); ix <= min(A.W - 1, x + 1); ++ix) {
-                if (ix == x && iy == y) continue;
-                const float3 h = f3(B_.hn, b * P + (size_t)iy * A.W + ix);
-                v.x += h.x;
-                v.y += h.y;
-                v.z += h.z;
-            }
-        g[X] = v;
-    }
-    const float3 ta = f3(A.bf[0].gt, p), tb = f3(A.bf[1].gt, p);
-    const float3 al = f3(A.galb, p), alt = f3(A.galb_t, p), nr = f3(A.gn, p), nrt = f3(A.gn_t, p);
-    st3(A.out_a, p, make_float3(g[0].x + ta.x, g[0].y + ta.y, g[0].z + ta.z));
-    st3(A.out_b, p, make_float3(g[1].x + tb.x, g[1].y + tb.y, g[1].z + tb.z));
-    st3(A.out_alb, p, make_float3(al.x + alt.x, al.y + alt.y, al.z + alt.z));
-    st3(A.out_n, p, make_float3(nr.x + nrt.x, nr.y + nrt.y, nr.z + nrt.z));
+    const GBuf &B_ = X ? A.bf[1] : A.bf[0];
+    const int sx = max(0, x - 1), ex = min(A.W - 1, x + 1), sy = max(0, y - 1), ey = min(A.H - 1, y + 1);
+    const float n = (float)((ex - sx + 1) * (ey - sy + 1) - 1);
+    const float3 g = f3(B_.gf, p), hp = f3(B_.hn, p);
+    float3 v = make_float3(g.x - n * hp.x, g.y - n * hp.y, g.z - n * hp.z);   // f_p's own term -h_p
+    for (int iy = sy; iy <= ey; ++iy)
+        for (int ix = sx; ix <= ex; ++ix) {
+            if (ix == x && iy == y) continue;
+            const float3 h = f3(B_.hn, b * P + (size_t)iy * A.W + ix);
+            v.x += h.x;
+            v.y += h.y;
+            v.z += h.z;
+        }
+    const float3 t = f3(B_.gt, p);
+    st3(X ? A.out_b : A.out_a, p, make_float3(v.x + t.x, v.y + t.y, v.z + t.z));
+    const float3 c = f3(X ? A.gn : A.galb, p), ct = f3(X ? A.gn_t : A.galb_t, p);
+    st3(X ? A.out_n : A.out_alb, p, make_float3(c.x + ct.x, c.y + ct.y, c.z + ct.z));
 }
 
 // Workspace layout, offsets in floats, every region 16-byte aligned.  It
@@ -1517,7 +1518,7 @@ cudaError_t launch_regression_grad(const float *imga, const float *imgb, const f
         regression_grad_tap_kernel<<<g_px, blk, 0, st>>>(A);
     }
     variance_grad_kernel<<<dim3(g_px.x, g_px.y, 2 * B), blk, 0, st>>>(A);
-    assemble_grad_kernel<<<g_px, blk, 0, st>>>(A);
+    assemble_grad_kernel<<<dim3(g_px.x, g_px.y, 2 * B), blk, 0, st>>>(A);
     return cudaGetLastError();
 }
 
