@@ -15,8 +15,13 @@ Regression backward: float64 autograd of oracle/regression_fp64.py on
 data within 4 hw + 2 s + 2 = 38 px, so pixels at least 40 px inside a crop
 have their full-image gradient; 256 of them (x 4 inputs x 3 channels) are
 compared, and 16 against float64 central differences on the crop (h = 1e-4).
-Tolerance: |g - g64| <= 5e-4 max|g64| + 1e-3 |g64| (per crop), as for the
-small-image regression-gradient tests.
+Tolerance, per crop: the image gradients |g - g64| <= 1e-4 max|g64| +
+1e-4 |g64|, as the small-image regression-gradient tests (measured: within
+1.3e-7 of max|g64|); the albedo and normal gradients 1e-3 max|g64| + 1e-3
+|g64|, because each is a sum of per-pair terms w (u r - a beta) that nearly
+cancel (the normal equations drive the weighted residuals r to zero) and
+FP32 keeps their rounding: measured up to 6.6e-4 of max|g64| at this size.
+The finite differences within 5e-4 (their own truncation error).
 """
 import numpy as np
 import pytest
@@ -135,7 +140,8 @@ def test_regression_gradient_512(cd, cuda):
             want = g64[i][qy, qx]
             have = got[i][b, oy + qy, ox + qx]
             scale = np.abs(g64[i][margin:C - margin, margin:C - margin]).max()
-            bad = np.abs(have - want) > 5e-4 * scale + 1e-3 * np.abs(want)
+            tol = 1e-4 if i < 2 else 1e-3   # images | albedo, normal
+            bad = np.abs(have - want) > tol * scale + tol * np.abs(want)
             assert not bad.any(), (f"crop {k} input {i}: {bad.sum()} of {bad.size} beyond tolerance, "
                                    f"max err {np.abs(have - want).max():.3g}, scale {scale:.3g}")
         checked += 32
