@@ -19,8 +19,10 @@ Tolerance, per crop: the image gradients |g - g64| <= 1e-4 max|g64| +
 1e-4 |g64|, as the small-image regression-gradient tests (measured: within
 1.3e-7 of max|g64|); the albedo and normal gradients 1e-3 max|g64| + 1e-3
 |g64|, because each is a sum of per-pair terms w (u r - a beta) that nearly
-cancel (the normal equations drive the weighted residuals r to zero) and
-FP32 keeps their rounding: measured up to 6.6e-4 of max|g64| at this size.
+cancel (the normal equations drive the weighted residuals r to zero), with
+u = A^-1 dL/dbeta large where A is ill-conditioned, so the FP32 solve's and
+sums' rounding remains in the small result: measured up to 6.6e-4 of
+max|g64| at this size.
 The finite differences within 5e-4 (their own truncation error).
 """
 import numpy as np
