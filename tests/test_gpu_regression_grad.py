@@ -59,8 +59,13 @@ def check(got, want, what):
                                f"max err {err.max():.3g}, max|g64| {np.abs(w).max():.3g}")
 
 
+# The last two cases reach the backward's unstaged forms: at sparsity 1 and
+# window 9 the staged pixel- and tap-side records exceed shared memory; at
+# window 63 a centre has more than 64 candidate columns, so the centre-side
+# pass runs one thread per centre testing the range rule in its loop.
 @pytest.mark.parametrize("H,W,win,sp,rs", [(16, 20, 5, 1, 1), (24, 32, 7, 2, 1), (24, 32, 7, 2, 2),
-                                            (32, 40, 9, 4, 1), (32, 40, 11, 4, 2), (24, 32, 5, 4, 4)])
+                                            (32, 40, 9, 4, 1), (32, 40, 11, 4, 2), (24, 32, 5, 4, 4),
+                                            (24, 32, 9, 1, 1), (72, 80, 63, 4, 1)])
 def test_vs_fp64_autograd(cd, cuda, H, W, win, sp, rs):
     ins = inputs(cd, H, W, seed=H + win)
     ups = upstream(1, H, W, rs, seed=win * 7 + sp)
